@@ -1,0 +1,174 @@
+// hx_internal.h -- host-side internals shared by the library's translation
+// units: grid description, device buffers, kernel launchers and the context.
+#pragma once
+#include <algorithm>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "hx_common.cuh"
+
+namespace hx {
+
+struct Grid {
+  int nxe, nye, nze;  // elements per axis
+  int nxn, nyn, nzn;  // nodes per axis (elements + 1)
+  __host__ __device__ int64_t nodes() const { return (int64_t)nxn * nyn * nzn; }
+  __host__ __device__ int64_t elems() const { return (int64_t)nxe * nye * nze; }
+  __host__ __device__ int64_t dofs() const { return 3 * nodes(); }
+};
+
+// Owning device buffer (grown on demand, never shrunk while a context lives).
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  T* ensure(size_t count) {
+    if (count > n) {
+      if (p) HX_CUDA(cudaFree(p));
+      p = nullptr;
+      n = 0;
+      HX_CUDA(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
+      n = count;
+    }
+    return p;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+// ---- operator (hx_operator.cu) ----
+int mv_kchunk(const Grid& g);
+size_t mv_num_blocks(const Grid& g);
+template <typename T>
+void launch_matvec(cudaStream_t s, int mode, const T* x, T* y, const T* fac, const uint8_t* nmask,
+                   const Grid& g, const ElemCoef<T>& K, T shift, CgState* st, double* partials,
+                   double* out);
+template <typename T>
+void launch_node_diag(cudaStream_t s, const T* fac, const uint8_t* bcfree, uint8_t* nmask, T* diag,
+                      const Grid& g, const ElemCoef<double>& K, double* partials, CgState* st,
+                      double* out);
+template <typename T>
+void launch_minv(cudaStream_t s, const uint8_t* nmask, const T* diag, T* minv, int64_t nn,
+                 double shift);
+
+// ---- vector kernels (hx_vector.cu) ----
+unsigned vec_blocks(int64_t n);
+constexpr int VEC_THREADS = 256;
+template <typename T>
+void launch_cg_init(cudaStream_t s, const T* b, const T* q, const T* minv, T* r, T* p, int64_t n,
+                    CgState* st, double* partials);
+template <typename T>
+void launch_cg_update(cudaStream_t s, T* x, const T* p, T* r, const T* q, const T* minv, int64_t n,
+                      CgState* st, double* partials);
+template <typename T>
+void launch_cg_pupdate(cudaStream_t s, T* p, const T* r, const T* minv, int64_t n, CgState* st);
+void launch_copy_if_snap(cudaStream_t s, double* dst, const double* src, int64_t n, CgState* st);
+// out = sum (b - q)^2 over the n entries, and sum b^2
+void launch_resid_norm(cudaStream_t s, const double* b, const double* q, int64_t n, CgState* st,
+                       double* partials, double* out2);
+// b = minv != 0 ? f : 0
+template <typename T>
+void launch_mask_rhs(cudaStream_t s, const double* f, const T* minv, double* b, int64_t n);
+// dot product, deterministic: out = sum a*b
+void launch_dot(cudaStream_t s, const double* a, const double* b, int64_t n, CgState* st,
+                double* partials, double* out);
+// Mixed precision helpers.
+// r = b - q (FP64), r32 = r * scale_from_state; also ||r||^2 into st->rr etc.
+void launch_ir_residual(cudaStream_t s, const double* b, const double* q, float* r32, int64_t n,
+                        CgState* st, double* partials);
+void launch_ir_correct(cudaStream_t s, double* x, const float* d32, int64_t n, const CgState* st);
+template <typename TD, typename TS>
+void launch_convert(cudaStream_t s, TD* dst, const TS* src, int64_t n);
+void launch_fill_zero(cudaStream_t s, void* p, size_t bytes);
+
+// ---- filter (hx_filter.cu) ----
+struct FilterCoef {
+  // assembled 1D tridiagonal entries per axis: [axis][0=boundary-lo row,
+  // 1=interior, 2=boundary-hi row][lo, diag, hi] for S and M
+  double S[3][3][3];
+  double M[3][3][3];
+  double r2;
+  double vol8;
+};
+FilterCoef make_filter_coef(double dx, double dy, double dz, double radius, int ref_compat);
+void launch_filter_rhs(cudaStream_t s, const double* rho, double* b, const Grid& g, double vol8);
+void launch_filter_invdiag(cudaStream_t s, double* invd, const Grid& g, const FilterCoef& F);
+void launch_filter_matvec(cudaStream_t s, const double* x, double* y, const Grid& g,
+                          const FilterCoef& F, CgState* st, double* partials);
+void launch_filter_extract(cudaStream_t s, const double* x, double* out, const Grid& g);
+
+// ---- stress / OC (hx_stress.cu) ----
+void launch_stress(cudaStream_t s, const double* u, const double* dens, double E, double nu,
+                   const Grid& g, double hx, double hy, double hz, double* principal, double* vm,
+                   double* voigt, double* l1, double* dir);
+void launch_energy(cudaStream_t s, const double* u, const Grid& g, const ElemCoef<double>& K,
+                   double* ce);
+void launch_oc(cudaStream_t s, const double* x, const double* dc, const double* dv, int64_t n,
+               double volfrac, double move, double* xnew, CgState* st, double* partials,
+               int max_steps);
+
+}  // namespace hx
+
+// ---------------------------------------------------------------------------
+// The context behind the opaque hx_ctx handle.
+// ---------------------------------------------------------------------------
+struct hx_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+
+  // mesh
+  bool has_mesh = false;
+  hx::Grid g{};
+  double h[3] = {1, 1, 1};
+  double E = 1.0, nu = 0.3;
+  hx::ElemCoef<double> K{};
+  // caller numbering -> grid numbering (empty vectors: identity)
+  std::vector<int64_t> node_map;  // caller node -> grid node
+  std::vector<int64_t> elem_map;  // caller element -> grid element
+  int64_t n_user_nodes = 0, n_user_elem = 0;
+  std::vector<uint8_t> present;   // grid node present in the caller's mesh
+
+  // boundary conditions: per grid node free-DOF bits
+  std::vector<uint8_t> bcfree;
+  bool bc_dirty = true;
+
+  // device buffers
+  hx::DevBuf<uint8_t> d_bcfree, d_nmask;
+  hx::DevBuf<double> d_f, d_b, d_fac, d_x, d_r, d_p, d_q, d_minv, d_xbest;
+  hx::DevBuf<double> d_partials, d_scalars;
+  hx::DevBuf<hx::CgState> d_state;
+  hx::DevBuf<float> d_fac32, d_minv32, d_r32, d_p32, d_q32, d_x32;
+  hx::DevBuf<double> d_aux0, d_aux1, d_aux2, d_aux3, d_aux4, d_aux5;
+  hx::CgState* h_state = nullptr;  // pinned mirror
+
+  // host<->device staging for F32 callers
+  hx::DevBuf<char> d_stage;
+
+  // filter grid and cache (the counterpart of GLOBAL_HELMHOLTZ_CACHE)
+  hx::Grid fg{};
+  double fh[3] = {1, 1, 1};
+  bool filt_ready = false;
+  double filt_radius = -1;
+  int filt_compat = -1;
+  hx::DevBuf<double> f_invd, f_x, f_r, f_p, f_q, f_b, f_rho, f_out;
+
+  // filter kernel coefficients of the last filter call (for timing)
+  double f_radius_last = 0;
+  int f_compat_last = 0;
+  bool f_used = false;
+
+  int64_t launches = 0;  // kernels launched on behalf of this context
+
+  size_t partial_capacity() const { return d_partials.n; }
+};

@@ -1,0 +1,262 @@
+/*
+ * hexat_b200.h -- C ABI of the B200-native inner-solve library for HEXA(T)
+ * v069 (voxel Hex8 linear elasticity + topology optimisation).
+ *
+ * The library replaces, on one GPU, the reference's Julia/CUDA.jl routines
+ * for the linear solve, the Helmholtz density filter and the element stress.
+ * Reference paths below are relative to the reference project root
+ * (v069_2025_12_09_HEXAS_TOPO_anti_checkerboard/).
+ *
+ * Conventions (identical to the reference's data layout):
+ *  - nodes: nN x 3 Float32, Julia column-major (x of node n at n, y at nN+n,
+ *    z at 2nN+n);  elements: nE x 8 Int64, column-major, 1-based, corner
+ *    order of src/Core/Element.jl:8-17;  bc_indicator: nN x 3 Float32
+ *    column-major, > 0 means the DOF is fixed;  f, u: 3nN interleaved
+ *    (dof = 3*node + component);  per-element arrays have length nE.
+ *  - Every call is blocking: results are in the caller's buffers on return.
+ *    The caller owns all buffers; no pointer is retained after a call.
+ *  - Every call returns an hx_status and never throws across the ABI.
+ *    hx_last_error() describes the last failure of a context.
+ *  - Nothing falls back to the CPU: without a usable device, calls return
+ *    HX_NO_DEVICE / HX_CUDA_ERROR.
+ */
+#ifndef HEXAT_B200_H
+#define HEXAT_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HX_API __attribute__((visibility("default")))
+
+typedef enum hx_status {
+  HX_OK = 0,
+  HX_NOT_CONVERGED = 1, /* iteration or wall-clock limit reached */
+  HX_STALLED = 2,       /* accepted stagnation / refinement made no progress */
+  HX_BREAKDOWN = 3,     /* p.Ap <= 0 or NaN */
+  HX_NONFINITE = 4,     /* NaN/Inf in the residual */
+  HX_OOM = 5,
+  HX_BAD_ARG = 6,
+  HX_CUDA_ERROR = 7,
+  HX_NO_DEVICE = 8,
+  HX_DIVERGED = 9 /* residual exploded or grew 100x over its best */
+} hx_status;
+
+typedef enum hx_dtype { HX_F32 = 0, HX_F64 = 1 } hx_dtype;
+
+typedef enum hx_precision {
+  HX_PREC_FP64 = 0,      /* plain FP64 Jacobi-PCG */
+  HX_PREC_MIXED32 = 1,   /* FP32 inner PCG inside FP64 iterative refinement */
+  HX_PREC_MIXED_BF16 = 2 /* as MIXED32 with the search direction stored in BF16 */
+} hx_precision;
+
+typedef enum hx_preconditioner {
+  HX_PC_JACOBI = 0,
+  HX_PC_LEARNED = 1, /* CNN preconditioner inside flexible CG (needs weights) */
+  HX_PC_NONE = 2
+} hx_preconditioner;
+
+typedef struct hx_solve_opts {
+  int32_t precision;       /* hx_precision */
+  int32_t preconditioner;  /* hx_preconditioner */
+  double tol;              /* stop when ||r||/||b|| < tol */
+  int32_t max_iter;
+  int32_t warm_start;      /* 1: u_inout holds the initial guess */
+  double shift_factor;     /* shift s = shift_factor * max(diag over free DOFs) */
+  double wall_limit_ms;    /* 0: no limit */
+  int32_t check_every;     /* host poll period in iterations (0: automatic) */
+  int32_t keep_best;       /* 1: keep the best iterate (reference semantics) */
+  double inner_tol;        /* mixed precision: inner relative tolerance */
+  int32_t max_refine;      /* mixed precision: outer refinement steps */
+  int32_t ref_retry;       /* 1: reference retry/shift-escalation semantics */
+  int32_t divergence_checks; /* 1: explosion and 100x-over-best checks */
+  int32_t verify_true_residual; /* 1: recompute ||b-Au|| in FP64 at the end */
+  int32_t reserved[6];
+} hx_solve_opts;
+
+typedef struct hx_solve_report {
+  int32_t status;       /* hx_status of the solve */
+  int32_t iterations;   /* CG iterations (all inner iterations when mixed) */
+  int32_t refinements;  /* outer refinement steps (mixed) */
+  int32_t attempts;     /* retry attempts used (ref_retry) */
+  int32_t fallback_used;/* learned -> Jacobi fallback taken */
+  int32_t zero_rhs;     /* 1: ||f_free|| == 0, u = 0 returned */
+  double rel_res;       /* recursive residual at stop (reference final_rel_res) */
+  double true_rel_res;  /* ||b - (K+sI)u|| / ||b|| recomputed in FP64 */
+  double shift;         /* diagonal shift actually used */
+  double time_setup_ms;
+  double time_solve_ms;
+  double time_total_ms;
+  double time_device_ms;   /* CUDA-event time of the call on the context stream */
+  double kernel_launches;  /* kernels launched by the call (graph nodes included) */
+  double reserved[2];
+} hx_solve_report;
+
+typedef struct hx_ctx hx_ctx;
+
+/* ---- context -------------------------------------------------------------
+ * One context per host thread; it owns one CUDA stream and the cached device
+ * buffers (the counterpart of the reference's GLOBAL_HELMHOLTZ_CACHE,
+ * src/Optimization/GPUHelmholtz.jl:12-33).  Uses the primary context of
+ * `device`, as CUDA.jl does (src/Main.jl:179). */
+HX_API hx_status hx_create(hx_ctx **out, int32_t device);
+HX_API void hx_destroy(hx_ctx *ctx);
+HX_API const char *hx_last_error(const hx_ctx *ctx);
+HX_API void hx_default_opts(hx_solve_opts *opts);
+HX_API const char *hx_status_string(int32_t status);
+/* The context's CUDA stream (a cudaStream_t), for callers that bracket
+ * library calls with their own CUDA events. */
+HX_API hx_status hx_get_stream(const hx_ctx *ctx, void **stream);
+/* Total kernels this context has launched (graph nodes included). */
+HX_API int64_t hx_kernel_launches(const hx_ctx *ctx);
+
+/* ---- mesh, material, boundary conditions ---------------------------------
+ * hx_set_grid: the structured mesh of src/Mesh/Mesh.jl:23-60 (generate_mesh)
+ * with nx*ny*nz elements of size dx*dy*dz.
+ * hx_set_mesh: any node/element arrays in the reference layout.  A mesh whose
+ * nodes sit on a lattice (generate_mesh output, or its pruned subset from
+ * src/Mesh/MeshPruner.jl:18-112) is embedded in its bounding grid so the
+ * structured kernels run; absent elements get zero stiffness and nodes
+ * without stiffness are held fixed (what reconstruct_full_solution,
+ * MeshPruner.jl:120-138, returns for them).  Element size is taken from the
+ * first element, as src/Solvers/GPUSolver.jl:136-145 does.
+ * hx_set_bc: src/Core/Boundary.jl:135-160 bc_indicator. */
+HX_API hx_status hx_set_grid(hx_ctx *ctx, int64_t nx, int64_t ny, int64_t nz,
+                             double dx, double dy, double dz);
+HX_API hx_status hx_set_mesh(hx_ctx *ctx, const float *nodes, int64_t n_nodes,
+                             const int64_t *elements, int64_t n_elem);
+HX_API hx_status hx_set_material(hx_ctx *ctx, double E, double nu);
+HX_API hx_status hx_set_bc(hx_ctx *ctx, const float *bc_indicator,
+                           int64_t n_nodes);
+/* Grid shape of the current mesh (elements per axis) and the mapping of the
+ * caller's node/element numbering to grid positions (-1: none). */
+HX_API hx_status hx_get_grid(const hx_ctx *ctx, int64_t dims[3], double h[3]);
+
+/* ---- stiffness operator ---------------------------------------------------
+ * y = sum_e factor_e * Ke * x_e over all elements, no boundary conditions,
+ * no shift: src/Solvers/CPUSolver.jl:50-94 apply_stiffness, with
+ * factor_e = E*density_e (0 for skipped elements).  Host arrays in the
+ * caller's numbering. */
+HX_API hx_status hx_apply_stiffness(hx_ctx *ctx, int32_t dtype, const void *x,
+                                    const void *factor, void *y);
+/* Jacobi diagonal, src/Solvers/CPUSolver.jl:109-148. */
+HX_API hx_status hx_diagonal(hx_ctx *ctx, int32_t dtype, const void *factor,
+                             void *diag);
+
+/* ---- linear solve ---------------------------------------------------------
+ * Solves (K_ff + s I) u_f = f_f on the free DOFs by Jacobi-PCG with
+ * M^-1 = 1/(diag + s) (src/Solvers/GPUSolver.jl:274-609, M_inv at :402).
+ * factor: per-element stiffness factor (E*density, or the caller's SIMP
+ * modulus).  u_inout: initial guess when opts->warm_start, full-length
+ * solution (zeros at fixed DOFs) on return.  Host arrays of `dtype`. */
+HX_API hx_status hx_solve(hx_ctx *ctx, int32_t dtype, const void *f,
+                          const void *factor, void *u_inout,
+                          const hx_solve_opts *opts, hx_solve_report *report);
+/* The same with FP64 device pointers in grid numbering (no host traffic). */
+HX_API hx_status hx_solve_device(hx_ctx *ctx, const double *f_dev,
+                                 const double *factor_dev, double *u_dev,
+                                 const hx_solve_opts *opts,
+                                 hx_solve_report *report);
+
+/* Drop-in for GPUSolver.solve_system_gpu(nodes, elements, E, nu,
+ * bc_indicator, f, density; max_iter, tol, shift_factor,
+ * min_stiffness_threshold, u_guess) -> (x_full, final_rel_res, prec_name),
+ * src/Solvers/GPUSolver.jl:611-627 (called from
+ * src/Solvers/IterativeSolver.jl:27-39).  Elements with density <
+ * min_stiffness_threshold are inactive (GPUSolver.jl:128); factor =
+ * E*density (:147).  u_guess may be NULL (cold start).  Writes x_full
+ * (3*n_nodes), *final_rel_res and the preconditioner name. */
+HX_API hx_status hx_solve_system_gpu(
+    hx_ctx *ctx, const float *nodes, int64_t n_nodes, const int64_t *elements,
+    int64_t n_elem, float E, float nu, const float *bc_indicator,
+    const float *f, const float *density, int32_t max_iter, double tol,
+    float shift_factor, float min_stiffness_threshold, const float *u_guess,
+    float *x_full, double *final_rel_res, char *prec_name,
+    int32_t prec_name_cap);
+
+/* ---- Helmholtz PDE density filter ------------------------------------------
+ * (r^2 K + M) x = T rho with T the lumped vol/8 scatter, Jacobi-CG (at most
+ * max_iter iterations, residual tested every 10), element value = mean of
+ * its 8 nodes: src/Optimization/GPUHelmholtz.jl:39-229.  ref_compat=1 uses
+ * the reference element whose top face sits at z=+dz (Element.jl:106-107,
+ * an element 1.5*dz tall); ref_compat=0 the geometric element.  Structured
+ * grids only (the reference always filters the full grid). */
+HX_API hx_status hx_filter(hx_ctx *ctx, int32_t dtype, const void *rho,
+                           void *rho_out, double radius, int32_t ref_compat,
+                           double tol, int32_t max_iter,
+                           hx_solve_report *report);
+HX_API hx_status hx_filter_device(hx_ctx *ctx, const double *rho_dev,
+                                  double *out_dev, double radius,
+                                  int32_t ref_compat, double tol,
+                                  int32_t max_iter, hx_solve_report *report);
+/* Drop-in for GPUHelmholtz.apply_gpu_filter!(density, nElem_x, nElem_y,
+ * nElem_z, dx, dy, dz, radius, elements, tol) -> (filtered, time, iters, res),
+ * src/Optimization/GPUHelmholtz.jl:344-376.  On failure returns a non-OK
+ * status (the reference returned Float32[] to request its CPU fallback). */
+HX_API hx_status hx_apply_gpu_filter(hx_ctx *ctx, const float *density,
+                                     int64_t nelem_x, int64_t nelem_y,
+                                     int64_t nelem_z, double dx, double dy,
+                                     double dz, double radius, double tol,
+                                     int32_t ref_compat, float *filtered,
+                                     double *time_s, int32_t *iters,
+                                     double *res);
+
+/* ---- stress ----------------------------------------------------------------
+ * Centre-point stress with modulus E*density[e] for density > 1e-6:
+ * principal values (descending, 3 per element), von Mises, Voigt
+ * (xx,yy,zz,xy,yz,xz), L1 = sum |principal|, unit direction of the largest
+ * principal stress (sign: largest-magnitude component positive; the
+ * reference's LAPACK sign is arbitrary).  src/Core/Stress.jl:10-100.
+ * Outputs are element-major (principal[3e+i], voigt[6e+i], dir[3e+i]),
+ * i.e. the memory layout of the reference's 3 x nE / 6 x nE matrices. */
+HX_API hx_status hx_stress(hx_ctx *ctx, int32_t dtype, const void *u,
+                           const void *density, double E, double nu,
+                           void *principal, void *vonmises, void *voigt,
+                           void *l1, void *dir);
+/* Drop-in for Stress.compute_stress_field(nodes, elements, U, E, nu,
+ * density), src/Core/Stress.jl:57-100. */
+HX_API hx_status hx_compute_stress_field(
+    hx_ctx *ctx, const float *nodes, int64_t n_nodes, const int64_t *elements,
+    int64_t n_elem, const float *U, float E, float nu, const float *density,
+    float *principal, float *vonmises, float *voigt, float *l1, float *dir);
+
+/* ---- compliance, sensitivities, OC update ------------------------------------
+ * hx_compliance: c = f.u in FP64 (src/Main.jl:428 computes it on the host).
+ * hx_element_energy: ce_e = u_e^T Ke u_e with unit modulus (no reference
+ * counterpart; the compliance sensitivity of the OC method is
+ * dc_e = -p*rho^(p-1)*(E0-Emin)*ce_e).
+ * hx_oc_update: optimality-criteria update with bisection on the volume
+ * multiplier (no reference counterpart: the reference updates by stress
+ * ratio, src/Optimization/TopOpt.jl:260-402; this is the published OC method
+ * of the top88/top3d family).  See the library documentation for the exact
+ * rule. */
+HX_API hx_status hx_compliance(hx_ctx *ctx, int32_t dtype, const void *f,
+                               const void *u, double *c);
+HX_API hx_status hx_element_energy(hx_ctx *ctx, int32_t dtype, const void *u,
+                                   void *ce);
+HX_API hx_status hx_oc_update(hx_ctx *ctx, int32_t dtype, const void *x,
+                              const void *dc, const void *dv, double volfrac,
+                              double move, void *xnew, double *lambda,
+                              int32_t *steps);
+
+/* ---- instrumentation ---------------------------------------------------------
+ * Average device time (CUDA events on the context stream) of `reps`
+ * back-to-back launches of one kernel on the buffers of the last hx_solve /
+ * hx_solve_device (kernel ids below); inputs are left unchanged except the
+ * kernels' scratch outputs.  Used by the benchmark for the live roofline. */
+enum {
+  HX_KERNEL_MATVEC_FP64 = 0, /* CG-mode K.p with the fused p.q reduction */
+  HX_KERNEL_UPDATE_FP64 = 1, /* x,r update + r.z, r.r reductions */
+  HX_KERNEL_PUPDATE_FP64 = 2,
+  HX_KERNEL_MATVEC_FP32 = 3,
+  HX_KERNEL_FILTER_MATVEC = 4
+};
+HX_API hx_status hx_time_kernel(hx_ctx *ctx, int32_t kernel, int32_t reps,
+                                double *avg_ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HEXAT_B200_H */

@@ -1,0 +1,189 @@
+"""ctypes wrapper of the C oracle (hexat_oracle.c) plus the OC loop restated
+in numpy.  TEST INFRASTRUCTURE ONLY (see hexat_oracle.c header): the product
+never imports this module.  Parity unpinned (the reference has no golden
+vectors); pinned instead against scipy and analytic properties in tests/.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "libhexat_oracle.so")
+_lib = None
+
+
+def build():
+    src = os.path.join(HERE, "hexat_oracle.c")
+    if not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(src):
+        subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = C.CDLL(LIB)
+        d, i32, i64, vp = C.c_double, C.c_int32, C.c_int64, C.c_void_p
+        sig = {
+            "hxo_canonical_ke": (None, [d, d, d, d, vp]),
+            "hxo_scalar_ke_me": (None, [d, d, d, C.c_int, vp, vp]),
+            "hxo_apply_stiffness": (None, [i64, i64, vp, vp, vp, vp, vp, C.c_int]),
+            "hxo_diagonal": (None, [i64, i64, vp, vp, vp, vp]),
+            "hxo_cg_solve": (C.c_int, [i64, i64, vp, vp, vp, vp, vp, vp, C.c_int, C.c_int, d, d,
+                                       C.c_int, C.c_int, C.POINTER(d), C.POINTER(d)]),
+            "hxo_helmholtz_filter": (C.c_int, [i64, i64, vp, d, d, d, d, C.c_int, vp, vp, d,
+                                               C.c_int, C.POINTER(d)]),
+            "hxo_sym3_eigen": (None, [vp, vp, vp]),
+            "hxo_stress": (None, [i64, i64, vp, vp, vp, d, d, vp, vp, vp, vp, vp, vp]),
+            "hxo_element_energy": (None, [i64, vp, vp, vp, vp]),
+            "hxo_oc_update": (C.c_int, [i64, vp, vp, vp, d, d, vp, C.POINTER(d)]),
+        }
+        for k, (r, a) in sig.items():
+            f = getattr(L, k)
+            f.restype = r
+            f.argtypes = a
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _c(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+def canonical_ke(dx=1.0, dy=1.0, dz=1.0, nu=0.3):
+    ke = np.zeros(576)
+    lib().hxo_canonical_ke(dx, dy, dz, nu, _p(ke))
+    return ke.reshape(24, 24)
+
+
+def scalar_ke_me(dx=1.0, dy=1.0, dz=1.0, ref_compat=1):
+    ke = np.zeros(64)
+    me = np.zeros(64)
+    lib().hxo_scalar_ke_me(dx, dy, dz, int(ref_compat), _p(ke), _p(me))
+    return ke.reshape(8, 8), me.reshape(8, 8)
+
+
+def apply_stiffness(conn0, n_nodes, ke, factor, x, nthreads=0):
+    conn0 = _c(conn0, np.int32)
+    ke = _c(ke, np.float64)
+    factor = _c(factor, np.float64)
+    x = _c(x, np.float64)
+    y = np.zeros(3 * n_nodes)
+    lib().hxo_apply_stiffness(n_nodes, conn0.shape[0], _p(conn0), _p(ke), _p(factor), _p(x),
+                              _p(y), int(nthreads))
+    return y
+
+
+def diagonal(conn0, n_nodes, ke, factor):
+    conn0 = _c(conn0, np.int32)
+    d = np.zeros(3 * n_nodes)
+    lib().hxo_diagonal(n_nodes, conn0.shape[0], _p(conn0), _p(_c(ke, np.float64)),
+                       _p(_c(factor, np.float64)), _p(d))
+    return d
+
+
+def free_mask_from(bc_indicator, diag):
+    """Free DOFs: not fixed by the BC indicator and carrying stiffness."""
+    fixed = (np.asarray(bc_indicator) > 0).reshape(-1)
+    return (~fixed & (diag > 0)).astype(np.uint8)
+
+
+def cg_solve(conn0, n_nodes, ke, factor, free_mask, f, x0=None, max_iter=40000, tol=1e-6,
+             shift_factor=0.0, precond_add=True, nthreads=0):
+    """Returns (x_full, iterations, rel_res, shift); iterations -1 = breakdown."""
+    conn0 = _c(conn0, np.int32)
+    x = np.zeros(3 * n_nodes) if x0 is None else _c(x0, np.float64).copy()
+    rel = C.c_double()
+    sh = C.c_double()
+    it = lib().hxo_cg_solve(n_nodes, conn0.shape[0], _p(conn0), _p(_c(ke, np.float64)),
+                            _p(_c(factor, np.float64)), _p(_c(free_mask, np.uint8)),
+                            _p(_c(f, np.float64)), _p(x), int(x0 is not None), int(max_iter),
+                            float(tol), float(shift_factor), int(bool(precond_add)),
+                            int(nthreads), C.byref(rel), C.byref(sh))
+    return x, it, rel.value, sh.value
+
+
+def helmholtz_filter(conn0, n_nodes, rho, dx, dy, dz, radius, ref_compat=1, tol=1e-5,
+                     max_iter=200):
+    conn0 = _c(conn0, np.int32)
+    rho = _c(rho, np.float64)
+    out = np.zeros_like(rho)
+    rel = C.c_double()
+    it = lib().hxo_helmholtz_filter(n_nodes, conn0.shape[0], _p(conn0), dx, dy, dz, radius,
+                                    int(ref_compat), _p(rho), _p(out), tol, int(max_iter),
+                                    C.byref(rel))
+    return out, it, rel.value
+
+
+def sym3_eigen(s6):
+    s6 = _c(s6, np.float64)
+    ev = np.zeros(3)
+    v0 = np.zeros(3)
+    lib().hxo_sym3_eigen(_p(s6), _p(ev), _p(v0))
+    return ev, v0
+
+
+def stress(conn0, nodes, u, E, nu, density):
+    conn0 = _c(conn0, np.int32)
+    ne = conn0.shape[0]
+    nodes = _c(nodes, np.float64)
+    out = [np.zeros((ne, 3)), np.zeros(ne), np.zeros((ne, 6)), np.zeros(ne), np.zeros((ne, 3))]
+    lib().hxo_stress(nodes.shape[0], ne, _p(conn0), _p(nodes), _p(_c(u, np.float64)), E, nu,
+                     _p(_c(density, np.float64)), *[_p(o) for o in out])
+    return tuple(out)
+
+
+def element_energy(conn0, ke, u):
+    conn0 = _c(conn0, np.int32)
+    ce = np.zeros(conn0.shape[0])
+    lib().hxo_element_energy(conn0.shape[0], _p(conn0), _p(_c(ke, np.float64)),
+                             _p(_c(u, np.float64)), _p(ce))
+    return ce
+
+
+def oc_update(x, dc, dv, volfrac, move):
+    x = _c(x, np.float64)
+    xn = np.zeros_like(x)
+    lam = C.c_double()
+    steps = lib().hxo_oc_update(x.shape[0], _p(x), _p(_c(dc, np.float64)),
+                                _p(_c(dv, np.float64)), volfrac, move, _p(xn), C.byref(lam))
+    return xn, lam.value, steps
+
+
+def topopt_oc_loop(conn0, n_nodes, dims, bc_indicator, f, volfrac, radius, n_iter, p=3.0,
+                   e0=1.0, emin=1e-9, nu=0.3, move=0.2, tol=1e-6, ref_compat=0,
+                   filter_tol=1e-5, filter_max_iter=200, nthreads=0):
+    """The OC loop (published method, no reference counterpart), restated with
+    the oracle's primitives in the order the library's driver uses:
+    rho = F(x); factor = SIMP(rho); warm-started PCG; c = f.u;
+    dc = -p rho^(p-1) (E0-Emin) ce; dc_x = F(dc); OC bisection on x.
+    Returns (compliance history, final x, final rho)."""
+    ke = canonical_ke(1.0, 1.0, 1.0, nu)
+    ne = conn0.shape[0]
+    x = np.full(ne, volfrac)
+    u = None
+    hist = []
+    rho = x
+    for _ in range(n_iter):
+        rho, _, _ = helmholtz_filter(conn0, n_nodes, x, 1.0, 1.0, 1.0, radius, ref_compat,
+                                     filter_tol, filter_max_iter)
+        fac = emin + np.power(np.clip(rho, 0.0, None), p) * (e0 - emin)
+        diag = diagonal(conn0, n_nodes, ke, fac)
+        free = free_mask_from(bc_indicator, diag)
+        u, it, rel, _ = cg_solve(conn0, n_nodes, ke, fac, free, f * free, x0=u, tol=tol,
+                                 nthreads=nthreads)
+        c = float(np.dot(f, u))
+        hist.append(c)
+        ce = element_energy(conn0, ke, u)
+        dc = -p * np.power(np.clip(rho, 0.0, None), p - 1) * (e0 - emin) * ce
+        dcf, _, _ = helmholtz_filter(conn0, n_nodes, dc, 1.0, 1.0, 1.0, radius, ref_compat,
+                                     filter_tol, filter_max_iter)
+        x, _, _ = oc_update(x, dcf, np.ones(ne), volfrac, move)
+    return np.array(hist), x, rho
