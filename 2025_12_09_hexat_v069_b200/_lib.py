@@ -17,7 +17,7 @@ HX_OOM, HX_BAD_ARG, HX_CUDA_ERROR, HX_NO_DEVICE, HX_DIVERGED = 5, 6, 7, 8, 9
 HX_F32, HX_F64 = 0, 1
 HX_PREC_FP64, HX_PREC_MIXED32, HX_PREC_MIXED_BF16 = 0, 1, 2
 HX_PC_JACOBI, HX_PC_LEARNED, HX_PC_NONE = 0, 1, 2
-(HX_KERNEL_MATVEC_FP64, HX_KERNEL_UPDATE_FP64, HX_KERNEL_PUPDATE_FP64, HX_KERNEL_MATVEC_FP32,
+(HX_KERNEL_PCG_STEP_FP64, HX_KERNEL_PCG_UPDATE_FP64, HX_KERNEL_APPLY_FP64, HX_KERNEL_PCG_STEP_FP32,
  HX_KERNEL_FILTER_MATVEC) = range(5)
 
 

@@ -53,6 +53,13 @@ template <typename T>
 void launch_matvec(cudaStream_t s, int mode, const T* x, T* y, const T* fac, const uint8_t* nmask,
                    const Grid& g, const ElemCoef<T>& K, T shift, CgState* st, double* partials,
                    double* out);
+// Fused PCG step (see hx_operator.cu): p_out = M^-1 r + beta p_in,
+// x += alpha_old p_in (owned nodes), q = mask(K p_out + s p_out),
+// st->alpha = rz / (p_out . q).
+template <typename T>
+void launch_pcg_step(cudaStream_t s, const T* pin, T* pout, const T* r, const T* minv, T* x, T* q,
+                     const T* fac, const uint8_t* nmask, const Grid& g, const ElemCoef<T>& K,
+                     T shift, CgState* st, double* partials);
 template <typename T>
 void launch_node_diag(cudaStream_t s, const T* fac, const uint8_t* bcfree, uint8_t* nmask, T* diag,
                       const Grid& g, const ElemCoef<double>& K, double* partials, CgState* st,
@@ -72,6 +79,12 @@ void launch_cg_update(cudaStream_t s, T* x, const T* p, T* r, const T* q, const 
                       CgState* st, double* partials);
 template <typename T>
 void launch_cg_pupdate(cudaStream_t s, T* p, const T* r, const T* minv, int64_t n, CgState* st);
+template <typename T>
+void launch_cg_update2(cudaStream_t s, T* r, const T* q, const T* minv, int64_t n, CgState* st,
+                       double* partials);
+template <typename T>
+void launch_axpy_state(cudaStream_t s, T* dst, const T* x, const T* p, int64_t n,
+                       const CgState* st, int when_snap);
 void launch_copy_if_snap(cudaStream_t s, double* dst, const double* src, int64_t n, CgState* st);
 // out = sum (b - q)^2 over the n entries, and sum b^2
 void launch_resid_norm(cudaStream_t s, const double* b, const double* q, int64_t n, CgState* st,
@@ -145,10 +158,10 @@ struct hx_ctx {
 
   // device buffers
   hx::DevBuf<uint8_t> d_bcfree, d_nmask;
-  hx::DevBuf<double> d_f, d_b, d_fac, d_x, d_r, d_p, d_q, d_minv, d_xbest;
+  hx::DevBuf<double> d_f, d_b, d_fac, d_x, d_r, d_p, d_p2, d_q, d_minv, d_xbest;
   hx::DevBuf<double> d_partials, d_scalars;
   hx::DevBuf<hx::CgState> d_state;
-  hx::DevBuf<float> d_fac32, d_minv32, d_r32, d_p32, d_q32, d_x32;
+  hx::DevBuf<float> d_fac32, d_minv32, d_r32, d_p32, d_p32b, d_q32, d_x32;
   hx::DevBuf<double> d_aux0, d_aux1, d_aux2, d_aux3, d_aux4, d_aux5;
   hx::CgState* h_state = nullptr;  // pinned mirror
 

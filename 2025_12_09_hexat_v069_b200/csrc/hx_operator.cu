@@ -1,4 +1,5 @@
-// hx_operator.cu -- structured-grid Hex8 stiffness operator K(f) x.
+// hx_operator.cu -- structured-grid Hex8 stiffness operator K(f) x, alone or
+// fused with the CG direction/solution updates.
 //
 // Layout in HBM: node n = i + NXn*(j + NYn*k) (i fastest, src/Mesh/Mesh.jl:
 // 114-116), vectors interleaved 3 per node (dof = 3n + c), element
@@ -6,21 +7,26 @@
 // byte of free-DOF bits per node.
 //
 // Kernel design (replaces the one-thread-per-element, 24-atomics kernel of
-// src/Solvers/GPUSolver.jl:37-79):
+// src/Solvers/GPUSolver.jl:37-79 and the broadcast kernels around it):
 //  * a CTA owns a 31 x (BY-1) column of output nodes and marches along z
 //    over a chunk of node planes; its 32 x BY threads each own one element
 //    column, recomputing the one-element halo in x and y (atomic-free and
 //    deterministic);
-//  * node planes are staged into shared memory with cp.async (zero-filled
-//    outside the grid), double-buffered so the next plane loads while the
-//    current element layer computes;
-//  * each element product runs in the Haar basis (45 nonzeros, see
-//    hx_common.cuh); bottom-corner results meet the carried top-corner
-//    results of the layer below in registers, then the four element columns
-//    around a node are summed with one warp shuffle (x) and one shared-memory
-//    exchange (y);
-//  * the epilogue applies the free-DOF mask and the diagonal shift and
-//    accumulates p.q for the CG step, reduced deterministically.
+//  * node planes (tile + one-node halo) are staged into shared memory with
+//    cp.async into a 4-slot ring: plane k+3 loads while plane k+2 is
+//    transformed in place and planes k, k+1 feed the element products;
+//  * the element product runs in the per-axis sum/difference (Haar) basis
+//    (45 nonzeros, see hx_common.cuh), one displacement component at a
+//    time to bound register pressure; the top-face outputs are carried in
+//    the Haar domain until the layer above adds its bottom face;
+//  * the four element columns around a node are summed with one warp
+//    shuffle (x) and one shared-memory exchange (y);
+//  * FUSED (the PCG step): the staged plane holds p_old, r, M^-1 and x; the
+//    in-place transform forms p = M^-1 r + beta p_old, and for owned nodes
+//    stores p and updates x += alpha_old p_old.  p ping-pongs between two
+//    buffers so neighbouring CTAs never read a value another CTA rewrote.
+//    The epilogue applies the free-DOF mask and the shift and reduces p.q
+//    deterministically into the CG state (alpha = rz / pq).
 #include "hx_internal.h"
 
 namespace hx {
@@ -28,161 +34,286 @@ namespace hx {
 namespace {
 
 constexpr int MV_BX = 32;
+constexpr int MV_BY = 8;
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
   return (unsigned)__cvta_generic_to_shared(p);
 }
 
 template <int BYTES>
-__device__ __forceinline__ void cp_async_zfill(void* sdst, const void* gsrc, bool valid) {
+__device__ __forceinline__ void cp_async_zfill(unsigned sdst, const void* gsrc, bool valid) {
   const unsigned n = valid ? BYTES : 0;
-  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(smem_u32(sdst)),
-               "l"(gsrc), "n"(BYTES), "r"(n));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(sdst), "l"(gsrc),
+               "n"(BYTES), "r"(n));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
-}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
 
-template <typename T, int BY>
-struct MvSmem {
-  T xs[2][BY + 1][MV_BX + 1][3];
-  T red[BY][MV_BX][3];
+// Shared-memory layout (dynamic).  Planes are component-major
+// ([c][row][node]) so the lanes of a warp touch consecutive words.
+template <typename T, int BY, bool FUSED>
+struct OpSmem {
+  static constexpr int PLANE = 3 * (BY + 1) * (MV_BX + 1);
+  T p[4][PLANE];                   // x or p, 4-slot ring
+  T r[FUSED ? 2 : 1][PLANE];       // r (FUSED), 2-slot ring
+  T m[FUSED ? 2 : 1][PLANE];       // M^-1 (FUSED), 2-slot ring
+  T x[FUSED ? 2 : 1][PLANE];       // x (FUSED), 2-slot ring
+  T red[BY][3][MV_BX];             // y-direction partials
 };
 
-// Issue the copies of node plane kp (tile incl. one-node halo) into slot.
-template <typename T, int BY>
-__device__ __forceinline__ void issue_plane(MvSmem<T, BY>& sm, int slot, const T* __restrict__ x,
-                                            const Grid& g, int i0, int j0, int kp, int tid) {
-  constexpr int ROW = (MV_BX + 1) * 3;
-  constexpr int NT = MV_BX * BY;
-  const bool kin = kp >= 0 && kp < g.nzn;
-  const int64_t base = (int64_t)kp * g.nxn * g.nyn;
-  for (int idx = tid; idx < (BY + 1) * ROW; idx += NT) {
-    const int b = idx / ROW, rem = idx - b * ROW;
-    const int a = rem / 3, c = rem - a * 3;
-    const int ii = i0 - 1 + a, jj = j0 - 1 + b;
-    const bool ok = kin && ii >= 0 && ii < g.nxn && jj >= 0 && jj < g.nyn;
-    const T* src = ok ? x + 3 * (base + (int64_t)jj * g.nxn + ii) + c : x;
-    cp_async_zfill<sizeof(T)>(&sm.xs[slot][b][a][c], src, ok);
-  }
-  cp_async_commit();
+template <typename T>
+struct OpArgs {
+  const T* pin;   // vector to multiply (MODE 0-2) or p_old (FUSED)
+  const T* r;     // FUSED: residual
+  const T* minv;  // FUSED: Jacobi inverse diagonal
+  T* x;           // FUSED: solution (x += alpha_old p_old on owned nodes)
+  T* pout;        // FUSED: new direction p
+  T* q;           // output K p (masked, shifted)
+  const T* fac;
+  const uint8_t* nmask;
+  Grid g;
+  int kchunk;
+  ElemCoef<T> K;
+  T shift;
+  CgState* st;
+  double* partials;
+  double* out;
+};
+
+__device__ __forceinline__ int ring4(int k) { return (k + 4) & 3; }
+__device__ __forceinline__ int ring2(int k) { return (k + 2) & 1; }
+
+// 2D sum/difference transform of a node-plane face: v = corners (bx + 2by)
+// -> P = coefficients (sigma_x + 2 sigma_y).
+template <typename T>
+__device__ __forceinline__ void face_fwd(const T (&v)[4], T (&P)[4]) {
+  const T e0s = v[0] + v[1], e0d = v[1] - v[0], e1s = v[2] + v[3], e1d = v[3] - v[2];
+  P[0] = e0s + e1s;
+  P[1] = e0d + e1d;
+  P[2] = e1s - e0s;
+  P[3] = e1d - e0d;
 }
 
-// MODE 0: y = mask(K x + s x);  MODE 1: also out[0] = sum x.y;
-// MODE 2: CG step, st->pq = p.q, st->alpha = rz / pq, breakdown detection.
-template <typename T, int BY, int MODE>
-__global__ void __launch_bounds__(MV_BX* BY)
-    k_matvec_struct(const T* __restrict__ x, T* __restrict__ y, const T* __restrict__ fac,
-                    const uint8_t* __restrict__ nmask, Grid g, int kchunk, ElemCoef<T> K,
-                    T shift, CgState* st, double* partials, double* out) {
-  if (MODE == 2 && st->status != HX_RUNNING) return;
-  __shared__ MvSmem<T, BY> sm;
+// Component C of f * Lambda U: the diagonal part plus the couplings with
+// the other two components (see haar_apply in hx_common.cuh).
+template <typename T, int C>
+__device__ __forceinline__ void lambda_row(const ElemCoef<T>& K, const T (&U)[3][8], T (&Y)[8]) {
+  Y[0] = T(0);
+#pragma unroll
+  for (int s = 1; s < 8; ++s) Y[s] = K.dg[C][s] * U[C][s];
+#pragma unroll
+  for (int t = 1; t <= 2; ++t) {
+    const int o = (C + t) % 3;
+    const int k = 3 - C - o;
+#pragma unroll
+    for (int sk = 0; sk < 2; ++sk) {
+      const int P = (1 << o) | (sk << k);  // sigma_C = s, sigma_o = d
+      const int Q = (1 << C) | (sk << k);  // sigma_C = d, sigma_o = s
+      Y[Q] += K.lam[k][sk] * U[o][P];
+      Y[P] += K.mu[k][sk] * U[o][Q];
+    }
+  }
+}
+
+// MODE 0: q = mask(K x + s x);  MODE 1: also out[0] = x.q;
+// MODE 2: CG matvec, st->pq = p.q, st->alpha = rz / pq, breakdown test;
+// MODE 3: fused PCG step (see file header), then as MODE 2.
+template <typename T, int BY, int MODE, int MINB>
+__global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
+  constexpr bool FUSED = MODE == 3;
+  constexpr int NT = MV_BX * BY;
+  constexpr int PLANE = OpSmem<T, BY, FUSED>::PLANE;
+  constexpr int RW = MV_BX + 1;          // nodes per staged row
+  constexpr int CPL = (BY + 1) * RW;      // staged nodes per component
+  constexpr int NCP = (PLANE + NT - 1) / NT;
+  if (MODE >= 2 && A.st->status != HX_RUNNING) return;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  OpSmem<T, BY, FUSED>& sm = *reinterpret_cast<OpSmem<T, BY, FUSED>*>(smraw);
+  const Grid g = A.g;
   const int lx = threadIdx.x, ly = threadIdx.y;
   const int tid = lx + MV_BX * ly;
   const int i0 = blockIdx.x * (MV_BX - 1), j0 = blockIdx.y * (BY - 1);
-  const int k0 = blockIdx.z * kchunk;
-  const int k1 = min(k0 + kchunk, g.nzn);
+  const int k0 = blockIdx.z * A.kchunk;
+  const int k1 = min(k0 + A.kchunk, g.nzn);
   const int in = i0 - 1 + lx, jn = j0 - 1 + ly;
   const bool col_ok = in >= 0 && jn >= 0 && in < g.nxe && jn < g.nye;
   const bool out_ok = lx >= 1 && ly >= 1 && in < g.nxn && jn < g.nyn;
   const int64_t nplane = (int64_t)g.nxn * g.nyn;
   const int64_t eplane = (int64_t)g.nxe * g.nye;
-
-  issue_plane<T, BY>(sm, (k0 - 1) & 1, x, g, i0, j0, k0 - 1, tid);
-  issue_plane<T, BY>(sm, k0 & 1, x, g, i0, j0, k0, tid);
-  cp_async_wait<1>();
-  __syncthreads();
-
-  T xb[4][3], acc[4][3];
-  {
-    const int s = (k0 - 1) & 1;
-#pragma unroll
-    for (int q = 0; q < 4; ++q)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        xb[q][c] = sm.xs[s][ly + (q >> 1)][lx + (q & 1)][c];
-        acc[q][c] = T(0);
-      }
+  T alpha_old = T(0), beta_old = T(0);
+  if (FUSED) {
+    alpha_old = (T)A.st->alpha;
+    beta_old = (T)A.st->beta;
   }
+
+  // Copy assignment, the same for every plane: staged value idx is the
+  // shared index itself, (component c, row b, node a) with a fastest.
+  int goff[NCP];       // offset within a plane (3 * node-in-plane + c)
+  unsigned flags = 0;  // bit q: in grid, bit 8+q: owned node
+#pragma unroll
+  for (int q = 0; q < NCP; ++q) {
+    const int idx = tid + q * NT;
+    const int c = idx / CPL, rem = idx - c * CPL;
+    const int b = rem / RW, a = rem - b * RW;
+    const int ii = i0 - 1 + a, jj = j0 - 1 + b;
+    const bool ok = idx < PLANE && ii >= 0 && ii < g.nxn && jj >= 0 && jj < g.nyn;
+    const bool own = ok && a >= 1 && a <= MV_BX - 1 && b >= 1 && b <= BY - 1;
+    goff[q] = ok ? 3 * (jj * g.nxn + ii) + c : 0;
+    flags |= (ok ? 1u : 0u) << q;
+    flags |= (own ? 1u : 0u) << (8 + q);
+  }
+
+  auto issue = [&](int kp) {
+    const bool kin = kp >= 0 && kp < g.nzn;
+    const int64_t base = (int64_t)kp * nplane * 3;
+    const unsigned sp = smem_u32(&sm.p[ring4(kp)][0]);
+    const unsigned sr = smem_u32(&sm.r[FUSED ? ring2(kp) : 0][0]);
+    const unsigned smv = smem_u32(&sm.m[FUSED ? ring2(kp) : 0][0]);
+    const unsigned sx = smem_u32(&sm.x[FUSED ? ring2(kp) : 0][0]);
+#pragma unroll
+    for (int q = 0; q < NCP; ++q) {
+      const int idx = tid + q * NT;
+      if (q == NCP - 1 && idx >= PLANE) continue;
+      const bool ok = kin && ((flags >> q) & 1u);
+      const int64_t gi = ok ? base + goff[q] : 0;
+      const unsigned so = (unsigned)idx * (unsigned)sizeof(T);
+      cp_async_zfill<sizeof(T)>(sp + so, A.pin + gi, ok);
+      if (FUSED) {
+        cp_async_zfill<sizeof(T)>(sr + so, A.r + gi, ok);
+        cp_async_zfill<sizeof(T)>(smv + so, A.minv + gi, ok);
+        cp_async_zfill<sizeof(T)>(sx + so, A.x + gi, ok);
+      }
+    }
+    cp_async_commit();
+  };
+
+  // FUSED: p = M^-1 r + beta p_old in place; owned nodes of owned planes
+  // store p and advance x with the old direction.
+  auto transform = [&](int kp) {
+    if (!FUSED) return;
+    const bool kown = kp >= k0 && kp < k1;
+    const int64_t base = (int64_t)kp * nplane * 3;
+    T* ps = &sm.p[ring4(kp)][0];
+    const T* rs = &sm.r[ring2(kp)][0];
+    const T* ms = &sm.m[ring2(kp)][0];
+    const T* xs = &sm.x[ring2(kp)][0];
+#pragma unroll
+    for (int q = 0; q < NCP; ++q) {
+      const int idx = tid + q * NT;
+      if (q == NCP - 1 && idx >= PLANE) continue;
+      const T pold = ps[idx];
+      const T pnew = ms[idx] * rs[idx] + beta_old * pold;
+      ps[idx] = pnew;
+      if (kown && ((flags >> (8 + q)) & 1u)) {
+        const int64_t gi = base + goff[q];
+        A.pout[gi] = pnew;
+        A.x[gi] = xs[idx] + alpha_old * pold;
+      }
+    }
+  };
+
+  auto face = [&](int kp, int c, T (&v)[4]) {
+    const T* ps = &sm.p[ring4(kp)][(c * (BY + 1) + ly) * RW + lx];
+    v[0] = ps[0];
+    v[1] = ps[1];
+    v[2] = ps[RW];
+    v[3] = ps[RW + 1];
+  };
+
+  // prologue: planes k0-1 and k0 staged (and transformed), k0+1 in flight
+  issue(k0 - 1);
+  issue(k0);
+  cp_async_wait_all();
+  __syncthreads();
+  transform(k0 - 1);
+  transform(k0);
+  if (k0 + 1 <= k1) issue(k0 + 1);
+  T Ytp[3][4];
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) Ytp[c][q] = T(0);
   double dsum = 0.0;
 
   for (int ke = k0 - 1; ke < k1; ++ke) {
     T f = T(0);
-    if (col_ok && ke >= 0 && ke < g.nze) f = fac[(int64_t)ke * eplane + (int64_t)jn * g.nxe + in];
-    cp_async_wait<0>();
-    __syncthreads();
-    // Slot ke&1 (plane ke) is no longer read by anyone: prefetch plane ke+2.
-    if (ke + 2 <= k1) issue_plane<T, BY>(sm, ke & 1, x, g, i0, j0, ke + 2, tid);
+    if (col_ok && ke >= 0 && ke < g.nze) f = A.fac[(int64_t)ke * eplane + (int64_t)jn * g.nxe + in];
+    cp_async_wait_all();
+    __syncthreads();  // A: planes ke, ke+1 ready; ke+2 landed; red consumed
+    if (ke + 2 <= k1) transform(ke + 2);
+    if (ke + 3 <= k1) issue(ke + 3);
 
-    const int s = (ke + 1) & 1;
-    T u[3][8], xt[4][3];
+    T U[3][8];
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
+    for (int c = 0; c < 3; ++c) {
+      T v[4], Pb[4], Pt[4];
+      face(ke, c, v);
+      face_fwd(v, Pb);
+      face(ke + 1, c, v);
+      face_fwd(v, Pt);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        xt[q][c] = sm.xs[s][ly + (q >> 1)][lx + (q & 1)][c];
-        u[c][q] = xb[q][c];
-        u[c][4 + q] = xt[q][c];
+      for (int q = 0; q < 4; ++q) {
+        U[c][q] = Pb[q] + Pt[q];
+        U[c][q + 4] = Pt[q] - Pb[q];
       }
-    T yv[3][8];
-    elem_apply<T>(K, f, u, yv);
-
+    }
     T rowA[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const T c0 = acc[0][c] + yv[c][0];
-      const T c1 = acc[1][c] + yv[c][1];
-      const T c2 = acc[2][c] + yv[c][2];
-      const T c3 = acc[3][c] + yv[c][3];
+      T Y[8];
+      if (c == 0) lambda_row<T, 0>(A.K, U, Y);
+      else if (c == 1) lambda_row<T, 1>(A.K, U, Y);
+      else lambda_row<T, 2>(A.K, U, Y);
+      T F[4];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) acc[q][c] = yv[c][4 + q];
+      for (int q = 0; q < 4; ++q) {
+        const T ys = Y[q] * f, yd = Y[q + 4] * f;
+        F[q] = (ys - yd) + Ytp[c][q];
+        Ytp[c][q] = ys + yd;
+      }
+      const T as = F[0] - F[2], ad = F[1] - F[3], bs = F[0] + F[2], bd = F[1] + F[3];
+      const T c0 = as - ad, c1 = as + ad, c2 = bs - bd, c3 = bs + bd;
       // element lx-1 contributes its +x corners to this thread's nodes
       const T l1 = __shfl_up_sync(0xffffffffu, c1, 1);
       const T l3 = __shfl_up_sync(0xffffffffu, c3, 1);
       rowA[c] = c0 + l1;
-      sm.red[ly][lx][c] = c2 + l3;
+      sm.red[ly][c][lx] = c2 + l3;
     }
-    __syncthreads();
+    __syncthreads();  // B: red of this layer visible
     if (ke >= k0 && out_ok) {
       const int64_t node = (int64_t)ke * nplane + (int64_t)jn * g.nxn + in;
-      const unsigned m = nmask ? nmask[node] : 7u;
+      const unsigned m = A.nmask ? A.nmask[node] : 7u;
+      const T* own = &sm.p[ring4(ke)][ly * RW + lx];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        T v = rowA[c] + sm.red[ly - 1][lx][c];
-        const T xv = xb[0][c];
-        v = ((m >> c) & 1u) ? v + shift * xv : T(0);
-        y[3 * node + c] = v;
+        T v = rowA[c] + sm.red[ly - 1][c][lx];
+        const T xv = own[c * (BY + 1) * RW];
+        v = ((m >> c) & 1u) ? v + A.shift * xv : T(0);
+        A.q[3 * node + c] = v;
         if (MODE != 0) dsum += (double)xv * (double)v;
       }
     }
-#pragma unroll
-    for (int q = 0; q < 4; ++q)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) xb[q][c] = xt[q][c];
   }
 
   if (MODE != 0) {
     double v[1] = {dsum};
-    if (grid_reduce<1>(v, partials, &st->ticket[TK_MATVEC]) && tid == 0) {
+    if (grid_reduce<1>(v, A.partials, &A.st->ticket[TK_MATVEC]) && tid == 0) {
       if (MODE == 1) {
-        out[0] = v[0];
+        A.out[0] = v[0];
       } else {
         const double pq = v[0];
-        st->pq = pq;
-        if (!(pq > 0.0) || !isfinite(pq)) {
-          st->status = HX_ST_BREAKDOWN;
-        } else {
-          st->alpha = st->rz / pq;
-        }
+        A.st->pq = pq;
+        if (!(pq > 0.0) || !isfinite(pq))
+          A.st->status = HX_ST_BREAKDOWN;
+        else
+          A.st->alpha = A.st->rz / pq;
       }
     }
   }
 }
 
 // Per-node Jacobi diagonal: diag(n,c) = kd[c] * sum of the factors of the
-// (up to 8) elements around n; node mask = fixed-DOF bits of `bcfree`
+// (up to 8) elements around n; node mask = free-DOF bits of `bcfree`
 // cleared where the node carries no stiffness.  Writes diag into `diag`,
 // the mask into `nmask`, and reduces the max diagonal over free DOFs.
 template <typename T>
@@ -218,9 +349,7 @@ __global__ void k_node_diag(const T* __restrict__ fac, const uint8_t* __restrict
     }
   }
   double v[1] = {mx};
-  if (grid_reduce<1, true>(v, partials, &st->ticket[TK_AUX]) &&
-      threadIdx.x == 0)
-    out[0] = v[0];
+  if (grid_reduce<1, true>(v, partials, &st->ticket[TK_AUX]) && threadIdx.x == 0) out[0] = v[0];
 }
 
 // minv = free ? 1/(diag + shift) : 0   (src/Solvers/GPUSolver.jl:402)
@@ -235,19 +364,32 @@ __global__ void k_minv(const uint8_t* __restrict__ nmask, const T* __restrict__ 
   }
 }
 
-constexpr int MV_BY = 8;
-
 inline dim3 mv_grid(const Grid& g, int kchunk) {
   return dim3(cdiv(g.nxn, MV_BX - 1), cdiv(g.nyn, MV_BY - 1), cdiv(g.nzn, kchunk));
+}
+
+template <typename T, int MODE>
+void launch_struct(cudaStream_t s, const OpArgs<T>& a) {
+  constexpr bool FUSED = MODE == 3;
+  constexpr int MINB = 2;
+  const size_t smem = sizeof(OpSmem<T, MV_BY, FUSED>);
+  static bool configured = false;  // per instantiation
+  if (!configured) {
+    HX_CUDA(cudaFuncSetAttribute(k_struct<T, MV_BY, MODE, MINB>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    configured = true;
+  }
+  k_struct<T, MV_BY, MODE, MINB><<<mv_grid(a.g, a.kchunk), dim3(MV_BX, MV_BY), smem, s>>>(a);
+  HX_CHECK_LAUNCH();
 }
 
 }  // namespace
 
 int mv_kchunk(const Grid& g) {
-  // Enough CTAs to fill every SM a few times; at least 8 planes per chunk so
-  // the recomputed halo layer stays small.
+  // About eight resident CTAs per SM's worth of work, at least 8 planes per
+  // chunk so the recomputed halo layer stays small.
   const int64_t cols = (int64_t)cdiv(g.nxn, MV_BX - 1) * cdiv(g.nyn, MV_BY - 1);
-  const int64_t want = 4LL * sm_count();
+  const int64_t want = 8LL * sm_count();
   int nch = (int)std::max<int64_t>(1, (want + cols - 1) / cols);
   int kc = (int)cdiv(g.nzn, nch);
   if (kc < 8) kc = std::min(8, g.nzn);
@@ -263,23 +405,46 @@ template <typename T>
 void launch_matvec(cudaStream_t s, int mode, const T* x, T* y, const T* fac, const uint8_t* nmask,
                    const Grid& g, const ElemCoef<T>& K, T shift, CgState* st, double* partials,
                    double* out) {
-  const int kc = mv_kchunk(g);
-  const dim3 grid = mv_grid(g, kc);
-  const dim3 block(MV_BX, MV_BY);
-  switch (mode) {
-    case 0:
-      k_matvec_struct<T, MV_BY, 0><<<grid, block, 0, s>>>(x, y, fac, nmask, g, kc, K, shift, st,
-                                                          partials, out);
-      break;
-    case 1:
-      k_matvec_struct<T, MV_BY, 1><<<grid, block, 0, s>>>(x, y, fac, nmask, g, kc, K, shift, st,
-                                                          partials, out);
-      break;
-    default:
-      k_matvec_struct<T, MV_BY, 2><<<grid, block, 0, s>>>(x, y, fac, nmask, g, kc, K, shift, st,
-                                                          partials, out);
-  }
-  HX_CHECK_LAUNCH();
+  OpArgs<T> a{};
+  a.pin = x;
+  a.q = y;
+  a.fac = fac;
+  a.nmask = nmask;
+  a.g = g;
+  a.kchunk = mv_kchunk(g);
+  a.K = K;
+  a.shift = shift;
+  a.st = st;
+  a.partials = partials;
+  a.out = out;
+  if (mode == 0)
+    launch_struct<T, 0>(s, a);
+  else if (mode == 1)
+    launch_struct<T, 1>(s, a);
+  else
+    launch_struct<T, 2>(s, a);
+}
+
+template <typename T>
+void launch_pcg_step(cudaStream_t s, const T* pin, T* pout, const T* r, const T* minv, T* x, T* q,
+                     const T* fac, const uint8_t* nmask, const Grid& g, const ElemCoef<T>& K,
+                     T shift, CgState* st, double* partials) {
+  OpArgs<T> a{};
+  a.pin = pin;
+  a.pout = pout;
+  a.r = r;
+  a.minv = minv;
+  a.x = x;
+  a.q = q;
+  a.fac = fac;
+  a.nmask = nmask;
+  a.g = g;
+  a.kchunk = mv_kchunk(g);
+  a.K = K;
+  a.shift = shift;
+  a.st = st;
+  a.partials = partials;
+  launch_struct<T, 3>(s, a);
 }
 
 template void launch_matvec<double>(cudaStream_t, int, const double*, double*, const double*,
@@ -288,6 +453,14 @@ template void launch_matvec<double>(cudaStream_t, int, const double*, double*, c
 template void launch_matvec<float>(cudaStream_t, int, const float*, float*, const float*,
                                    const uint8_t*, const Grid&, const ElemCoef<float>&, float,
                                    CgState*, double*, double*);
+template void launch_pcg_step<double>(cudaStream_t, const double*, double*, const double*,
+                                      const double*, double*, double*, const double*,
+                                      const uint8_t*, const Grid&, const ElemCoef<double>&,
+                                      double, CgState*, double*);
+template void launch_pcg_step<float>(cudaStream_t, const float*, float*, const float*,
+                                     const float*, float*, float*, const float*, const uint8_t*,
+                                     const Grid&, const ElemCoef<float>&, float, CgState*,
+                                     double*);
 
 template <typename T>
 void launch_node_diag(cudaStream_t s, const T* fac, const uint8_t* bcfree, uint8_t* nmask, T* diag,

@@ -192,40 +192,66 @@ static double jacobi_setup(hx_ctx* c, const double* fac, double shift_factor, do
 }
 
 // ---------------------------------------------------------------------------
-// Plain FP64 Jacobi-PCG.  b must already be masked; x holds the initial
-// guess (masked) when warm.  Returns the final device state.
+// Jacobi-PCG on the fused kernels (T = double: the plain FP64 solve; T =
+// float: the inner solve of mixed precision).  b must already be masked; x
+// holds the initial guess (masked) when warm.  Iteration k reads p_{k-1}
+// from P[(k+1)%2] and writes p_k into P[k%2]; the graph body runs two
+// iterations so the buffer roles stay fixed.  On exit the pending
+// x += alpha p of the last iteration is applied.  Returns the final state.
 // ---------------------------------------------------------------------------
-static CgState pcg_fp64(hx_ctx* c, const double* fac, const double* b, double* x, bool warm,
-                        double shift, const hx_solve_opts& o, double t0, bool* timed_out) {
+template <typename T>
+static CgState pcg_fused(hx_ctx* c, int slot, const T* fac, const T* b, T* x, bool warm, T shift,
+                         const ElemCoef<T>& K, T* r, T* P0, T* P1, T* q, const T* minv,
+                         T* xbest, const CgState& init, int check_every, double wall_ms,
+                         double t0, bool* timed_out) {
   const Grid& g = c->g;
   const int64_t n = g.dofs();
-  double* r = c->d_r.ensure(n);
-  double* p = c->d_p.ensure(n);
-  double* q = c->d_q.ensure(n);
-  double* minv = c->d_minv.p;
-  double* xbest = o.keep_best ? c->d_xbest.ensure(n) : nullptr;
-  CgState* st = c->d_state.p;
-  put_state(c, 0, fresh_state(o.tol, o.max_iter, 1, o.divergence_checks != 0, o.keep_best != 0));
+  CgState* st = c->d_state.p + slot;
+  put_state(c, slot, init);
   if (warm) {
-    launch_matvec<double>(c->stream, 0, x, q, fac, c->d_nmask.p, g, c->K, shift, st,
-                          c->d_partials.p, nullptr);
-    launch_cg_init<double>(c->stream, b, q, minv, r, p, n, st, c->d_partials.p);
+    launch_matvec<T>(c->stream, 0, x, q, fac, c->d_nmask.p, g, K, shift, c->d_state.p + 3,
+                     c->d_partials.p, nullptr);
+    launch_cg_init<T>(c->stream, b, q, minv, r, P1, n, st, c->d_partials.p);
   } else {
-    launch_fill_zero(c->stream, x, n * sizeof(double));
-    launch_cg_init<double>(c->stream, b, nullptr, minv, r, p, n, st, c->d_partials.p);
+    launch_fill_zero(c->stream, x, n * sizeof(T));
+    launch_cg_init<T>(c->stream, b, nullptr, minv, r, P1, n, st, c->d_partials.p);
   }
-  if (xbest) HX_CUDA(cudaMemcpyAsync(xbest, x, n * sizeof(double), cudaMemcpyDeviceToDevice,
-                                     c->stream));
-  CgState s0 = get_state(c, 0);
-  if (s0.status != HX_RUNNING || o.max_iter <= 0) return s0;
+  if (xbest) HX_CUDA(cudaMemcpyAsync(xbest, x, n * sizeof(T), cudaMemcpyDeviceToDevice, c->stream));
+  CgState s0 = get_state(c, slot);
+  if (s0.status != HX_RUNNING || init.max_iter <= 0) return s0;
   auto body = [&]() {
-    launch_matvec<double>(c->stream, 2, p, q, fac, c->d_nmask.p, g, c->K, shift, st,
-                          c->d_partials.p, nullptr);
-    launch_cg_update<double>(c->stream, x, p, r, q, minv, n, st, c->d_partials.p);
-    if (xbest) launch_copy_if_snap(c->stream, xbest, x, n, st);
-    launch_cg_pupdate<double>(c->stream, p, r, minv, n, st);
+    launch_pcg_step<T>(c->stream, P1, P0, r, minv, x, q, fac, c->d_nmask.p, g, K, shift, st,
+                       c->d_partials.p);
+    launch_cg_update2<T>(c->stream, r, q, minv, n, st, c->d_partials.p);
+    if (xbest) launch_axpy_state<T>(c->stream, xbest, x, P0, n, st, 1);
+    launch_pcg_step<T>(c->stream, P0, P1, r, minv, x, q, fac, c->d_nmask.p, g, K, shift, st,
+                       c->d_partials.p);
+    launch_cg_update2<T>(c->stream, r, q, minv, n, st, c->d_partials.p);
+    if (xbest) launch_axpy_state<T>(c->stream, xbest, x, P1, n, st, 1);
   };
-  return run_batched(c, 0, auto_batch(g, o.check_every), body, o.wall_limit_ms, t0, timed_out);
+  const int reps = std::max(1, check_every / 2);
+  CgState sf = run_batched(c, slot, reps, body, wall_ms, t0, timed_out);
+  // apply the pending step x_{k+1} = x_k + alpha_k p_k (not after a breakdown,
+  // whose alpha is invalid); p_k sits in P[(iter-1) % 2]
+  if (sf.status != HX_ST_BREAKDOWN && sf.iter > 0) {
+    T* pk = ((sf.iter - 1) % 2 == 0) ? P0 : P1;
+    launch_axpy_state<T>(c->stream, x, x, pk, n, st, 0);
+  }
+  return sf;
+}
+
+static CgState pcg_fp64(hx_ctx* c, const double* fac, const double* b, double* x, bool warm,
+                        double shift, const hx_solve_opts& o, double t0, bool* timed_out) {
+  const int64_t n = c->g.dofs();
+  double* r = c->d_r.ensure(n);
+  double* P0 = c->d_p.ensure(n);
+  double* P1 = c->d_p2.ensure(n);
+  double* q = c->d_q.ensure(n);
+  double* xbest = o.keep_best ? c->d_xbest.ensure(n) : nullptr;
+  const CgState init =
+      fresh_state(o.tol, o.max_iter, 1, o.divergence_checks != 0, o.keep_best != 0);
+  return pcg_fused<double>(c, 0, fac, b, x, warm, shift, c->K, r, P0, P1, q, c->d_minv.p, xbest,
+                           init, auto_batch(c->g, o.check_every), o.wall_limit_ms, t0, timed_out);
 }
 
 // FP64 true residual ||b - (K+sI)x|| / ||b||.
@@ -264,7 +290,6 @@ static CgState solve_mixed(hx_ctx* c, const double* fac, const double* b, double
   launch_convert<float, double>(c->stream, minv32, c->d_minv.p, n);
   const ElemCoef<float> K32 = to_float(c->K);
   CgState* so = c->d_state.p;      // outer
-  CgState* si = c->d_state.p + 1;  // inner
   // outer state: ||b|| from a dot product
   CgState s = fresh_state(o.tol, std::max(1, o.max_refine), 1, false, false);
   put_state(c, 0, s);
@@ -301,18 +326,11 @@ static CgState solve_mixed(hx_ctx* c, const double* fac, const double* b, double
       return so_h;
     }
     const int inner_max = std::max(1, o.max_iter - *inner_total);
-    put_state(c, 1, fresh_state(inner_tol, inner_max, 1, false, false));
-    launch_fill_zero(c->stream, d32, n * sizeof(float));
-    launch_cg_init<float>(c->stream, r32, nullptr, minv32, r32, p32, n, si, c->d_partials.p);
-    const float sh32 = (float)shift;
-    auto body = [&]() {
-      launch_matvec<float>(c->stream, 2, p32, q32, fac32, c->d_nmask.p, g, K32, sh32, si,
-                           c->d_partials.p, nullptr);
-      launch_cg_update<float>(c->stream, d32, p32, r32, q32, minv32, n, si, c->d_partials.p);
-      launch_cg_pupdate<float>(c->stream, p32, r32, minv32, n, si);
-    };
-    CgState si_h = run_batched(c, 1, auto_batch(g, o.check_every), body, o.wall_limit_ms, t0,
-                               timed_out);
+    float* p32b = c->d_p32b.ensure(n);
+    CgState si_h = pcg_fused<float>(c, 1, fac32, r32, d32, false, (float)shift, K32, r32, p32,
+                                    p32b, q32, minv32, nullptr,
+                                    fresh_state(inner_tol, inner_max, 1, false, false),
+                                    auto_batch(g, o.check_every), o.wall_limit_ms, t0, timed_out);
     *inner_total += si_h.iter;
     launch_ir_correct(c->stream, x, d32, n, so);
     if (*timed_out) {
@@ -552,36 +570,49 @@ hx_status time_kernel(hx_ctx* c, int kernel, int reps, double* avg_ms) {
   HX_CUDA(cudaEventCreate(&e0));
   HX_CUDA(cudaEventCreate(&e1));
   std::function<void()> body;
-  if (kernel == HX_KERNEL_MATVEC_FP64 || kernel == HX_KERNEL_UPDATE_FP64 ||
-      kernel == HX_KERNEL_PUPDATE_FP64) {
-    HX_REQUIRE(ready(c->d_p.n, n) && ready(c->d_q.n, n) && ready(c->d_r.n, n) &&
-                   ready(c->d_minv.n, n) && ready(c->d_fac.n, ne) && ready(c->d_nmask.n, g.nodes()),
+  if (kernel == HX_KERNEL_PCG_STEP_FP64 || kernel == HX_KERNEL_PCG_UPDATE_FP64 ||
+      kernel == HX_KERNEL_APPLY_FP64) {
+    HX_REQUIRE(ready(c->d_p.n, n) && ready(c->d_p2.n, n) && ready(c->d_q.n, n) &&
+                   ready(c->d_r.n, n) && ready(c->d_minv.n, n) && ready(c->d_fac.n, ne) &&
+                   ready(c->d_nmask.n, g.nodes()),
                "run a solve before timing its kernels");
     double* xs = c->d_aux0.ensure(n);
     HX_CUDA(cudaMemsetAsync(xs, 0, n * sizeof(double), c->stream));
-    if (kernel == HX_KERNEL_MATVEC_FP64)
+    if (kernel == HX_KERNEL_PCG_STEP_FP64)
       body = [&] {
-        launch_matvec<double>(c->stream, 2, c->d_p.p, c->d_q.p, c->d_fac.p, c->d_nmask.p, g, c->K,
-                              0.0, st, c->d_partials.p, nullptr);
+        launch_pcg_step<double>(c->stream, c->d_p.p, c->d_p2.p, c->d_r.p, c->d_minv.p, xs,
+                                c->d_q.p, c->d_fac.p, c->d_nmask.p, g, c->K, 0.0, st,
+                                c->d_partials.p);
       };
-    else if (kernel == HX_KERNEL_UPDATE_FP64)
+    else if (kernel == HX_KERNEL_PCG_UPDATE_FP64)
       body = [&] {
-        launch_cg_update<double>(c->stream, xs, c->d_p.p, c->d_r.p, c->d_q.p, c->d_minv.p, n, st,
-                                 c->d_partials.p);
+        launch_cg_update2<double>(c->stream, c->d_r.p, c->d_q.p, c->d_minv.p, n, st,
+                                  c->d_partials.p);
       };
     else
-      body = [&] { launch_cg_pupdate<double>(c->stream, c->d_p.p, c->d_r.p, c->d_minv.p, n, st); };
-  } else if (kernel == HX_KERNEL_MATVEC_FP32) {
-    HX_REQUIRE(ready(c->d_fac.n, ne) && ready(c->d_nmask.n, g.nodes()), "run a solve first");
+      body = [&] {
+        launch_matvec<double>(c->stream, 0, c->d_p.p, c->d_q.p, c->d_fac.p, c->d_nmask.p, g, c->K,
+                              0.0, st, c->d_partials.p, nullptr);
+      };
+  } else if (kernel == HX_KERNEL_PCG_STEP_FP32) {
+    HX_REQUIRE(ready(c->d_fac.n, ne) && ready(c->d_nmask.n, g.nodes()) && ready(c->d_minv.n, n),
+               "run a solve first");
     float* f32 = c->d_fac32.ensure(ne);
     float* p32 = c->d_p32.ensure(n);
+    float* p32b = c->d_p32b.ensure(n);
     float* q32 = c->d_q32.ensure(n);
+    float* r32 = c->d_r32.ensure(n);
+    float* m32 = c->d_minv32.ensure(n);
+    float* x32 = c->d_x32.ensure(n);
     launch_convert<float, double>(c->stream, f32, c->d_fac.p, ne);
+    launch_convert<float, double>(c->stream, m32, c->d_minv.p, n);
     HX_CUDA(cudaMemsetAsync(p32, 0, n * sizeof(float), c->stream));
+    HX_CUDA(cudaMemsetAsync(r32, 0, n * sizeof(float), c->stream));
+    HX_CUDA(cudaMemsetAsync(x32, 0, n * sizeof(float), c->stream));
     const ElemCoef<float> K32 = to_float(c->K);
-    body = [&, f32, p32, q32, K32] {
-      launch_matvec<float>(c->stream, 2, p32, q32, f32, c->d_nmask.p, g, K32, 0.0f, st,
-                           c->d_partials.p, nullptr);
+    body = [&, f32, p32, p32b, q32, r32, m32, x32, K32] {
+      launch_pcg_step<float>(c->stream, p32, p32b, r32, m32, x32, q32, f32, c->d_nmask.p, g, K32,
+                             0.0f, st, c->d_partials.p);
     };
   } else if (kernel == HX_KERNEL_FILTER_MATVEC) {
     HX_REQUIRE(c->f_used, "run a filter before timing its kernel");

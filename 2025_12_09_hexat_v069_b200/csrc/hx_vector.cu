@@ -2,12 +2,15 @@
 //
 // One CG iteration of the reference (src/Solvers/GPUSolver.jl:452-526) is
 // ~8 broadcast kernels plus 3 cuBLAS dots, each dot a host round trip.  Here
-// it is three kernels and no host round trip:
-//   matvec (hx_operator.cu, mode 2):  q = A p, pq = p.q, alpha = rz/pq
-//   k_cg_update:   x += alpha p; r -= alpha q; z = M^-1 r (not stored);
-//                  rz' = r.z, rr = r.r; convergence / divergence tests;
-//                  beta = rz'/rz
-//   k_cg_pupdate:  p = M^-1 r + beta p
+// it is two kernels and no host round trip:
+//   PCG step (hx_operator.cu):  p = M^-1 r + beta p_old; x += alpha_old p_old;
+//                  q = A p; pq = p.q; alpha = rz/pq
+//   k_cg_update2:  r -= alpha q; z = M^-1 r (not stored); rz' = r.z,
+//                  rr = r.r; convergence / divergence tests; beta = rz'/rz
+// x lags one step behind (x += alpha p happens in the next PCG step); the
+// host applies the last step with k_axpy_state once the loop stops.
+// The three-kernel form (k_cg_update + k_cg_pupdate around a plain matvec)
+// is kept for the Helmholtz filter, whose operator is not fused.
 // All reductions are FP64 and deterministic (fixed-order block partials).
 #include "hx_internal.h"
 
@@ -138,6 +141,51 @@ __global__ void k_cg_update(T* __restrict__ x, const T* __restrict__ p, T* __res
     cg_finish_iteration(st, v[0], v[1]);
 }
 
+// Second half of a fused PCG iteration: r -= alpha q, dots, tests.
+template <typename T>
+__global__ void k_cg_update2(T* __restrict__ r, const T* __restrict__ q,
+                             const T* __restrict__ minv, int64_t n, CgState* st,
+                             double* partials) {
+  if (st->status != HX_RUNNING) return;
+  const T alpha = (T)st->alpha;
+  double rz = 0, rr = 0;
+  using V = typename Vec2<T>::type;
+  const int64_t n2 = n >> 1;
+  V* r2 = reinterpret_cast<V*>(r);
+  const V* q2 = reinterpret_cast<const V*>(q);
+  const V* m2 = reinterpret_cast<const V*>(minv);
+  for (int64_t i = gtid(); i < n2; i += gstride()) {
+    V rv = r2[i];
+    const V qv = q2[i], mv = m2[i];
+    rv.x -= alpha * qv.x;
+    rv.y -= alpha * qv.y;
+    r2[i] = rv;
+    rz += (double)rv.x * (double)(mv.x * rv.x) + (double)rv.y * (double)(mv.y * rv.y);
+    rr += (double)rv.x * (double)rv.x + (double)rv.y * (double)rv.y;
+  }
+  if ((n & 1) && gtid() == 0) {
+    const int64_t i = n - 1;
+    const T ri = r[i] - alpha * q[i];
+    r[i] = ri;
+    rz += (double)ri * (double)(minv[i] * ri);
+    rr += (double)ri * (double)ri;
+  }
+  double v[2] = {rz, rr};
+  if (grid_reduce<2>(v, partials, &st->ticket[TK_UPDATE]) && threadIdx.x == 0)
+    cg_finish_iteration(st, v[0], v[1]);
+}
+
+// dst = x + alpha p, with alpha from the state; `when_snap` restricts it to
+// iterations flagged as the best so far.
+template <typename T>
+__global__ void k_axpy_state(T* __restrict__ dst, const T* __restrict__ x,
+                             const T* __restrict__ p, int64_t n, const CgState* st,
+                             int when_snap) {
+  if (when_snap && !st->snap) return;
+  const T a = (T)st->alpha;
+  for (int64_t i = gtid(); i < n; i += gstride()) dst[i] = x[i] + a * p[i];
+}
+
 template <typename T>
 __global__ void k_cg_pupdate(T* __restrict__ p, const T* __restrict__ r,
                              const T* __restrict__ minv, int64_t n, const CgState* st) {
@@ -259,12 +307,30 @@ void launch_cg_pupdate(cudaStream_t s, T* p, const T* r, const T* minv, int64_t 
   HX_CHECK_LAUNCH();
 }
 
+template <typename T>
+void launch_cg_update2(cudaStream_t s, T* r, const T* q, const T* minv, int64_t n, CgState* st,
+                       double* partials) {
+  k_cg_update2<T><<<vec_blocks(n), VEC_THREADS, 0, s>>>(r, q, minv, n, st, partials);
+  HX_CHECK_LAUNCH();
+}
+
+template <typename T>
+void launch_axpy_state(cudaStream_t s, T* dst, const T* x, const T* p, int64_t n,
+                       const CgState* st, int when_snap) {
+  k_axpy_state<T><<<vec_blocks(n), VEC_THREADS, 0, s>>>(dst, x, p, n, st, when_snap);
+  HX_CHECK_LAUNCH();
+}
+
 #define HX_INST_CG(T)                                                                         \
   template void launch_cg_init<T>(cudaStream_t, const T*, const T*, const T*, T*, T*, int64_t, \
                                   CgState*, double*);                                         \
   template void launch_cg_update<T>(cudaStream_t, T*, const T*, T*, const T*, const T*,       \
                                     int64_t, CgState*, double*);                              \
-  template void launch_cg_pupdate<T>(cudaStream_t, T*, const T*, const T*, int64_t, CgState*);
+  template void launch_cg_pupdate<T>(cudaStream_t, T*, const T*, const T*, int64_t, CgState*); \
+  template void launch_cg_update2<T>(cudaStream_t, T*, const T*, const T*, int64_t, CgState*,  \
+                                     double*);                                                 \
+  template void launch_axpy_state<T>(cudaStream_t, T*, const T*, const T*, int64_t,            \
+                                     const CgState*, int);
 HX_INST_CG(double)
 HX_INST_CG(float)
 

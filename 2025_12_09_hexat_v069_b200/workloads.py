@@ -36,8 +36,18 @@ def simp(rho, p=3.0, e0=1.0, emin=1e-9):
     return emin + np.power(rho, p) * (e0 - emin)
 
 
-def cantilever(nx, ny, nz, load=1.0):
-    nodes, elements, dims = mesh.generate_mesh(nx, ny, nz)
+def lattice_nodes(nx, ny, nz):
+    """Node coordinates of generate_mesh (unit spacing) without the elements."""
+    k, j, i = np.meshgrid(np.arange(nz + 1, dtype=np.float32), np.arange(ny + 1, dtype=np.float32),
+                          np.arange(nx + 1, dtype=np.float32), indexing="ij")
+    return np.stack([i.ravel(), j.ravel(), k.ravel()], axis=1)
+
+
+def cantilever(nx, ny, nz, load=1.0, with_elements=True):
+    if with_elements:
+        nodes, elements, dims = mesh.generate_mesh(nx, ny, nz)
+    else:
+        nodes, elements = lattice_nodes(nx, ny, nz), None
     bc = boundary.get_bc_indicator(nodes.shape[0], nodes,
                                    [{"location": [0, ":", ":"], "DoFs": [1, 2, 3]}])
     f = np.zeros(3 * nodes.shape[0], np.float64)
@@ -51,8 +61,11 @@ def cantilever(nx, ny, nz, load=1.0):
     return nodes, elements, bc, f
 
 
-def mbb_half_beam(nx, ny, nz, load=1.0):
-    nodes, elements, dims = mesh.generate_mesh(nx, ny, nz)
+def mbb_half_beam(nx, ny, nz, load=1.0, with_elements=True):
+    if with_elements:
+        nodes, elements, dims = mesh.generate_mesh(nx, ny, nz)
+    else:
+        nodes, elements = lattice_nodes(nx, ny, nz), None
     n = nodes.shape[0]
     bc = np.zeros((n, 3), np.float32)
     bc[np.abs(nodes[:, 0]) < 1e-4, 0] = 1.0

@@ -1,0 +1,339 @@
+#!/usr/bin/env python
+"""Benchmark of the HEXA(T) inner solve on B200: seconds per FP64 Jacobi-PCG
+solve to rtol 1e-6 (FP64 true residual) on the 320x160x160 cantilever
+(8,192,000 Hex8 elements, 24,961,923 DOFs), synthetic seeded density.
+
+One step = one full solve from u0 = 0.  `value` is device time (CUDA events on
+the library's stream) per solve with inputs resident in HBM; `e2e` is the same
+solve through the C ABI with pinned host buffers (copies in the timed region).
+Under torchrun each rank runs an independent replica (weak scaling; the
+reference path is single-GPU and has no exchange step).
+
+--impl reference times the reference's CPU algorithm (the C/OpenMP
+restatement of its matrix-free CG, no GPU) on the host cores.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "s per solve to rtol 1e-6 at 8.2M Hex8, learned+mixed vs plain FP64; HBM GB/s"
+DIMS = (320, 160, 160)
+SEED = 20251209
+PEAKS = {"hbm_gbs": 6545.9, "source": "fallback"}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def dist_info():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Clocks:
+    """nvidia-smi sampler for the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.tmp, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        self.tmp.flush()
+        self.tmp.seek(0)
+        rows = [r.split(",") for r in self.tmp.read().strip().splitlines() if r.strip()]
+        os.unlink(self.tmp.name)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+                for n, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def c1_inputs(hx, ctx, dims=DIMS):
+    """C1 workload: cantilever 320x160x160; density = Helmholtz-smoothed (r=3,
+    geometric element) splitmix64 field mapped to [1e-3, 1]; SIMP p=3.
+    Other dims give the same construction at another size (profiling only)."""
+    W = hx.workloads
+    nx, ny, nz = dims
+    nodes, _, bc, f = W.cantilever(nx, ny, nz, with_elements=False)
+    ctx.set_grid(nx, ny, nz)
+    ctx.set_material(1.0, 0.3)
+    ctx.set_bc(bc)
+    raw = W.raw_density(nx * ny * nz, SEED)
+    rho_f, frep = ctx.filter(raw, 3.0, ref_compat=0, tol=1e-5, max_iter=200)
+    rho = W.map_density(rho_f, 1e-3)
+    fac = W.simp(rho, 3.0, 1.0, 1e-9)
+    return f, fac, frep
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    ws, rank, local = dist_info()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=900),
+                                device_id=torch.device("cuda", local))
+    import importlib
+    hx = importlib.import_module("2025_12_09_hexat_v069_b200")
+    L = importlib.import_module("2025_12_09_hexat_v069_b200._lib")
+    ctx = hx.Context(local)
+    f, fac, frep = c1_inputs(hx, ctx, tuple(args.dims))
+    n, ne = f.shape[0], fac.shape[0]
+    dev = torch.device("cuda", local)
+    f_d = torch.from_numpy(f).to(dev)
+    fac_d = torch.from_numpy(fac).to(dev)
+    u_d = torch.zeros(n, dtype=torch.float64, device=dev)
+    opts = hx.default_opts(tol=1e-6, max_iter=100000, precision=args.precision)
+    lib_stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+
+    def barrier():
+        if ws > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if ws == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        rep = ctx.solve_device(f_d.data_ptr(), fac_d.data_ptr(), u_d.data_ptr(), opts=opts)
+    # ---- timed region: device-resident inputs ----
+    clocks = Clocks(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(lib_stream)
+    reps, launches = [], 0
+    for _ in range(args.steps):
+        rep = ctx.solve_device(f_d.data_ptr(), fac_d.data_ptr(), u_d.data_ptr(), opts=opts)
+        reps.append(rep)
+        launches += int(rep.kernel_launches)
+    e1.record(lib_stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    barrier()
+    t_dev = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    iters = reps[-1].iterations
+    true_rel = reps[-1].true_rel_res
+    # ---- e2e: host (pinned) buffers through the C ABI ----
+    f_h = torch.from_numpy(f).pin_memory()
+    fac_h = torch.from_numpy(fac).pin_memory()
+    u_h = torch.zeros(n, dtype=torch.float64).pin_memory()
+    f_np, fac_np, u_np = f_h.numpy(), fac_h.numpy(), u_h.numpy()
+    e_steps = max(1, min(args.steps, 3))
+    barrier()
+    torch.cuda.synchronize()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(lib_stream)
+    for _ in range(e_steps):
+        st = ctx.lib.hx_solve(ctx.h, L.HX_F64, L._ptr(f_np), L._ptr(fac_np), L._ptr(u_np),
+                              L.C.byref(opts), L.C.byref(L.SolveReport()))
+        ctx.check(st, "hx_solve")
+    e3.record(lib_stream)
+    e3.synchronize()
+    barrier()
+    t_e2e = max_over_ranks(e2.elapsed_time(e3) / 1e3)
+    # ---- live per-kernel timing for the roofline ----
+    t_st = ctx.time_kernel(L.HX_KERNEL_PCG_STEP_FP64, 20)
+    t_up = ctx.time_kernel(L.HX_KERNEL_PCG_UPDATE_FP64, 20)
+    t_ap = ctx.time_kernel(L.HX_KERNEL_APPLY_FP64, 20)
+    peaks = load_peaks()
+    nn = n // 3
+    # algorithmic bytes per launch (8-byte words; mask 1 byte per node):
+    # PCG step reads p_old, r, M^-1, x, factor, mask; writes p, q, x
+    b_st = 7 * 8 * n + 8 * ne + nn
+    b_up = 4 * 8 * n          # r, q, M^-1 read; r written
+    b_ap = 2 * 8 * n + 8 * ne + nn   # plain K.x: x read, y written, factor, mask
+    kern = {
+        "pcg_step_fp64": {"ms": t_st, "bytes": b_st, "gbs": b_st / t_st / 1e6},
+        "pcg_update_fp64": {"ms": t_up, "bytes": b_up, "gbs": b_up / t_up / 1e6},
+        "apply_fp64": {"ms": t_ap, "bytes": b_ap, "gbs": b_ap / t_ap / 1e6},
+    }
+    dom = max(("pcg_step_fp64", "pcg_update_fp64"), key=lambda k: kern[k]["ms"])
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as fh:
+            traffic = json.load(fh).get(dom)
+    it_ms = t_dev / args.steps / max(iters, 1) * 1e3
+    b_it = b_st + b_up
+    out = {
+        "metric": METRIC, "value": t_dev / (args.steps * ws), "unit": "s/solve",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_dev / args.steps * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if args.precision == 0 else "f32-in-f64-refinement",
+        "data": "synthetic: splitmix64(seed 20251209) density, Helmholtz r=3 smoothed, "
+                "mapped to [1e-3,1], SIMP p=3 (contrast 1e9)",
+        "config": {"workload": "C1 cantilever 320x160x160 Hex8 (8,192,000 elements, "
+                               "24,961,923 DOFs), Jacobi-PCG to rtol 1e-6 from u0=0, shift 0",
+                   "elements": ne, "dofs": n, "cg_iterations": iters,
+                   "true_rel_res": true_rel, "precision": ["fp64", "mixed32"][args.precision],
+                   "l2": "working set 1.4 GB >> 126 MB L2 (no flush needed)",
+                   "parallelism": f"replicas x{ws}"},
+        "e2e": {"value": t_e2e / (e_steps * ws), "unit": "s/solve",
+                "h2d_bytes_per_step": 8 * n + 8 * ne, "d2h_bytes_per_step": 8 * n,
+                "steps": e_steps},
+        "gpu_launches": launches,
+        "clocks": clk,
+        "roofline": {"bound": "hbm", "kernel": dom,
+                     "achieved": kern[dom]["gbs"], "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": kern[dom]["gbs"] / peaks["hbm_gbs"], "traffic": traffic,
+                     "peak_source": peaks["source"]},
+        "kernels": {k: v for k, v in kern.items() if k != "apply_fp64"},
+        "apply_fp64": kern["apply_fp64"],
+        "pcg_iteration": {"ms": it_ms, "bytes": b_it, "gbs": b_it / it_ms / 1e6,
+                          "frac": b_it / it_ms / 1e6 / peaks["hbm_gbs"]},
+        "filter_setup": {"iterations": frep.iterations, "rel_res": frep.rel_res},
+    }
+    if tuple(args.dims) != DIMS:
+        out["config"]["workload"] = f"profiling case {tuple(args.dims)} (not the C1 workload)"
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline and tuple(args.dims) == DIMS:
+        out["cpu_baseline"] = cpu_baseline(hx, iters, args.cpu_iters)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    ctx.close()
+    if ws > 1:
+        dist.destroy_process_group()
+
+
+def _cpu_threads():
+    n = os.cpu_count() or 1
+    try:
+        import psutil
+        avail = psutil.virtual_memory().available
+        n = min(n, max(1, int(avail * 0.5 // (3 * 8 * 8_400_000))))
+    except Exception:
+        pass
+    return max(1, min(n, 64))
+
+
+def cpu_baseline(hx, gpu_iters, sample_iters):
+    """Reference CPU algorithm (matrix-free CG with per-thread accumulators,
+    restated in C/OpenMP) on a bounded sample of C1: per-iteration time from
+    two runs (1 and 1+k iterations), extrapolated to the solve's iteration
+    count."""
+    from oracle import oracle
+    W = hx.workloads
+    nx, ny, nz = DIMS
+    nodes, el, bc, f = W.cantilever(nx, ny, nz)
+    c0 = hx.mesh.connectivity0(el)
+    del el
+    rho = W.map_density(W.raw_density(c0.shape[0], SEED), 1e-3)
+    fac = W.simp(rho)
+    ke = oracle.canonical_ke()
+    nn = nodes.shape[0]
+    free = (~(bc > 0).reshape(-1)).astype(np.uint8)
+    th = _cpu_threads()
+    t = []
+    for k in (1, 1 + sample_iters):
+        t0 = time.perf_counter()
+        oracle.cg_solve(c0, nn, ke, fac, free, f * free, max_iter=k, tol=1e-30, nthreads=th)
+        t.append(time.perf_counter() - t0)
+    per_it = (t[1] - t[0]) / sample_iters
+    return {"value": per_it * gpu_iters, "unit": "s/solve", "cores": th, "kind": "port",
+            "sample": f"{sample_iters} CG iterations of the C1 system (unsmoothed density of "
+                      f"the same shape; cost is data-independent), {per_it:.3f} s/iteration x "
+                      f"{gpu_iters} iterations of the FP64 solve"}
+
+
+def run_reference(args):
+    ws, rank, local = dist_info()
+    if rank != 0:
+        return
+    import importlib
+    hx = importlib.import_module("2025_12_09_hexat_v069_b200")
+    iters = None
+    p = os.path.join(ROOT, "profiles", "c1_solve.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            iters = json.load(fh).get("cg_iterations")
+    iters = iters or 5000
+    vals = []
+    for _ in range(args.warmup + args.steps):
+        cb = cpu_baseline(hx, iters, args.cpu_iters)
+        vals.append(cb["value"])
+    v = float(np.mean(vals[args.warmup:]))
+    cb["value"] = v
+    out = {"metric": METRIC, "value": v, "unit": "s/solve", "impl": "reference", "n_gpus": ws,
+           "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": "C1 cantilever 320x160x160 Hex8, Jacobi-CG to rtol 1e-6, "
+                                  "reference CPU algorithm on host cores",
+                      "cg_iterations_extrapolated": iters},
+           "cpu_baseline": cb,
+           "e2e": {"value": v, "unit": "s/solve", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", type=int, default=0, help="0 fp64, 1 mixed32")
+    ap.add_argument("--cpu-iters", type=int, default=6)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--dims", type=int, nargs=3, default=list(DIMS),
+                    help="grid size; other than 320 160 160 only for profiling")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -247,10 +247,10 @@ HX_API hx_status hx_oc_update(hx_ctx *ctx, int32_t dtype, const void *x,
  * hx_solve_device (kernel ids below); inputs are left unchanged except the
  * kernels' scratch outputs.  Used by the benchmark for the live roofline. */
 enum {
-  HX_KERNEL_MATVEC_FP64 = 0, /* CG-mode K.p with the fused p.q reduction */
-  HX_KERNEL_UPDATE_FP64 = 1, /* x,r update + r.z, r.r reductions */
-  HX_KERNEL_PUPDATE_FP64 = 2,
-  HX_KERNEL_MATVEC_FP32 = 3,
+  HX_KERNEL_PCG_STEP_FP64 = 0,   /* fused p/x update + K.p + p.q reduction */
+  HX_KERNEL_PCG_UPDATE_FP64 = 1, /* r update + r.z, r.r reductions */
+  HX_KERNEL_APPLY_FP64 = 2,      /* plain K.x */
+  HX_KERNEL_PCG_STEP_FP32 = 3,
   HX_KERNEL_FILTER_MATVEC = 4
 };
 HX_API hx_status hx_time_kernel(hx_ctx *ctx, int32_t kernel, int32_t reps,
