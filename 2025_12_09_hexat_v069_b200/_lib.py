@@ -65,6 +65,8 @@ PROTOTYPES = {
     "hx_get_grid": (_i32, [_vp, _vp, _vp]),
     "hx_apply_stiffness": (_i32, [_vp, _i32, _vp, _vp, _vp]),
     "hx_diagonal": (_i32, [_vp, _i32, _vp, _vp]),
+    "hx_apply_stiffness_noalloc": (_i32, [_i64, _i64, _i64, _dbl, _dbl, _dbl, _dbl, _vp, _vp, _vp,
+                                          _vp, _vp]),
     "hx_solve": (_i32, [_vp, _i32, _vp, _vp, _vp, C.POINTER(SolveOpts), C.POINTER(SolveReport)]),
     "hx_solve_device": (_i32, [_vp, _vp, _vp, _vp, C.POINTER(SolveOpts), C.POINTER(SolveReport)]),
     "hx_solve_system_gpu": (_i32, [_vp, _f32p, _i64, _i64p, _i64, C.c_float, C.c_float, _f32p,

@@ -141,6 +141,31 @@ HX_API hx_status hx_get_grid(const hx_ctx *ctx, int64_t dims[3], double h[3]);
  * caller's numbering. */
 HX_API hx_status hx_apply_stiffness(hx_ctx *ctx, int32_t dtype, const void *x,
                                     const void *factor, void *y);
+/* Allocation-free K(f)x -- no counterpart in the reference.
+ * Some callers cannot let a library allocate device memory: cudaMalloc and
+ * cudaFree synchronize the device (stalling every other stream of a caller
+ * that keeps work in flight), and a host runtime that pools device memory
+ * itself (CUDA.jl in the reference's Julia host) may hold most of the
+ * device, so a foreign allocation fails.  This entry point computes
+ * y = K(f)x on the structured nx*ny*nz grid (no boundary conditions, no
+ * shift, as hx_apply_stiffness) and *xKx = x.y (FP64, deterministic), all
+ * arrays FP64 DEVICE pointers in grid numbering, on `stream` (a
+ * cudaStream_t; NULL = default stream).  It allocates nothing: its scratch
+ * (one partial sum per CTA plus a completion counter) lives in a static
+ * device array of 256 + 8*HX_NOALLOC_MAX_BLOCKS bytes that every GPU
+ * loading the library holds until exit.  Grids needing more than
+ * HX_NOALLOC_MAX_BLOCKS CTAs (beyond about 1880 x 1880 nodes per plane)
+ * are rejected with HX_BAD_ARG.  The first call on a device resolves the
+ * array's device address (cudaGetSymbolAddress) with that device current;
+ * make that first call before any stream capture.  All calls on a device
+ * share the array: calls that overlap on the GPU race, so order them
+ * (e.g. on one stream).  Returns without waiting for the GPU. */
+#define HX_NOALLOC_MAX_BLOCKS 16384
+HX_API hx_status hx_apply_stiffness_noalloc(int64_t nx, int64_t ny, int64_t nz,
+                                            double dx, double dy, double dz,
+                                            double nu, const double *x,
+                                            const double *factor, double *y,
+                                            double *xKx, void *stream);
 /* Jacobi diagonal, src/Solvers/CPUSolver.jl:109-148. */
 HX_API hx_status hx_diagonal(hx_ctx *ctx, int32_t dtype, const void *factor,
                              void *diag);
