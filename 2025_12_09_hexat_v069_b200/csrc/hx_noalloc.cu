@@ -68,6 +68,8 @@ extern "C" HX_API hx_status hx_apply_stiffness_noalloc(int64_t nx, int64_t ny, i
                                                        const double* x, const double* factor,
                                                        double* y, double* xKx, void* stream) {
   if (!x || !factor || !y || !xKx) return HX_BAD_ARG;
+  // the operator stages x with 8-byte copies
+  if ((reinterpret_cast<uintptr_t>(x) & 7u) != 0) return HX_BAD_ARG;
   if (nx < 1 || ny < 1 || nz < 1 || nx >= (1 << 20) || ny >= (1 << 20) || nz >= (1 << 20))
     return HX_BAD_ARG;
   if (!(dx > 0 && dy > 0 && dz > 0) || !(nu > -1.0 && nu < 0.5)) return HX_BAD_ARG;

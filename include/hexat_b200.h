@@ -149,7 +149,7 @@ HX_API hx_status hx_apply_stiffness(hx_ctx *ctx, int32_t dtype, const void *x,
  * device, so a foreign allocation fails.  This entry point computes
  * y = K(f)x on the structured nx*ny*nz grid (no boundary conditions, no
  * shift, as hx_apply_stiffness) and *xKx = x.y (FP64, deterministic), all
- * arrays FP64 DEVICE pointers in grid numbering, on `stream` (a
+ * arrays FP64 DEVICE pointers in grid numbering (8-byte aligned), on `stream` (a
  * cudaStream_t; NULL = default stream).  It allocates nothing: its scratch
  * (one partial sum per CTA plus a completion counter) lives in a static
  * device array of 256 + 8*HX_NOALLOC_MAX_BLOCKS bytes that every GPU
