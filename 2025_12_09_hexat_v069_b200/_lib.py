@@ -81,6 +81,14 @@ PROTOTYPES = {
     "hx_compute_stress_field": (_i32, [_vp, _f32p, _i64, _i64p, _i64, _f32p, C.c_float,
                                        C.c_float, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p]),
     "hx_compliance": (_i32, [_vp, _i32, _vp, _vp, C.POINTER(_dbl)]),
+    "hx_net_init": (_i32, [_vp, C.c_uint64]),
+    "hx_net_set_params": (_i32, [_vp, _vp]),
+    "hx_net_get_params": (_i32, [_vp, _vp]),
+    "hx_net_forward_backward": (_i32, [_vp, _i32, _i32, _i32, _vp, _vp, _vp, _vp]),
+    "hx_net_prepare": (_i32, [_vp, _vp]),
+    "hx_net_train_step": (_i32, [_vp, _vp, _vp, _dbl, C.POINTER(_dbl)]),
+    "hx_pcg_snapshots": (_i32, [_vp, _vp, _vp, _i32, _i32, _dbl, _vp, C.POINTER(_i32)]),
+    "hx_residual_device": (_i32, [_vp, _vp, _vp, _vp, _vp]),
     "hx_element_energy": (_i32, [_vp, _i32, _vp, _vp]),
     "hx_oc_update": (_i32, [_vp, _i32, _vp, _vp, _vp, _dbl, _dbl, _vp, C.POINTER(_dbl),
                             C.POINTER(_i32)]),
@@ -259,6 +267,53 @@ class Context:
         self.check(self.lib.hx_time_kernel(self.h, int(kernel), int(reps), C.byref(ms)),
                    "hx_time_kernel")
         return ms.value
+
+    # ---- learned preconditioner ----
+    NET_PARAMS = 4 * (27 * 256 + 16)
+
+    def net_init(self, seed=1):
+        self.check(self.lib.hx_net_init(self.h, int(seed)), "hx_net_init")
+
+    def net_set_params(self, params):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        assert p.size == self.NET_PARAMS
+        self.check(self.lib.hx_net_set_params(self.h, _ptr(p)), "hx_net_set_params")
+
+    def net_get_params(self):
+        p = np.empty(self.NET_PARAMS, np.float32)
+        self.check(self.lib.hx_net_get_params(self.h, _ptr(p)), "hx_net_get_params")
+        return p
+
+    def net_forward_backward(self, dims, x0, dy):
+        x0 = np.ascontiguousarray(x0, dtype=np.float32)
+        dy = np.ascontiguousarray(dy, dtype=np.float32)
+        y = np.empty_like(x0)
+        g = np.empty(self.NET_PARAMS, np.float32)
+        self.check(self.lib.hx_net_forward_backward(self.h, *dims, _ptr(x0), _ptr(dy), _ptr(y),
+                                                    _ptr(g)), "hx_net_forward_backward")
+        return y, g
+
+    def net_prepare(self, fac_ptr):
+        self.check(self.lib.hx_net_prepare(self.h, C.c_void_p(fac_ptr)), "hx_net_prepare")
+
+    def net_train_step(self, r_ptr, e_ptr, lr):
+        loss = C.c_double()
+        self.check(self.lib.hx_net_train_step(self.h, C.c_void_p(r_ptr), C.c_void_p(e_ptr),
+                                              float(lr), C.byref(loss)), "hx_net_train_step")
+        return loss.value
+
+    def pcg_snapshots(self, f_ptr, fac_ptr, every, count, tol, snaps_ptr):
+        taken = C.c_int32()
+        self.check(self.lib.hx_pcg_snapshots(self.h, C.c_void_p(f_ptr), C.c_void_p(fac_ptr),
+                                             int(every), int(count), float(tol),
+                                             C.c_void_p(snaps_ptr), C.byref(taken)),
+                   "hx_pcg_snapshots")
+        return taken.value
+
+    def residual_device(self, f_ptr, fac_ptr, x_ptr, r_ptr):
+        self.check(self.lib.hx_residual_device(self.h, C.c_void_p(f_ptr), C.c_void_p(fac_ptr),
+                                               C.c_void_p(x_ptr), C.c_void_p(r_ptr)),
+                   "hx_residual_device")
 
     # ---- filter ----
     def filter(self, rho, radius, ref_compat=0, tol=1e-5, max_iter=200):

@@ -1,0 +1,525 @@
+// hx_cnn.cu -- 3D convolutional preconditioner network on the node grid:
+// BF16 implicit-GEMM conv3d (3x3x3, 16 input channels) on the tensor cores
+// with FP32 accumulation, its backward (data and weights), Adam, and the
+// input/output assembly around a Krylov solver.
+//
+// Activations are channels-last BF16, [node][16] (32 bytes per node, node
+// numbering of the grid).  A conv layer is a GEMM per CTA tile: M = 512
+// nodes (16 x 8 x 4), N = output channels, K = 27 taps x 16 channels; each
+// warp owns four 16-node x-rows and issues one m16n8k16 MMA per (row, tap,
+// 8 output channels).  The input tile with its one-node halo (18 x 10 x 6
+// nodes) and the layer's weights are staged with 16-byte cp.async; the A
+// fragment of a shifted tap is loaded with ldmatrix from the shifted rows,
+// the 16-byte halves of each node are XOR-swizzled so the 8 rows of a
+// matrix hit distinct banks.  The backward-data pass is the same kernel with
+// the taps flipped and each tap's weights transposed; the weight gradient
+// is a per-CTA tensor-core reduction over the tile's nodes (one tap per
+// warp at a time) summed across CTAs in a fixed order.
+#include <cuda_bf16.h>
+
+#include "hx_cnn.h"
+
+namespace hx {
+
+namespace {
+
+constexpr int TX = 16, TY = 8, TZ = 4;           // output tile
+constexpr int HX_ = TX + 2, HY = TY + 2, HZ = TZ + 2;
+constexpr int HNODES = HX_ * HY * HZ;             // 1080
+constexpr int C = 16;                             // channels per node (storage)
+constexpr int NTHREADS = 256;
+
+__device__ __forceinline__ unsigned su32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void cp16(unsigned dst, const void* src, bool ok) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src),
+               "r"(ok ? 16 : 0));
+}
+__device__ __forceinline__ void cp_commit_wait() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::);
+}
+__device__ __forceinline__ void ldsm_x4(unsigned addr, unsigned (&r)[4]) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(addr));
+}
+__device__ __forceinline__ void ldsm_x4_t(unsigned addr, unsigned (&r)[4]) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(addr));
+}
+__device__ __forceinline__ void ldsm_x2(unsigned addr, unsigned (&r)[2]) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x2.shared.b16 {%0,%1}, [%2];\n"
+               : "=r"(r[0]), "=r"(r[1])
+               : "r"(addr));
+}
+__device__ __forceinline__ void mma16816(float (&d)[4], const unsigned (&a)[4], unsigned b0,
+                                         unsigned b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// byte offset of 16-byte half `h` of a 32-byte row `row` (XOR swizzle)
+__device__ __forceinline__ unsigned swz(int row, int h) {
+  return (unsigned)(row * 32 + ((h ^ ((row >> 2) & 1)) << 4));
+}
+
+struct ConvSmem {
+  __nv_bfloat16 x[HNODES * C];  // 34,560 B
+  __nv_bfloat16 w[27 * 16 * C]; // 13,824 B, per tap [co][ci]
+};
+
+// Stage the input tile (with halo) and the layer weights.
+__device__ __forceinline__ void stage_tile(ConvSmem& sm, const __nv_bfloat16* __restrict__ X,
+                                           const __nv_bfloat16* __restrict__ W, int cout,
+                                           const GridN& g, int x0, int y0, int z0) {
+  const unsigned xb = su32(sm.x), wb = su32(sm.w);
+  for (int ch = threadIdx.x; ch < HNODES * 2; ch += NTHREADS) {
+    const int node = ch >> 1, h = ch & 1;
+    const int hx = node % HX_, r = node / HX_;
+    const int hy = r % HY, hz = r / HY;
+    const int gx = x0 - 1 + hx, gy = y0 - 1 + hy, gz = z0 - 1 + hz;
+    const bool ok = gx >= 0 && gy >= 0 && gz >= 0 && gx < g.nx && gy < g.ny && gz < g.nz;
+    const int64_t gn = ok ? ((int64_t)gz * g.ny + gy) * g.nx + gx : 0;
+    cp16(xb + swz(node, h), X + gn * C + h * 8, ok);
+  }
+  for (int ch = threadIdx.x; ch < 27 * cout * 2; ch += NTHREADS) {
+    const int row = ch >> 1, h = ch & 1;  // row = tap * cout + co
+    const int tap = row / cout, co = row - tap * cout;
+    cp16(wb + swz(tap * 16 + co, h), W + ((int64_t)tap * 16 + co) * C + h * 8, true);
+  }
+  cp_commit_wait();
+  __syncthreads();
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Forward / backward-data convolution.
+// Y[n, co] = EPI( sum_{tap, ci} X[n + off(tap), ci] * W[tap][co][ci] )
+// EPI 0: + bias, ReLU;  1: + bias;  2: * (M[n, co] > 0)  (ReLU derivative)
+// COUT: 16 or 8 output channels (stored with stride COUT).
+// ---------------------------------------------------------------------------
+template <int COUT, int EPI>
+__global__ void __launch_bounds__(NTHREADS) k_conv3(const __nv_bfloat16* __restrict__ X,
+                                                    __nv_bfloat16* __restrict__ Y,
+                                                    const __nv_bfloat16* __restrict__ W,
+                                                    const float* __restrict__ bias,
+                                                    const __nv_bfloat16* __restrict__ M,
+                                                    GridN g) {
+  constexpr int NT = COUT / 8;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  ConvSmem& sm = *reinterpret_cast<ConvSmem*>(smraw);
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = blockIdx.z * TZ;
+  stage_tile(sm, X, W, COUT, g, x0, y0, z0);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned xb = su32(sm.x), wb = su32(sm.w);
+  float acc[4][NT][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) acc[i][nt][k] = 0.f;
+  // A rows this lane addresses: node x = (mi&1)*8 + lane%8, half = mi>>1
+  const int mi = lane >> 3;
+  const int ax = ((mi & 1) << 3) + (lane & 7), ah = mi >> 1;
+  for (int tap = 0; tap < 27; ++tap) {
+    const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+    unsigned b[4];
+    if (COUT == 16) {
+      const int co = ((mi >> 1) << 3) + (lane & 7), h = mi & 1;
+      ldsm_x4(wb + swz(tap * 16 + co, h), b);
+    } else {
+      unsigned b2[2];
+      const int co = lane & 7, h = (lane >> 3) & 1;
+      ldsm_x2(wb + swz(tap * 16 + co, h), b2);
+      b[0] = b2[0];
+      b[1] = b2[1];
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int row = warp * 4 + i;  // 32 x-rows: y = row % 8, z = row / 8
+      const int hy = (row & 7) + 1 + dy, hz = (row >> 3) + 1 + dz;
+      const int hx = ax + 1 + dx;
+      unsigned a[4];
+      ldsm_x4(xb + swz((hz * HY + hy) * HX_ + hx, ah), a);
+      mma16816(acc[i][0], a, b[0], b[1]);
+      if (NT == 2) mma16816(acc[i][NT - 1], a, b[2], b[3]);
+    }
+  }
+  // epilogue: lane holds nodes x = lane/4 and lane/4 + 8, channels 2t, 2t+1
+  const int gq = lane >> 2, tq = lane & 3;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int row = warp * 4 + i;
+    const int gy = y0 + (row & 7), gz = z0 + (row >> 3);
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+      const int gx = x0 + gq + half * 8;
+      if (gx >= g.nx || gy >= g.ny || gz >= g.nz) continue;
+      const int64_t node = ((int64_t)gz * g.ny + gy) * g.nx + gx;
+#pragma unroll
+      for (int nt = 0; nt < NT; ++nt) {
+        const int co = nt * 8 + 2 * tq;
+        float v0 = acc[i][nt][2 * half], v1 = acc[i][nt][2 * half + 1];
+        if (EPI <= 1) {
+          v0 += bias[co];
+          v1 += bias[co + 1];
+          if (EPI == 0) {
+            v0 = fmaxf(v0, 0.f);
+            v1 = fmaxf(v1, 0.f);
+          }
+        } else {
+          const __nv_bfloat162 mm =
+              *reinterpret_cast<const __nv_bfloat162*>(M + node * COUT + co);
+          v0 = __bfloat162float(mm.x) > 0.f ? v0 : 0.f;
+          v1 = __bfloat162float(mm.y) > 0.f ? v1 : 0.f;
+        }
+        *reinterpret_cast<__nv_bfloat162*>(Y + node * COUT + co) = __floats2bfloat162_rn(v0, v1);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Weight/bias gradient partials of one CTA tile:
+// dW[tap][co][ci] = sum_n D[n, co] X[n + off(tap), ci],  db[co] = sum_n D[n, co]
+// D = gradient w.r.t. the pre-activation (16 channels, node-major).  Warp w
+// handles taps w, w+8, w+16, w+24 over all 512 nodes of the tile; the
+// result goes to part[cta][27*256 + 16] (FP32), summed later in fixed order.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(NTHREADS) k_conv3_wgrad(const __nv_bfloat16* __restrict__ X,
+                                                          const __nv_bfloat16* __restrict__ D,
+                                                          float* __restrict__ part, GridN g) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  __nv_bfloat16* xs = reinterpret_cast<__nv_bfloat16*>(smraw);
+  __nv_bfloat16* ds = xs + HNODES * C;  // [512 nodes][16], swizzled rows
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = blockIdx.z * TZ;
+  const unsigned xb = su32(xs), db = su32(ds);
+  for (int ch = threadIdx.x; ch < HNODES * 2; ch += NTHREADS) {
+    const int node = ch >> 1, h = ch & 1;
+    const int hx = node % HX_, r = node / HX_;
+    const int hy = r % HY, hz = r / HY;
+    const int gx = x0 - 1 + hx, gy = y0 - 1 + hy, gz = z0 - 1 + hz;
+    const bool ok = gx >= 0 && gy >= 0 && gz >= 0 && gx < g.nx && gy < g.ny && gz < g.nz;
+    const int64_t gn = ok ? ((int64_t)gz * g.ny + gy) * g.nx + gx : 0;
+    cp16(xb + swz(node, h), X + gn * C + h * 8, ok);
+  }
+  for (int ch = threadIdx.x; ch < TX * TY * TZ * 2; ch += NTHREADS) {
+    const int node = ch >> 1, h = ch & 1;  // node = x + 16 (y + 8 z)
+    const int tx = node & 15, ty = (node >> 4) & 7, tz = node >> 7;
+    const int gx = x0 + tx, gy = y0 + ty, gz = z0 + tz;
+    const bool ok = gx < g.nx && gy < g.ny && gz < g.nz;  // outside: zero gradient
+    const int64_t gn = ok ? ((int64_t)gz * g.ny + gy) * g.nx + gx : 0;
+    cp16(db + swz(node, h), D + gn * C + h * 8, ok);
+  }
+  cp_commit_wait();
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gq = lane >> 2, tq = lane & 3;
+  float* out = part + (size_t)(blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)) *
+                          (27 * 256 + 16);
+  // ldmatrix.trans row addresses: matrix mi = lane/8, row r = lane%8
+  const int mi = lane >> 3, rr = lane & 7;
+  for (int tap = warp; tap < 27; tap += 8) {
+    const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+    float acc[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};  // M = ci, N = co
+    for (int row = 0; row < 32; ++row) {  // 16-node k-steps
+      const int ty = row & 7, tz = row >> 3;
+      // A = X^T (ci x nodes): matrices (ci 0-7, n 0-7), (ci 8-15, n 0-7),
+      // (ci 0-7, n 8-15), (ci 8-15, n 8-15) from X[n][ci] via .trans
+      unsigned a[4];
+      {
+        const int nx_ = ((mi >> 1) << 3) + rr, h = mi & 1;
+        const int hx = nx_ + 1 + dx, hy = ty + 1 + dy, hz = tz + 1 + dz;
+        ldsm_x4_t(xb + swz((hz * HY + hy) * HX_ + hx, h), a);
+      }
+      // B = D (nodes x co): matrices (n 0-7, co 0-7), (n 8-15, co 0-7),
+      // (n 0-7, co 8-15), (n 8-15, co 8-15) via .trans
+      unsigned b[4];
+      {
+        const int nx_ = ((mi & 1) << 3) + rr, h = mi >> 1;
+        ldsm_x4_t(db + swz(nx_ + 16 * (ty + 8 * tz), h), b);
+      }
+      mma16816(acc[0], a, b[0], b[1]);
+      mma16816(acc[1], a, b[2], b[3]);
+    }
+    // acc[nt]: rows ci = gq (+8), cols co = nt*8 + 2tq (+1)
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+      for (int hh = 0; hh < 2; ++hh) {
+        const int ci = gq + hh * 8, co = nt * 8 + 2 * tq;
+        out[tap * 256 + co * 16 + ci] = acc[nt][2 * hh];
+        out[tap * 256 + (co + 1) * 16 + ci] = acc[nt][2 * hh + 1];
+      }
+  }
+  // bias gradient: 16 sums over the tile's nodes (fixed order)
+  if (threadIdx.x < 16) {
+    float s = 0.f;
+    for (int node = 0; node < TX * TY * TZ; ++node) {
+      const unsigned off = swz(node, threadIdx.x >> 3) + (threadIdx.x & 7) * 2;
+      s += __bfloat162float(*reinterpret_cast<const __nv_bfloat16*>(
+          reinterpret_cast<const unsigned char*>(ds) + off));
+    }
+    out[27 * 256 + threadIdx.x] = s;
+  }
+}
+
+// Sum the per-CTA partials in a fixed order: grad[k] = sum_c part[c][k].
+__global__ void k_reduce_parts(const float* __restrict__ part, int nparts, int len,
+                               float* __restrict__ grad) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= len) return;
+  double s = 0.0;
+  for (int c = 0; c < nparts; ++c) s += (double)part[(size_t)c * len + k];
+  grad[k] = (float)s;
+}
+
+// Adam step on FP32 master parameters (weights [27][16][16] then bias[16]
+// per layer, concatenated); writes the BF16 forward weights and their
+// flipped-transposed copy for the backward-data pass.  `live` masks the
+// parameters that exist (padding channels stay zero).
+__global__ void k_adam(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v,
+                       const float* __restrict__ grad, const unsigned char* __restrict__ live,
+                       int n, float lr, float b1, float b2, float eps, float c1, float c2) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n || !live[k]) return;
+  const float gk = grad[k];
+  const float mk = b1 * m[k] + (1.f - b1) * gk;
+  const float vk = b2 * v[k] + (1.f - b2) * gk * gk;
+  m[k] = mk;
+  v[k] = vk;
+  w[k] -= lr * (mk / c1) / (sqrtf(vk / c2) + eps);
+}
+
+// Master FP32 parameters of one layer -> BF16 weights [27][16][16] and the
+// flipped/transposed weights [27][16 ci][16 co] of its backward-data pass.
+__global__ void k_pack_weights(const float* __restrict__ w, __nv_bfloat16* __restrict__ wf,
+                               __nv_bfloat16* __restrict__ wb) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= 27 * 256) return;
+  const int tap = k / 256, co = (k / 16) % 16, ci = k % 16;
+  const __nv_bfloat16 v = __float2bfloat16_rn(w[k]);
+  wf[k] = v;
+  wb[(26 - tap) * 256 + ci * 16 + co] = v;
+}
+
+// ---------------------------------------------------------------------------
+// Solver <-> network glue (node grid, interleaved FP64 vectors)
+// ---------------------------------------------------------------------------
+// X0[n] = (s^-1 * dinvs * r (3 ch), rho feature, 0...)
+__global__ void k_net_input(const double* __restrict__ r, const double* __restrict__ dinvs,
+                            const float* __restrict__ feat, const CgState* st, double scale_mul,
+                            __nv_bfloat16* __restrict__ X0, int64_t nn) {
+  const double inv_s = 1.0 / fmax(sqrt(st->rz * scale_mul), 1e-300);
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn;
+       n += (int64_t)gridDim.x * blockDim.x) {
+    __align__(16) __nv_bfloat16 v[16];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) v[c] = __float2bfloat16_rn((float)(r[3 * n + c] * dinvs[3 * n + c] * inv_s));
+    v[3] = __float2bfloat16_rn(feat[n]);
+#pragma unroll
+    for (int c = 4; c < 16; ++c) v[c] = __float2bfloat16_rn(0.f);
+    uint4* dst = reinterpret_cast<uint4*>(X0 + n * 16);
+    dst[0] = *reinterpret_cast<uint4*>(&v[0]);
+    dst[1] = *reinterpret_cast<uint4*>(&v[8]);
+  }
+}
+
+// z = M^-1 r + s * dinvs * NN(r)   (masked DOFs have minv = dinvs = 0).
+// With q_old: reduces z.q_old and sets the flexible-CG coefficient
+// st->beta = -(z.q_old) / (p_old.q_old) (0 when there is no previous step).
+__global__ void k_net_output(const double* __restrict__ r, const double* __restrict__ minv,
+                             const double* __restrict__ dinvs, const __nv_bfloat16* __restrict__ Y,
+                             int ystride, CgState* st, double scale_mul, double* __restrict__ z,
+                             const double* __restrict__ q_old, double* partials, int64_t nn) {
+  if (st->status != HX_RUNNING) return;
+  const double s = sqrt(st->rz * scale_mul);
+  double zq = 0.0;
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn;
+       n += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int64_t i = 3 * n + c;
+      const double zi = minv[i] * r[i] + s * dinvs[i] * (double)__bfloat162float(Y[n * ystride + c]);
+      z[i] = zi;
+      if (q_old) zq += zi * q_old[i];
+    }
+  }
+  if (!q_old) return;
+  double v[1] = {zq};
+  if (grid_reduce<1>(v, partials, &st->ticket[TK_AUX2]) && threadIdx.x == 0) {
+    const double pq = st->pq;
+    st->beta = (pq > 0.0 && isfinite(v[0])) ? -v[0] / pq : 0.0;
+  }
+}
+
+// Training loss in the Jacobi-scaled space.  Input scaling s = |r~|_2/sqrt(nf)
+// (st->rz = r.M^-1 r).  target = s^-1 D^1/2 e - s^-1 D^-1/2 r (what Jacobi
+// misses); loss = sum |NN - target|^2 / nf; D = dLoss/dNN (16 channels).
+__global__ void k_net_loss(const double* __restrict__ r, const double* __restrict__ e,
+                           const double* __restrict__ dinvs, const __nv_bfloat16* __restrict__ Y,
+                           const CgState* st, double scale_mul, double inv_nf,
+                           __nv_bfloat16* __restrict__ D, double* partials, CgState* rst,
+                           double* out, int64_t nn) {
+  const double inv_s = 1.0 / fmax(sqrt(st->rz * scale_mul), 1e-300);
+  double loss = 0.0;
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn;
+       n += (int64_t)gridDim.x * blockDim.x) {
+    __align__(16) __nv_bfloat16 v[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) v[c] = __float2bfloat16_rn(0.f);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int64_t i = 3 * n + c;
+      const double di = dinvs[i];
+      double t = 0.0, y = 0.0;
+      if (di > 0.0) {
+        t = (e[i] / di - r[i] * di) * inv_s;
+        y = (double)__bfloat162float(Y[n * 16 + c]);
+      }
+      const double d = y - t;
+      loss += d * d;
+      v[c] = __float2bfloat16_rn((float)(2.0 * d * inv_nf));
+    }
+    uint4* dst = reinterpret_cast<uint4*>(D + n * 16);
+    dst[0] = *reinterpret_cast<uint4*>(&v[0]);
+    dst[1] = *reinterpret_cast<uint4*>(&v[8]);
+  }
+  double vv[1] = {loss * inv_nf};
+  if (grid_reduce<1>(vv, partials, &rst->ticket[TK_AUX]) && threadIdx.x == 0) out[0] = vv[0];
+}
+
+// ---------------------------------------------------------------------------
+// host launchers
+// ---------------------------------------------------------------------------
+static dim3 conv_grid(const GridN& g) {
+  return dim3((unsigned)cdiv(g.nx, TX), (unsigned)cdiv(g.ny, TY), (unsigned)cdiv(g.nz, TZ));
+}
+
+size_t conv_num_tiles(const GridN& g) {
+  const dim3 d = conv_grid(g);
+  return (size_t)d.x * d.y * d.z;
+}
+
+void launch_conv3(cudaStream_t s, int cout, int epi, const __nv_bfloat16* X, __nv_bfloat16* Y,
+                  const __nv_bfloat16* W, const float* bias, const __nv_bfloat16* M,
+                  const GridN& g) {
+  const size_t smem = sizeof(ConvSmem);
+  static bool cfg[6] = {false, false, false, false, false, false};
+#define HX_CONV_CASE(CO, EP, IDX)                                                          \
+  if (cout == CO && epi == EP) {                                                           \
+    if (!cfg[IDX]) {                                                                       \
+      HX_CUDA(cudaFuncSetAttribute(k_conv3<CO, EP>,                                        \
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+      cfg[IDX] = true;                                                                     \
+    }                                                                                      \
+    k_conv3<CO, EP><<<conv_grid(g), NTHREADS, smem, s>>>(X, Y, W, bias, M, g);            \
+    HX_CHECK_LAUNCH();                                                                     \
+    return;                                                                                \
+  }
+  HX_CONV_CASE(16, 0, 0)
+  HX_CONV_CASE(16, 1, 1)
+  HX_CONV_CASE(16, 2, 2)
+  HX_CONV_CASE(8, 1, 3)
+#undef HX_CONV_CASE
+  throw Error{HX_BAD_ARG, "unsupported conv configuration"};
+}
+
+void launch_conv3_wgrad(cudaStream_t s, const __nv_bfloat16* X, const __nv_bfloat16* D,
+                        float* part, float* grad, const GridN& g) {
+  const size_t smem = (HNODES + TX * TY * TZ) * C * sizeof(__nv_bfloat16);
+  static bool cfg = false;
+  if (!cfg) {
+    HX_CUDA(cudaFuncSetAttribute(k_conv3_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+    cfg = true;
+  }
+  k_conv3_wgrad<<<conv_grid(g), NTHREADS, smem, s>>>(X, D, part, g);
+  HX_CHECK_LAUNCH();
+  const int len = 27 * 256 + 16;
+  k_reduce_parts<<<cdiv(len, 256), 256, 0, s>>>(part, (int)conv_num_tiles(g), len, grad);
+  HX_CHECK_LAUNCH();
+}
+
+void launch_adam(cudaStream_t s, float* w, float* m, float* v, const float* grad,
+                 const unsigned char* live, int n, float lr, int step) {
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  const float c1 = 1.f - powf(b1, (float)step), c2 = 1.f - powf(b2, (float)step);
+  k_adam<<<cdiv(n, 256), 256, 0, s>>>(w, m, v, grad, live, n, lr, b1, b2, eps, c1, c2);
+  HX_CHECK_LAUNCH();
+}
+
+void launch_pack_weights(cudaStream_t s, const float* w, __nv_bfloat16* wf, __nv_bfloat16* wb) {
+  k_pack_weights<<<cdiv(27 * 256, 256), 256, 0, s>>>(w, wf, wb);
+  HX_CHECK_LAUNCH();
+}
+
+void launch_net_input(cudaStream_t s, const double* r, const double* dinvs, const float* feat,
+                      const CgState* st, double scale_mul, __nv_bfloat16* X0, int64_t nn) {
+  k_net_input<<<vec_blocks(nn), 256, 0, s>>>(r, dinvs, feat, st, scale_mul, X0, nn);
+  HX_CHECK_LAUNCH();
+}
+
+void launch_net_output(cudaStream_t s, const double* r, const double* minv, const double* dinvs,
+                       const __nv_bfloat16* Y, int ystride, CgState* st, double scale_mul,
+                       double* z, const double* q_old, double* partials, int64_t nn) {
+  k_net_output<<<vec_blocks(nn), 256, 0, s>>>(r, minv, dinvs, Y, ystride, st, scale_mul, z, q_old,
+                                              partials, nn);
+  HX_CHECK_LAUNCH();
+}
+
+// dinvs = sqrt(minv) (the Jacobi scaling D^-1/2 on free DOFs, 0 elsewhere)
+__global__ void k_sqrt(const double* __restrict__ a, double* __restrict__ b, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = sqrt(a[i]);
+}
+void launch_sqrt(cudaStream_t s, const double* a, double* b, int64_t n) {
+  k_sqrt<<<vec_blocks(n), 256, 0, s>>>(a, b, n);
+  HX_CHECK_LAUNCH();
+}
+
+// Density feature of a node: mean over its elements of (log10 f + 9) / 9,
+// clamped to [0, 1] (f = stiffness factor, 1e-9 .. 1 under SIMP).
+__global__ void k_rho_feature(const double* __restrict__ fac, float* __restrict__ feat, Grid g) {
+  const int64_t nn = g.nodes();
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn;
+       n += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(n % g.nxn);
+    const int64_t rr = n / g.nxn;
+    const int j = (int)(rr % g.nyn), k = (int)(rr / g.nyn);
+    double s = 0.0;
+    int cnt = 0;
+    for (int dk = -1; dk <= 0; ++dk)
+      for (int dj = -1; dj <= 0; ++dj)
+        for (int di = -1; di <= 0; ++di) {
+          const int ei = i + di, ej = j + dj, ek = k + dk;
+          if (ei < 0 || ej < 0 || ek < 0 || ei >= g.nxe || ej >= g.nye || ek >= g.nze) continue;
+          const double f = fac[((int64_t)ek * g.nye + ej) * g.nxe + ei];
+          s += fmin(fmax((log10(fmax(f, 1e-12)) + 9.0) / 9.0, 0.0), 1.0);
+          ++cnt;
+        }
+    feat[n] = cnt ? (float)(s / cnt) : 0.f;
+  }
+}
+void launch_rho_feature(cudaStream_t s, const double* fac, float* feat, const Grid& g) {
+  k_rho_feature<<<vec_blocks(g.nodes()), 256, 0, s>>>(fac, feat, g);
+  HX_CHECK_LAUNCH();
+}
+
+void launch_net_loss(cudaStream_t s, const double* r, const double* e, const double* dinvs,
+                     const __nv_bfloat16* Y, const CgState* st, double scale_mul, double inv_nf,
+                     __nv_bfloat16* D, double* partials, CgState* rst, double* out, int64_t nn) {
+  k_net_loss<<<vec_blocks(nn), 256, 0, s>>>(r, e, dinvs, Y, st, scale_mul, inv_nf, D, partials,
+                                            rst, out, nn);
+  HX_CHECK_LAUNCH();
+}
+
+}  // namespace hx

@@ -59,6 +59,7 @@ enum : int {
   HX_ST_DIVERGED = 4,
   HX_ST_MAXITER = 5,
   HX_ST_ZERO_RHS = 6,
+  HX_ST_PAUSED = 7,  // reliable-update point reached (mixed precision)
 };
 
 struct CgState {
@@ -73,7 +74,8 @@ struct CgState {
   double tol;
   double explode;   // status DIVERGED when ||r|| > explode * ||b|| (0: off)
   double div_ratio; // status DIVERGED when rel > div_ratio*best after 50 its (0: off)
-  double aux[4];    // free slots for derived scalars (e.g. inner-solve data)
+  double aux[4];    // derived scalars; CG with reliable updates uses
+                    // aux[1] = delta (> 0 enables), aux[2] = max r.r since update
   int iter;         // completed iterations
   int max_iter;
   int status;

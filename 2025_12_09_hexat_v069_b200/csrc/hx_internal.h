@@ -6,6 +6,8 @@
 #include <string>
 #include <vector>
 
+#include <cuda_bf16.h>
+
 #include "hx_common.cuh"
 
 namespace hx {
@@ -60,6 +62,12 @@ template <typename T>
 void launch_pcg_step(cudaStream_t s, const T* pin, T* pout, const T* r, const T* minv, T* x, T* q,
                      const T* fac, const uint8_t* nmask, const Grid& g, const ElemCoef<T>& K,
                      T shift, CgState* st, double* partials);
+// Flexible-CG step: p_out = z + beta p_in, x += alpha_old p_in (owned
+// nodes), q = mask(K p_out + s p_out), st->alpha = (p_out . r) / (p_out . q).
+template <typename T>
+void launch_fcg_step(cudaStream_t s, const T* pin, T* pout, const T* z, const T* r, T* x, T* q,
+                     const T* fac, const uint8_t* nmask, const Grid& g, const ElemCoef<T>& K,
+                     T shift, CgState* st, double* partials);
 template <typename T>
 void launch_node_diag(cudaStream_t s, const T* fac, const uint8_t* bcfree, uint8_t* nmask, T* diag,
                       const Grid& g, const ElemCoef<double>& K, double* partials, CgState* st,
@@ -103,6 +111,8 @@ void launch_ir_correct(cudaStream_t s, double* x, const float* d32, int64_t n, c
 template <typename TD, typename TS>
 void launch_convert(cudaStream_t s, TD* dst, const TS* src, int64_t n);
 void launch_fill_zero(cudaStream_t s, void* p, size_t bytes);
+// r = a - b
+void launch_axpby(cudaStream_t s, double* r, const double* a, const double* b, int64_t n);
 
 // ---- filter (hx_filter.cu) ----
 struct FilterCoef {
@@ -182,6 +192,16 @@ struct hx_ctx {
   bool f_used = false;
 
   int64_t launches = 0;  // kernels launched on behalf of this context
+
+  // convolutional preconditioner network (see hx_net.cu)
+  struct Net {
+    bool ready = false;
+    int step = 0;  // Adam steps taken
+    hx::DevBuf<float> w, m, v, grad, part, feat;
+    hx::DevBuf<unsigned char> live;
+    hx::DevBuf<__nv_bfloat16> wf, wb, x0, a1, a2, a3, y, da, db;
+    hx::DevBuf<double> dinvs, z, scal;
+  } net;
 
   size_t partial_capacity() const { return d_partials.n; }
 };

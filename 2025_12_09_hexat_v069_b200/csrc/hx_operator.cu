@@ -65,7 +65,7 @@ template <typename T>
 struct OpArgs {
   const T* pin;   // vector to multiply (MODE 0-2) or p_old (FUSED)
   const T* r;     // FUSED: residual
-  const T* minv;  // FUSED: Jacobi inverse diagonal
+  const T* minv;  // MODE 3: Jacobi inverse diagonal; MODE 4: preconditioned z
   T* x;           // FUSED: solution (x += alpha_old p_old on owned nodes)
   T* pout;        // FUSED: new direction p
   T* q;           // output K p (masked, shifted)
@@ -117,10 +117,12 @@ __device__ __forceinline__ void lambda_row(const ElemCoef<T>& K, const T (&U)[3]
 
 // MODE 0: q = mask(K x + s x);  MODE 1: also out[0] = x.q;
 // MODE 2: CG matvec, st->pq = p.q, st->alpha = rz / pq, breakdown test;
-// MODE 3: fused PCG step (see file header), then as MODE 2.
+// MODE 3: fused PCG step (see file header), then as MODE 2;
+// MODE 4: flexible-CG step: p = z + beta p_old (z from a nonlinear
+//         preconditioner), x += alpha_old p_old, q = K p; alpha = p.r / p.q.
 template <typename T, int BY, int MODE, int MINB>
 __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
-  constexpr bool FUSED = MODE == 3;
+  constexpr bool FUSED = MODE >= 3;
   constexpr int NT = MV_BX * BY;
   constexpr int PLANE = OpSmem<T, BY, FUSED>::PLANE;
   constexpr int RW = MV_BX + 1;          // nodes per staged row
@@ -187,8 +189,9 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
     cp_async_commit();
   };
 
-  // FUSED: p = M^-1 r + beta p_old in place; owned nodes of owned planes
-  // store p and advance x with the old direction.
+  // FUSED: p = M^-1 r + beta p_old (MODE 4: z + beta p_old) in place; owned
+  // nodes of owned planes store p and advance x with the old direction.
+  double prsum = 0.0;  // MODE 4: p.r over owned DOFs
   auto transform = [&](int kp) {
     if (!FUSED) return;
     const bool kown = kp >= k0 && kp < k1;
@@ -202,12 +205,13 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
       const int idx = tid + q * NT;
       if (q == NCP - 1 && idx >= PLANE) continue;
       const T pold = ps[idx];
-      const T pnew = ms[idx] * rs[idx] + beta_old * pold;
+      const T pnew = (MODE == 4 ? ms[idx] : ms[idx] * rs[idx]) + beta_old * pold;
       ps[idx] = pnew;
       if (kown && ((flags >> (8 + q)) & 1u)) {
         const int64_t gi = base + goff[q];
         A.pout[gi] = pnew;
         A.x[gi] = xs[idx] + alpha_old * pold;
+        if (MODE == 4) prsum += (double)pnew * (double)rs[idx];
       }
     }
   };
@@ -295,7 +299,17 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
     }
   }
 
-  if (MODE != 0) {
+  if (MODE == 4) {
+    double v[2] = {dsum, prsum};
+    if (grid_reduce<2>(v, A.partials, &A.st->ticket[TK_MATVEC]) && tid == 0) {
+      const double pq = v[0];
+      A.st->pq = pq;
+      if (!(pq > 0.0) || !isfinite(pq) || !isfinite(v[1]))
+        A.st->status = HX_ST_BREAKDOWN;
+      else
+        A.st->alpha = v[1] / pq;
+    }
+  } else if (MODE != 0) {
     double v[1] = {dsum};
     if (grid_reduce<1>(v, A.partials, &A.st->ticket[TK_MATVEC]) && tid == 0) {
       if (MODE == 1) {
@@ -370,7 +384,7 @@ inline dim3 mv_grid(const Grid& g, int kchunk) {
 
 template <typename T, int MODE>
 void launch_struct(cudaStream_t s, const OpArgs<T>& a) {
-  constexpr bool FUSED = MODE == 3;
+  constexpr bool FUSED = MODE >= 3;
   constexpr int MINB = 2;
   const size_t smem = sizeof(OpSmem<T, MV_BY, FUSED>);
   static bool configured = false;  // per instantiation
@@ -446,6 +460,32 @@ void launch_pcg_step(cudaStream_t s, const T* pin, T* pout, const T* r, const T*
   a.partials = partials;
   launch_struct<T, 3>(s, a);
 }
+
+template <typename T>
+void launch_fcg_step(cudaStream_t s, const T* pin, T* pout, const T* z, const T* r, T* x, T* q,
+                     const T* fac, const uint8_t* nmask, const Grid& g, const ElemCoef<T>& K,
+                     T shift, CgState* st, double* partials) {
+  OpArgs<T> a{};
+  a.pin = pin;
+  a.pout = pout;
+  a.r = r;
+  a.minv = z;
+  a.x = x;
+  a.q = q;
+  a.fac = fac;
+  a.nmask = nmask;
+  a.g = g;
+  a.kchunk = mv_kchunk(g);
+  a.K = K;
+  a.shift = shift;
+  a.st = st;
+  a.partials = partials;
+  launch_struct<T, 4>(s, a);
+}
+template void launch_fcg_step<double>(cudaStream_t, const double*, double*, const double*,
+                                      const double*, double*, double*, const double*,
+                                      const uint8_t*, const Grid&, const ElemCoef<double>&,
+                                      double, CgState*, double*);
 
 template void launch_matvec<double>(cudaStream_t, int, const double*, double*, const double*,
                                     const uint8_t*, const Grid&, const ElemCoef<double>&, double,

@@ -5,6 +5,7 @@
 #include <chrono>
 #include <cmath>
 #include <functional>
+#include <limits>
 
 #include "hx_solver.h"
 
@@ -91,8 +92,8 @@ void upload_bc(hx_ctx* c) {
   c->bc_dirty = false;
 }
 
-static CgState fresh_state(double tol, int max_iter, int check_every, bool divchecks,
-                           bool keep_best) {
+CgState fresh_state(double tol, int max_iter, int check_every, bool divchecks,
+                    bool keep_best) {
   CgState s{};
   s.tol = tol;
   s.max_iter = max_iter;
@@ -105,13 +106,13 @@ static CgState fresh_state(double tol, int max_iter, int check_every, bool divch
   return s;
 }
 
-static void put_state(hx_ctx* c, int slot, const CgState& s) {
+void put_state(hx_ctx* c, int slot, const CgState& s) {
   c->h_state[slot] = s;
   HX_CUDA(cudaMemcpyAsync(c->d_state.p + slot, c->h_state + slot, sizeof(CgState),
                           cudaMemcpyHostToDevice, c->stream));
 }
 
-static CgState get_state(hx_ctx* c, int slot) {
+CgState get_state(hx_ctx* c, int slot) {
   HX_CUDA(cudaMemcpyAsync(c->h_state + slot, c->d_state.p + slot, sizeof(CgState),
                           cudaMemcpyDeviceToHost, c->stream));
   HX_CUDA(cudaStreamSynchronize(c->stream));
@@ -119,11 +120,11 @@ static CgState get_state(hx_ctx* c, int slot) {
 }
 
 // Run `body` (a sequence of launches on c->stream) `reps` times as one CUDA
-// graph launch per poll; stop when the state in `slot` leaves RUNNING or the
-// wall-clock limit is hit.  Returns the final state.
-template <typename Body>
-static CgState run_batched(hx_ctx* c, int slot, int reps, Body&& body, double wall_limit_ms,
-                           double t0, bool* timed_out) {
+// graph launch per poll; stop when the state in `slot` leaves RUNNING, the
+// wall-clock limit is hit, or after `max_launches` graph launches (0: no
+// limit).  Returns the final state.
+CgState run_batched(hx_ctx* c, int slot, int reps, const std::function<void()>& body,
+                    double wall_limit_ms, double t0, bool* timed_out, int max_launches) {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   const int64_t before = launch_counter();
@@ -144,11 +145,12 @@ static CgState run_batched(hx_ctx* c, int slot, int reps, Body&& body, double wa
   CgState st{};
   *timed_out = false;
   try {
-    for (;;) {
+    for (int nl = 1;; ++nl) {
       HX_CUDA(cudaGraphLaunch(exec, c->stream));
       launch_counter() += per_graph;
       st = get_state(c, slot);
       if (st.status != HX_RUNNING) break;
+      if (max_launches > 0 && nl >= max_launches) break;
       if (wall_limit_ms > 0 && now_ms() - t0 > wall_limit_ms) {
         *timed_out = true;
         break;
@@ -162,7 +164,7 @@ static CgState run_batched(hx_ctx* c, int slot, int reps, Body&& body, double wa
   return st;
 }
 
-static int auto_batch(const Grid& g, int check_every) {
+int auto_batch(const Grid& g, int check_every) {
   if (check_every > 0) return check_every;
   const int64_t n = g.dofs();
   if (n > 4000000) return 16;
@@ -172,7 +174,7 @@ static int auto_batch(const Grid& g, int check_every) {
 
 // Jacobi set-up: node masks, diagonal, shift, M^-1 (FP64) into c->d_minv.
 // Returns max diagonal over free DOFs.
-static double jacobi_setup(hx_ctx* c, const double* fac, double shift_factor, double* shift_out) {
+double jacobi_setup_public(hx_ctx* c, const double* fac, double shift_factor, double* shift_out) {
   const Grid& g = c->g;
   const int64_t nn = g.nodes(), n = g.dofs();
   c->d_nmask.ensure(nn);
@@ -200,10 +202,10 @@ static double jacobi_setup(hx_ctx* c, const double* fac, double shift_factor, do
 // x += alpha p of the last iteration is applied.  Returns the final state.
 // ---------------------------------------------------------------------------
 template <typename T>
-static CgState pcg_fused(hx_ctx* c, int slot, const T* fac, const T* b, T* x, bool warm, T shift,
-                         const ElemCoef<T>& K, T* r, T* P0, T* P1, T* q, const T* minv,
-                         T* xbest, const CgState& init, int check_every, double wall_ms,
-                         double t0, bool* timed_out) {
+CgState pcg_fused(hx_ctx* c, int slot, const T* fac, const T* b, T* x, bool warm, T shift,
+                  const ElemCoef<T>& K, T* r, T* P0, T* P1, T* q, const T* minv, T* xbest,
+                  const CgState& init, int check_every, double wall_ms, double t0,
+                  bool* timed_out) {
   const Grid& g = c->g;
   const int64_t n = g.dofs();
   CgState* st = c->d_state.p + slot;
@@ -230,7 +232,7 @@ static CgState pcg_fused(hx_ctx* c, int slot, const T* fac, const T* b, T* x, bo
     if (xbest) launch_axpy_state<T>(c->stream, xbest, x, P1, n, st, 1);
   };
   const int reps = std::max(1, check_every / 2);
-  CgState sf = run_batched(c, slot, reps, body, wall_ms, t0, timed_out);
+  CgState sf = run_batched(c, slot, reps, body, wall_ms, t0, timed_out, 0);
   // apply the pending step x_{k+1} = x_k + alpha_k p_k (not after a breakdown,
   // whose alpha is invalid); p_k sits in P[(iter-1) % 2]
   if (sf.status != HX_ST_BREAKDOWN && sf.iter > 0) {
@@ -239,6 +241,15 @@ static CgState pcg_fused(hx_ctx* c, int slot, const T* fac, const T* b, T* x, bo
   }
   return sf;
 }
+
+template CgState pcg_fused<double>(hx_ctx*, int, const double*, const double*, double*, bool,
+                                   double, const ElemCoef<double>&, double*, double*, double*,
+                                   double*, const double*, double*, const CgState&, int, double,
+                                   double, bool*);
+template CgState pcg_fused<float>(hx_ctx*, int, const float*, const float*, float*, bool, float,
+                                  const ElemCoef<float>&, float*, float*, float*, float*,
+                                  const float*, float*, const CgState&, int, double, double,
+                                  bool*);
 
 static CgState pcg_fp64(hx_ctx* c, const double* fac, const double* b, double* x, bool warm,
                         double shift, const hx_solve_opts& o, double t0, bool* timed_out) {
@@ -272,7 +283,14 @@ static double true_residual(hx_ctx* c, const double* fac, const double* b, const
 }
 
 // ---------------------------------------------------------------------------
-// Mixed precision: FP32 Jacobi-PCG inner solves inside FP64 refinement.
+// Mixed precision: FP32 Jacobi-PCG with reliable updates.  The Krylov
+// iteration (fused step + residual update) runs in FP32 with FP64 dot
+// products; it accumulates its correction in d32.  Whenever the recursive
+// FP32 residual has dropped by `delta` (opts.inner_tol) since the last
+// replacement, or claims convergence, the host folds d32 into the FP64
+// solution, recomputes the true residual b - (K+sI)x in FP64, replaces the
+// FP32 residual with it and resumes with the same search direction (no
+// restart).  Convergence is judged only on the FP64 true residual.
 // ---------------------------------------------------------------------------
 static CgState solve_mixed(hx_ctx* c, const double* fac, const double* b, double* x, bool warm,
                            double shift, const hx_solve_opts& o, double t0, bool* timed_out,
@@ -282,17 +300,21 @@ static CgState solve_mixed(hx_ctx* c, const double* fac, const double* b, double
   float* fac32 = c->d_fac32.ensure(ne);
   float* minv32 = c->d_minv32.ensure(n);
   float* r32 = c->d_r32.ensure(n);
-  float* p32 = c->d_p32.ensure(n);
+  float* P0 = c->d_p32.ensure(n);
+  float* P1 = c->d_p32b.ensure(n);
   float* q32 = c->d_q32.ensure(n);
   float* d32 = c->d_x32.ensure(n);
   double* q = c->d_q.ensure(n);
   launch_convert<float, double>(c->stream, fac32, fac, ne);
   launch_convert<float, double>(c->stream, minv32, c->d_minv.p, n);
   const ElemCoef<float> K32 = to_float(c->K);
-  CgState* so = c->d_state.p;      // outer
-  // outer state: ||b|| from a dot product
-  CgState s = fresh_state(o.tol, std::max(1, o.max_refine), 1, false, false);
-  put_state(c, 0, s);
+  const float sh32 = (float)shift;
+  CgState* so = c->d_state.p;      // FP64 outer: ||b||, true residual
+  CgState* si = c->d_state.p + 1;  // FP32 Krylov iteration
+  *inner_total = 0;
+  // ||b||
+  CgState s = fresh_state(o.tol, std::numeric_limits<int>::max(), 1, false, false);
+  put_state(c, 3, CgState{});
   launch_dot(c->stream, b, b, n, c->d_state.p + 3, c->d_partials.p, c->d_scalars.p);
   double bb = 0;
   HX_CUDA(cudaMemcpyAsync(&bb, c->d_scalars.p, sizeof(double), cudaMemcpyDeviceToHost,
@@ -307,47 +329,86 @@ static CgState solve_mixed(hx_ctx* c, const double* fac, const double* b, double
   }
   put_state(c, 0, s);
   if (!warm) launch_fill_zero(c->stream, x, n * sizeof(double));
-  const double inner_tol = o.inner_tol > 0 ? o.inner_tol : 1e-4;
-  *inner_total = 0;
-  bool first = !warm;
+  // true residual of the initial guess -> r32 = r / ||b||
+  if (warm)
+    launch_matvec<double>(c->stream, 0, x, q, fac, c->d_nmask.p, g, c->K, shift,
+                          c->d_state.p + 3, c->d_partials.p, nullptr);
+  else
+    launch_fill_zero(c->stream, q, n * sizeof(double));
+  launch_ir_residual(c->stream, b, q, r32, n, so, c->d_partials.p);
+  CgState so_h = get_state(c, 0);
+  if (so_h.status != HX_RUNNING) return so_h;
+  // FP32 iteration state: rz from the replaced residual, p_{-1} = z, alpha =
+  // beta = 0; bnorm = 1 because r32 is already scaled by 1/||b||
+  const double delta = (o.inner_tol > 0 && o.inner_tol < 1) ? o.inner_tol : 0.1;
+  CgState init = fresh_state(o.tol, o.max_iter, 1, false, false);
+  put_state(c, 1, init);
+  launch_fill_zero(c->stream, d32, n * sizeof(float));
+  launch_cg_init<float>(c->stream, r32, nullptr, minv32, r32, P1, n, si, c->d_partials.p);
+  CgState st = get_state(c, 1);
+  st.bnorm = 1.0;
+  st.aux[1] = delta;
+  st.aux[2] = st.rr;
+  st.max_iter = o.max_iter;
+  put_state(c, 1, st);
+  const int reps = std::max(1, auto_batch(g, o.check_every) / 2);
+  int parity = 0;  // which P buffer holds p_{k-1}: P1 when parity == 0
   for (;;) {
-    if (first) {
-      launch_fill_zero(c->stream, q, n * sizeof(double));
-      first = false;
-    } else {
-      launch_matvec<double>(c->stream, 0, x, q, fac, c->d_nmask.p, g, c->K, shift, c->d_state.p + 3,
-                            c->d_partials.p, nullptr);
+    float* Pin = parity ? P0 : P1;
+    float* Pout = parity ? P1 : P0;
+    auto body = [&]() {
+      launch_pcg_step<float>(c->stream, Pin, Pout, r32, minv32, d32, q32, fac32, c->d_nmask.p, g,
+                             K32, sh32, si, c->d_partials.p);
+      launch_cg_update2<float>(c->stream, r32, q32, minv32, n, si, c->d_partials.p);
+      launch_pcg_step<float>(c->stream, Pout, Pin, r32, minv32, d32, q32, fac32, c->d_nmask.p, g,
+                             K32, sh32, si, c->d_partials.p);
+      launch_cg_update2<float>(c->stream, r32, q32, minv32, n, si, c->d_partials.p);
+    };
+    const int it_before = st.iter;
+    CgState sf = run_batched(c, 1, reps, body, o.wall_limit_ms, t0, timed_out, 0);
+    const int done = sf.iter - it_before;
+    *inner_total += done;
+    // p_k of the last completed iteration: iterations alternate Pin -> Pout
+    float* pk = (done % 2 == 1) ? Pout : Pin;
+    if (done % 2 == 1) parity ^= 1;
+    if (sf.status != HX_ST_BREAKDOWN && done > 0) {
+      launch_axpy_state<float>(c->stream, d32, d32, pk, n, si, 0);  // pending step
     }
+    // fold the FP32 correction into x and replace the residual in FP64
+    launch_ir_correct(c->stream, x, d32, n, so);
+    launch_fill_zero(c->stream, d32, n * sizeof(float));
+    launch_matvec<double>(c->stream, 0, x, q, fac, c->d_nmask.p, g, c->K, shift,
+                          c->d_state.p + 3, c->d_partials.p, nullptr);
     launch_ir_residual(c->stream, b, q, r32, n, so, c->d_partials.p);
-    CgState so_h = get_state(c, 0);
-    if (so_h.status != HX_RUNNING) return so_h;
-    if (o.wall_limit_ms > 0 && now_ms() - t0 > o.wall_limit_ms) {
-      *timed_out = true;
+    so_h = get_state(c, 0);
+    if (so_h.status != HX_RUNNING) {
+      so_h.iter = *inner_total;
+      return so_h;  // converged on the true residual (or non-finite)
+    }
+    if (*timed_out || sf.status == HX_ST_BREAKDOWN || sf.status == HX_ST_NONFINITE ||
+        sf.status == HX_ST_DIVERGED || *inner_total >= o.max_iter) {
+      so_h.status = (sf.status == HX_ST_PAUSED || sf.status == HX_ST_CONVERGED ||
+                     sf.status == HX_RUNNING)
+                        ? HX_ST_MAXITER
+                        : sf.status;
+      so_h.iter = *inner_total;
       return so_h;
     }
-    const int inner_max = std::max(1, o.max_iter - *inner_total);
-    float* p32b = c->d_p32b.ensure(n);
-    CgState si_h = pcg_fused<float>(c, 1, fac32, r32, d32, false, (float)shift, K32, r32, p32,
-                                    p32b, q32, minv32, nullptr,
-                                    fresh_state(inner_tol, inner_max, 1, false, false),
-                                    auto_batch(g, o.check_every), o.wall_limit_ms, t0, timed_out);
-    *inner_total += si_h.iter;
-    launch_ir_correct(c->stream, x, d32, n, so);
-    if (*timed_out) {
-      // residual of the corrected iterate
-      launch_matvec<double>(c->stream, 0, x, q, fac, c->d_nmask.p, g, c->K, shift,
-                            c->d_state.p + 3, c->d_partials.p, nullptr);
-      launch_ir_residual(c->stream, b, q, r32, n, so, c->d_partials.p);
-      return get_state(c, 0);
-    }
-    if (*inner_total >= o.max_iter) {
-      launch_matvec<double>(c->stream, 0, x, q, fac, c->d_nmask.p, g, c->K, shift,
-                            c->d_state.p + 3, c->d_partials.p, nullptr);
-      launch_ir_residual(c->stream, b, q, r32, n, so, c->d_partials.p);
-      CgState f = get_state(c, 0);
-      if (f.status == HX_RUNNING) f.status = HX_ST_MAXITER;
-      return f;
-    }
+    // resume: rz from the replaced residual (p, beta kept), alpha = 0 so the
+    // next step does not re-apply the step already folded into x
+    st = get_state(c, 1);
+    launch_cg_init<float>(c->stream, r32, nullptr, minv32, r32, q32, n, si, c->d_partials.p);
+    CgState s2 = get_state(c, 1);
+    s2.bnorm = 1.0;
+    s2.alpha = 0.0;
+    s2.beta = st.beta;
+    s2.iter = sf.iter;
+    s2.aux[1] = delta;
+    s2.aux[2] = s2.rr;
+    s2.max_iter = o.max_iter;
+    s2.status = HX_RUNNING;
+    put_state(c, 1, s2);
+    st = s2;
   }
 }
 
@@ -375,8 +436,10 @@ hx_status solve_grid(hx_ctx* c, const double* f, const double* fac, double* u,
   const double t0 = now_ms();
   HX_REQUIRE(c->has_mesh, "no mesh: call hx_set_grid or hx_set_mesh first");
   HX_REQUIRE(o.tol > 0, "tol must be > 0");
-  HX_REQUIRE(o.preconditioner == HX_PC_JACOBI,
-             "only the Jacobi preconditioner is available through this entry point");
+  HX_REQUIRE(o.preconditioner == HX_PC_JACOBI || o.preconditioner == HX_PC_LEARNED,
+             "unknown preconditioner");
+  HX_REQUIRE(o.preconditioner != HX_PC_LEARNED || o.precision == HX_PREC_FP64,
+             "the learned preconditioner runs with FP64 vectors");
   ensure_workspace(c);
   if (c->bc_dirty) upload_bc(c);
   const Grid& g = c->g;
@@ -397,7 +460,7 @@ hx_status solve_grid(hx_ctx* c, const double* f, const double* fac, double* u,
   for (int attempt = 1; attempt <= attempts; ++attempt) {
     const double ts = now_ms();
     if (attempt == 1) {
-      maxd = jacobi_setup(c, fac, factor, &shift);
+      maxd = jacobi_setup_public(c, fac, factor, &shift);
       launch_mask_rhs<double>(c->stream, f, c->d_minv.p, b, n);
     } else {
       shift = factor * maxd;
@@ -410,14 +473,19 @@ hx_status solve_grid(hx_ctx* c, const double* f, const double* fac, double* u,
     HX_CUDA(cudaStreamSynchronize(c->stream));
     t_setup += now_ms() - ts;
     CgState st{};
-    if (o.precision == HX_PREC_FP64) {
+    if (o.preconditioner == HX_PC_LEARNED) {
+      int fb = 0, its = 0;
+      st = solve_learned(c, fac, b, u, warm, shift, o, t0, &timed_out, &fb, &its);
+      total_iters += its;
+      R.fallback_used = fb;
+    } else if (o.precision == HX_PREC_FP64) {
       st = pcg_fp64(c, fac, b, u, warm, shift, o, t0, &timed_out);
       total_iters += st.iter;
     } else {
       int inner = 0;
       st = solve_mixed(c, fac, b, u, warm, shift, o, t0, &timed_out, &inner);
       total_iters += inner;
-      R.refinements = st.iter;
+      R.refinements = c->h_state[0].iter;
     }
     last = st;
     R.attempts = attempt;
@@ -534,7 +602,7 @@ hx_status filter_grid(hx_ctx* c, const Grid& g, const double h[3], const double*
     launch_cg_pupdate<double>(c->stream, p, r, invd, nn, st);
   };
   bool to = false;
-  CgState sf = run_batched(c, 2, 10, body, 0.0, t0, &to);
+  CgState sf = run_batched(c, 2, 10, body, 0.0, t0, &to, 0);
   launch_filter_extract(c->stream, x, out, g);
   HX_CUDA(cudaStreamSynchronize(c->stream));
   R.iterations = sf.iter;
@@ -607,7 +675,7 @@ hx_status time_kernel(hx_ctx* c, int kernel, int reps, double* avg_ms) {
     launch_convert<float, double>(c->stream, f32, c->d_fac.p, ne);
     launch_convert<float, double>(c->stream, m32, c->d_minv.p, n);
     HX_CUDA(cudaMemsetAsync(p32, 0, n * sizeof(float), c->stream));
-    HX_CUDA(cudaMemsetAsync(r32, 0, n * sizeof(float), c->stream));
+    launch_convert<float, double>(c->stream, r32, c->d_r.p, n);
     HX_CUDA(cudaMemsetAsync(x32, 0, n * sizeof(float), c->stream));
     const ElemCoef<float> K32 = to_float(c->K);
     body = [&, f32, p32, p32b, q32, r32, m32, x32, K32] {

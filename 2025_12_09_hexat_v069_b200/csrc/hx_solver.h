@@ -1,9 +1,38 @@
 // hx_solver.h -- device-level solver entry points (grid numbering, FP64
 // device arrays) used by the C ABI layer.
 #pragma once
+#include <functional>
+
 #include "hx_internal.h"
 
 namespace hx {
+// device-state plumbing shared by the solvers
+CgState fresh_state(double tol, int max_iter, int check_every, bool divchecks, bool keep_best);
+void put_state(hx_ctx* c, int slot, const CgState& s);
+CgState get_state(hx_ctx* c, int slot);
+int auto_batch(const Grid& g, int check_every);
+CgState run_batched(hx_ctx* c, int slot, int reps, const std::function<void()>& body,
+                    double wall_limit_ms, double t0, bool* timed_out, int max_launches);
+// node masks, diagonal, shift and M^-1 (FP64) for `fac`; returns max diag
+double jacobi_setup_public(hx_ctx* c, const double* fac, double shift_factor, double* shift_out);
+template <typename T>
+CgState pcg_fused(hx_ctx* c, int slot, const T* fac, const T* b, T* x, bool warm, T shift,
+                  const ElemCoef<T>& K, T* r, T* P0, T* P1, T* q, const T* minv, T* xbest,
+                  const CgState& init, int check_every, double wall_ms, double t0,
+                  bool* timed_out);
+// learned preconditioner (hx_net.cu)
+void net_init(hx_ctx* c, uint64_t seed);
+void net_set_params(hx_ctx* c, const float* params);
+void net_get_params(hx_ctx* c, float* params);
+void net_forward_backward(hx_ctx* c, int nx, int ny, int nz, const float* x0, const float* dy,
+                          float* y, float* grads);
+double net_train_step(hx_ctx* c, const double* r, const double* e, double lr);
+void net_prepare(hx_ctx* c, const double* fac);
+CgState solve_learned(hx_ctx* c, const double* fac, const double* b, double* x, bool warm,
+                      double shift, const hx_solve_opts& o, double t0, bool* timed_out,
+                      int* fallback, int* iters_out);
+int pcg_snapshots(hx_ctx* c, const double* f, const double* fac, int every, int count,
+                  double tol, double* snaps);
 void ensure_workspace(hx_ctx* c);
 void upload_bc(hx_ctx* c);
 hx_status solve_grid(hx_ctx* c, const double* f, const double* fac, double* u,

@@ -94,6 +94,11 @@ __device__ __forceinline__ void cg_finish_iteration(CgState* st, double rzn, dou
       if (st->keep_best) st->snap = 1;
     } else if (st->iter >= st->max_iter) {
       status = HX_ST_MAXITER;
+    } else if (st->aux[1] > 0.0) {
+      // reliable updates: pause once the recursive residual has dropped by
+      // delta since the last FP64 residual replacement
+      if (rr > st->aux[2]) st->aux[2] = rr;
+      if (rr < st->aux[1] * st->aux[1] * st->aux[2]) status = HX_ST_PAUSED;
     }
     st->beta = rzn / st->rz;
     st->rz = rzn;
@@ -380,6 +385,17 @@ void launch_convert(cudaStream_t s, TD* dst, const TS* src, int64_t n) {
 template void launch_convert<float, double>(cudaStream_t, float*, const double*, int64_t);
 template void launch_convert<double, float>(cudaStream_t, double*, const float*, int64_t);
 template void launch_convert<double, double>(cudaStream_t, double*, const double*, int64_t);
+
+__global__ void k_sub(double* __restrict__ r, const double* __restrict__ a,
+                      const double* __restrict__ b, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    r[i] = a[i] - b[i];
+}
+void launch_axpby(cudaStream_t s, double* r, const double* a, const double* b, int64_t n) {
+  k_sub<<<vec_blocks(n), VEC_THREADS, 0, s>>>(r, a, b, n);
+  HX_CHECK_LAUNCH();
+}
 
 void launch_fill_zero(cudaStream_t s, void* p, size_t bytes) {
   HX_CUDA(cudaMemsetAsync(p, 0, bytes, s));

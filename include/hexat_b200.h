@@ -48,7 +48,8 @@ typedef enum hx_dtype { HX_F32 = 0, HX_F64 = 1 } hx_dtype;
 
 typedef enum hx_precision {
   HX_PREC_FP64 = 0,      /* plain FP64 Jacobi-PCG */
-  HX_PREC_MIXED32 = 1,   /* FP32 inner PCG inside FP64 iterative refinement */
+  HX_PREC_MIXED32 = 1,   /* FP32 PCG with FP64 reliable updates (true-residual
+                            replacement, FP64 dots, FP64 convergence test) */
   HX_PREC_MIXED_BF16 = 2 /* as MIXED32 with the search direction stored in BF16 */
 } hx_precision;
 
@@ -68,8 +69,10 @@ typedef struct hx_solve_opts {
   double wall_limit_ms;    /* 0: no limit */
   int32_t check_every;     /* host poll period in iterations (0: automatic) */
   int32_t keep_best;       /* 1: keep the best iterate (reference semantics) */
-  double inner_tol;        /* mixed precision: inner relative tolerance */
-  int32_t max_refine;      /* mixed precision: outer refinement steps */
+  double inner_tol;        /* mixed precision: the FP32 recursive residual is
+                              replaced by the FP64 true residual each time it
+                              has dropped by this factor (default 0.1) */
+  int32_t max_refine;      /* reserved */
   int32_t ref_retry;       /* 1: reference retry/shift-escalation semantics */
   int32_t divergence_checks; /* 1: explosion and 100x-over-best checks */
   int32_t verify_true_residual; /* 1: recompute ||b-Au|| in FP64 at the end */
@@ -79,7 +82,7 @@ typedef struct hx_solve_opts {
 typedef struct hx_solve_report {
   int32_t status;       /* hx_status of the solve */
   int32_t iterations;   /* CG iterations (all inner iterations when mixed) */
-  int32_t refinements;  /* outer refinement steps (mixed) */
+  int32_t refinements;  /* FP64 residual replacements (mixed) */
   int32_t attempts;     /* retry attempts used (ref_retry) */
   int32_t fallback_used;/* learned -> Jacobi fallback taken */
   int32_t zero_rhs;     /* 1: ||f_free|| == 0, u = 0 returned */
@@ -265,6 +268,48 @@ HX_API hx_status hx_oc_update(hx_ctx *ctx, int32_t dtype, const void *x,
                               const void *dc, const void *dv, double volfrac,
                               double move, void *xnew, double *lambda,
                               int32_t *steps);
+
+/* ---- learned preconditioner -----------------------------------------------------
+ * No reference counterpart.  A 3D CNN on the node grid (4 conv3d layers,
+ * 3x3x3, 4 -> 16 -> 16 -> 16 -> 3 channels, ReLU, BF16 weights and
+ * activations, FP32 accumulation on the tensor cores) corrects the Jacobi
+ * preconditioner: z = D^-1 r + s D^-1/2 NN(D^-1/2 r / s, density), with s the
+ * RMS of D^-1/2 r.  hx_solve with preconditioner HX_PC_LEARNED applies it in
+ * flexible CG (Notay, one stored direction) and falls back to Jacobi-PCG from
+ * the current iterate on breakdown or stagnation (report->fallback_used).
+ * Parameters: HX_NET_PARAMS floats, 4 layers of [27 taps][16 out][16 in]
+ * weights followed by 16 biases; padding channels are forced to zero. */
+#define HX_NET_PARAMS (4 * (27 * 256 + 16))
+HX_API hx_status hx_net_init(hx_ctx *ctx, uint64_t seed);
+HX_API hx_status hx_net_set_params(hx_ctx *ctx, const float *params);
+HX_API hx_status hx_net_get_params(hx_ctx *ctx, float *params);
+/* Forward and backward on an nx*ny*nz NODE grid from host arrays [node][16]
+ * (FP32, rounded to BF16): y = network output (16 channels, the last layer
+ * without ReLU), grads = dLoss/dparams for dLoss/dy = dy (gradient check). */
+HX_API hx_status hx_net_forward_backward(hx_ctx *ctx, int32_t nx, int32_t ny,
+                                         int32_t nz, const float *x0,
+                                         const float *dy, float *y,
+                                         float *grads);
+/* Operator inputs of the network (Jacobi scaling, density feature) for the
+ * FP64 device factors `fac` on the current mesh and BCs. */
+HX_API hx_status hx_net_prepare(hx_ctx *ctx, const double *fac_dev);
+/* One Adam step on a residual/error pair (FP64 device vectors, grid
+ * numbering) of the prepared operator; *loss = mean squared error in the
+ * Jacobi-scaled space. */
+HX_API hx_status hx_net_train_step(hx_ctx *ctx, const double *r_dev,
+                                   const double *e_dev, double lr,
+                                   double *loss);
+/* FP64 Jacobi-PCG from zero on (f, fac) storing the iterate every `every`
+ * (even) iterations into snaps_dev[count][3*nodes] until rtol `tol`;
+ * *taken = snapshots stored.  Training data for the network. */
+HX_API hx_status hx_pcg_snapshots(hx_ctx *ctx, const double *f_dev,
+                                  const double *fac_dev, int32_t every,
+                                  int32_t count, double tol, double *snaps_dev,
+                                  int32_t *taken);
+/* r = f - K(fac) x on the free DOFs (0 on fixed ones), FP64 device arrays. */
+HX_API hx_status hx_residual_device(hx_ctx *ctx, const double *f_dev,
+                                    const double *fac_dev, const double *x_dev,
+                                    double *r_dev);
 
 /* ---- instrumentation ---------------------------------------------------------
  * Average device time (CUDA events on the context stream) of `reps`
