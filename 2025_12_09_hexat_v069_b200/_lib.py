@@ -28,7 +28,7 @@ class SolveOpts(C.Structure):
         ("wall_limit_ms", C.c_double), ("check_every", C.c_int32), ("keep_best", C.c_int32),
         ("inner_tol", C.c_double), ("max_refine", C.c_int32), ("ref_retry", C.c_int32),
         ("divergence_checks", C.c_int32), ("verify_true_residual", C.c_int32),
-        ("reserved", C.c_int32 * 6),
+        ("learned_no_fallback", C.c_int32), ("reserved", C.c_int32 * 5),
     ]
 
 
@@ -86,7 +86,8 @@ PROTOTYPES = {
     "hx_net_get_params": (_i32, [_vp, _vp]),
     "hx_net_forward_backward": (_i32, [_vp, _i32, _i32, _i32, _vp, _vp, _vp, _vp]),
     "hx_net_prepare": (_i32, [_vp, _vp]),
-    "hx_net_train_step": (_i32, [_vp, _vp, _vp, _dbl, C.POINTER(_dbl)]),
+    "hx_net_apply": (_i32, [_vp, _vp, _vp]),
+    "hx_net_train_step": (_i32, [_vp, _vp, _vp, _dbl, _i32, C.POINTER(_dbl)]),
     "hx_pcg_snapshots": (_i32, [_vp, _vp, _vp, _i32, _i32, _dbl, _vp, C.POINTER(_i32)]),
     "hx_residual_device": (_i32, [_vp, _vp, _vp, _vp, _vp]),
     "hx_element_energy": (_i32, [_vp, _i32, _vp, _vp]),
@@ -269,7 +270,7 @@ class Context:
         return ms.value
 
     # ---- learned preconditioner ----
-    NET_PARAMS = 4 * (27 * 256 + 16)
+    NET_PARAMS = 4 * 27 * 256
 
     def net_init(self, seed=1):
         self.check(self.lib.hx_net_init(self.h, int(seed)), "hx_net_init")
@@ -296,10 +297,15 @@ class Context:
     def net_prepare(self, fac_ptr):
         self.check(self.lib.hx_net_prepare(self.h, C.c_void_p(fac_ptr)), "hx_net_prepare")
 
-    def net_train_step(self, r_ptr, e_ptr, lr):
+    def net_apply(self, r_ptr, z_ptr):
+        self.check(self.lib.hx_net_apply(self.h, C.c_void_p(r_ptr), C.c_void_p(z_ptr)),
+                   "hx_net_apply")
+
+    def net_train_step(self, r_ptr, e_ptr, lr, loss_kind=0):
         loss = C.c_double()
-        self.check(self.lib.hx_net_train_step(self.h, C.c_void_p(r_ptr), C.c_void_p(e_ptr),
-                                              float(lr), C.byref(loss)), "hx_net_train_step")
+        self.check(self.lib.hx_net_train_step(self.h, C.c_void_p(r_ptr), C.c_void_p(e_ptr or 0),
+                                              float(lr), int(loss_kind), C.byref(loss)),
+                   "hx_net_train_step")
         return loss.value
 
     def pcg_snapshots(self, f_ptr, fac_ptr, every, count, tol, snaps_ptr):

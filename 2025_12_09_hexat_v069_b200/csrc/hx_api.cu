@@ -804,13 +804,23 @@ HX_API hx_status hx_net_prepare(hx_ctx* c, const double* fac) {
   });
 }
 
-HX_API hx_status hx_net_train_step(hx_ctx* c, const double* r, const double* e, double lr,
-                                   double* loss) {
+HX_API hx_status hx_net_apply(hx_ctx* c, const double* r, double* z) {
   return guard(c, [&] {
     need_mesh(c);
-    HX_REQUIRE(r && e, "null argument");
+    HX_REQUIRE(r && z, "null argument");
+    hx::net_apply_vec(c, r, z);
+    return HX_OK;
+  });
+}
+
+HX_API hx_status hx_net_train_step(hx_ctx* c, const double* r, const double* e, double lr,
+                                   int32_t loss_kind, double* loss) {
+  return guard(c, [&] {
+    need_mesh(c);
+    HX_REQUIRE(r != nullptr, "null argument");
     HX_REQUIRE(lr > 0, "lr must be positive");
-    const double l = hx::net_train_step(c, r, e, lr);
+    HX_REQUIRE(loss_kind == 0 || loss_kind == 1, "loss_kind must be 0 or 1");
+    const double l = hx::net_train_step(c, r, e, lr, loss_kind);
     if (loss) *loss = l;
     return HX_OK;
   });

@@ -1,7 +1,8 @@
 // hx_cnn.cu -- 3D convolutional preconditioner network on the node grid:
-// BF16 implicit-GEMM conv3d (3x3x3, 16 input channels) on the tensor cores
-// with FP32 accumulation, its backward (data and weights), Adam, and the
-// input/output assembly around a Krylov solver.
+// BF16 implicit-GEMM conv3d (3x3x3, 16 input channels, no bias) on the
+// tensor cores with FP32 accumulation, its transpose (the backward-data
+// pass), the weight gradient, Adam, and the input/output assembly around a
+// Krylov solver.
 //
 // Activations are channels-last BF16, [node][16] (32 bytes per node, node
 // numbering of the grid).  A conv layer is a GEMM per CTA tile: M = 512
@@ -99,17 +100,15 @@ __device__ __forceinline__ void stage_tile(ConvSmem& sm, const __nv_bfloat16* __
 }  // namespace
 
 // ---------------------------------------------------------------------------
-// Forward / backward-data convolution.
-// Y[n, co] = EPI( sum_{tap, ci} X[n + off(tap), ci] * W[tap][co][ci] )
-// EPI 0: + bias, ReLU;  1: + bias;  2: * (M[n, co] > 0)  (ReLU derivative)
-// COUT: 16 or 8 output channels (stored with stride COUT).
+// Convolution and its transpose (zero padding at the grid boundary):
+// Y[n, co] = sum_{tap, ci} X[n + off(tap), ci] * W[tap][co][ci]
+// The transpose is this kernel on the flipped, per-tap transposed weights
+// (k_pack_weights).  COUT: 16 or 8 output channels (stored with stride COUT).
 // ---------------------------------------------------------------------------
-template <int COUT, int EPI>
+template <int COUT>
 __global__ void __launch_bounds__(NTHREADS) k_conv3(const __nv_bfloat16* __restrict__ X,
                                                     __nv_bfloat16* __restrict__ Y,
                                                     const __nv_bfloat16* __restrict__ W,
-                                                    const float* __restrict__ bias,
-                                                    const __nv_bfloat16* __restrict__ M,
                                                     GridN g) {
   constexpr int NT = COUT / 8;
   extern __shared__ __align__(128) unsigned char smraw[];
@@ -166,32 +165,21 @@ __global__ void __launch_bounds__(NTHREADS) k_conv3(const __nv_bfloat16* __restr
 #pragma unroll
       for (int nt = 0; nt < NT; ++nt) {
         const int co = nt * 8 + 2 * tq;
-        float v0 = acc[i][nt][2 * half], v1 = acc[i][nt][2 * half + 1];
-        if (EPI <= 1) {
-          v0 += bias[co];
-          v1 += bias[co + 1];
-          if (EPI == 0) {
-            v0 = fmaxf(v0, 0.f);
-            v1 = fmaxf(v1, 0.f);
-          }
-        } else {
-          const __nv_bfloat162 mm =
-              *reinterpret_cast<const __nv_bfloat162*>(M + node * COUT + co);
-          v0 = __bfloat162float(mm.x) > 0.f ? v0 : 0.f;
-          v1 = __bfloat162float(mm.y) > 0.f ? v1 : 0.f;
-        }
-        *reinterpret_cast<__nv_bfloat162*>(Y + node * COUT + co) = __floats2bfloat162_rn(v0, v1);
+        *reinterpret_cast<__nv_bfloat162*>(Y + node * COUT + co) =
+            __floats2bfloat162_rn(acc[i][nt][2 * half], acc[i][nt][2 * half + 1]);
       }
     }
   }
 }
 
 // ---------------------------------------------------------------------------
-// Weight/bias gradient partials of one CTA tile:
-// dW[tap][co][ci] = sum_n D[n, co] X[n + off(tap), ci],  db[co] = sum_n D[n, co]
-// D = gradient w.r.t. the pre-activation (16 channels, node-major).  Warp w
-// handles taps w, w+8, w+16, w+24 over all 512 nodes of the tile; the
-// result goes to part[cta][27*256 + 16] (FP32), summed later in fixed order.
+// Weight-gradient partials of one CTA tile:
+// dW[tap][co][ci] = sum_n D[n, co] X[n + off(tap), ci]
+// For a forward use, X is the layer input and D the gradient w.r.t. its
+// output; for a transposed use (output = W^T * x') the roles swap: X = the
+// gradient w.r.t. the output, D = x'.  Warp w handles taps w, w+8, w+16,
+// w+24 over all 512 nodes of the tile; the result goes to part[cta][27*256]
+// (FP32), summed later in fixed order.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(NTHREADS) k_conv3_wgrad(const __nv_bfloat16* __restrict__ X,
                                                           const __nv_bfloat16* __restrict__ D,
@@ -223,7 +211,7 @@ __global__ void __launch_bounds__(NTHREADS) k_conv3_wgrad(const __nv_bfloat16* _
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gq = lane >> 2, tq = lane & 3;
   float* out = part + (size_t)(blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)) *
-                          (27 * 256 + 16);
+                          (27 * 256);
   // ldmatrix.trans row addresses: matrix mi = lane/8, row r = lane%8
   const int mi = lane >> 3, rr = lane & 7;
   for (int tap = warp; tap < 27; tap += 8) {
@@ -259,32 +247,21 @@ __global__ void __launch_bounds__(NTHREADS) k_conv3_wgrad(const __nv_bfloat16* _
         out[tap * 256 + (co + 1) * 16 + ci] = acc[nt][2 * hh + 1];
       }
   }
-  // bias gradient: 16 sums over the tile's nodes (fixed order)
-  if (threadIdx.x < 16) {
-    float s = 0.f;
-    for (int node = 0; node < TX * TY * TZ; ++node) {
-      const unsigned off = swz(node, threadIdx.x >> 3) + (threadIdx.x & 7) * 2;
-      s += __bfloat162float(*reinterpret_cast<const __nv_bfloat16*>(
-          reinterpret_cast<const unsigned char*>(ds) + off));
-    }
-    out[27 * 256 + threadIdx.x] = s;
-  }
 }
 
-// Sum the per-CTA partials in a fixed order: grad[k] = sum_c part[c][k].
+// Sum the per-CTA partials in a fixed order: grad[k] (+)= sum_c part[c][k].
 __global__ void k_reduce_parts(const float* __restrict__ part, int nparts, int len,
-                               float* __restrict__ grad) {
+                               float* __restrict__ grad, int accumulate) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= len) return;
   double s = 0.0;
   for (int c = 0; c < nparts; ++c) s += (double)part[(size_t)c * len + k];
-  grad[k] = (float)s;
+  grad[k] = accumulate ? grad[k] + (float)s : (float)s;
 }
 
-// Adam step on FP32 master parameters (weights [27][16][16] then bias[16]
-// per layer, concatenated); writes the BF16 forward weights and their
-// flipped-transposed copy for the backward-data pass.  `live` masks the
-// parameters that exist (padding channels stay zero).
+// Adam step on the FP32 master parameters (weights [27][16][16] per layer,
+// concatenated).  `live` masks the parameters that exist (padding channels
+// stay zero).
 __global__ void k_adam(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v,
                        const float* __restrict__ grad, const unsigned char* __restrict__ live,
                        int n, float lr, float b1, float b2, float eps, float c1, float c2) {
@@ -313,41 +290,62 @@ __global__ void k_pack_weights(const float* __restrict__ w, __nv_bfloat16* __res
 // ---------------------------------------------------------------------------
 // Solver <-> network glue (node grid, interleaved FP64 vectors)
 // ---------------------------------------------------------------------------
-// X0[n] = (s^-1 * dinvs * r (3 ch), rho feature, 0...)
-__global__ void k_net_input(const double* __restrict__ r, const double* __restrict__ dinvs,
-                            const float* __restrict__ feat, const CgState* st, double scale_mul,
-                            __nv_bfloat16* __restrict__ X0, int64_t nn) {
-  const double inv_s = 1.0 / fmax(sqrt(st->rz * scale_mul), 1e-300);
+// The lifting E: X[n] = (k v~ (3 ch), k v~ * feat (3 ch), 0 ...), v~ = dinvs * v,
+// with the coefficient k of `mode`:  0: 1/s (network input, s the RMS of
+// D^-1/2 r);  1: 2 s / (e.r) (energy-loss gradient);  2: 2 s / (r.M^-1 r)
+// (residual-loss gradient).  s from sst->rz; e.r from lst->aux[0].
+__global__ void k_net_lift(const double* __restrict__ v, const double* __restrict__ dinvs,
+                           const float* __restrict__ feat, const CgState* sst, const CgState* lst,
+                           int mode, double scale_mul, __nv_bfloat16* __restrict__ X, int64_t nn) {
+  const double s = sqrt(sst->rz * scale_mul);
+  double k;
+  if (mode == 0) {
+    k = 1.0 / fmax(s, 1e-300);
+  } else {
+    const double den = (mode == 1) ? lst->aux[0] : sst->rz;
+    k = den > 0.0 ? 2.0 * s / den : 0.0;
+  }
   for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn;
        n += (int64_t)gridDim.x * blockDim.x) {
-    __align__(16) __nv_bfloat16 v[16];
+    __align__(16) __nv_bfloat16 o[16];
+    const double fn = (double)feat[n];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) v[c] = __float2bfloat16_rn((float)(r[3 * n + c] * dinvs[3 * n + c] * inv_s));
-    v[3] = __float2bfloat16_rn(feat[n]);
+    for (int c = 0; c < 3; ++c) {
+      const double t = k * dinvs[3 * n + c] * v[3 * n + c];
+      o[c] = __float2bfloat16_rn((float)t);
+      o[c + 3] = __float2bfloat16_rn((float)(t * fn));
+    }
 #pragma unroll
-    for (int c = 4; c < 16; ++c) v[c] = __float2bfloat16_rn(0.f);
-    uint4* dst = reinterpret_cast<uint4*>(X0 + n * 16);
-    dst[0] = *reinterpret_cast<uint4*>(&v[0]);
-    dst[1] = *reinterpret_cast<uint4*>(&v[8]);
+    for (int c = 6; c < 16; ++c) o[c] = __float2bfloat16_rn(0.f);
+    uint4* dst = reinterpret_cast<uint4*>(X + n * 16);
+    dst[0] = *reinterpret_cast<uint4*>(&o[0]);
+    dst[1] = *reinterpret_cast<uint4*>(&o[8]);
   }
 }
 
-// z = M^-1 r + s * dinvs * NN(r)   (masked DOFs have minv = dinvs = 0).
-// With q_old: reduces z.q_old and sets the flexible-CG coefficient
-// st->beta = -(z.q_old) / (p_old.q_old) (0 when there is no previous step).
+// z = M^-1 r + s * dinvs * E^T(Y), E^T(Y)_c = Y[c] + feat * Y[c + 3]
+// (Y: the network's 6-channel output with stride 8; masked DOFs have
+// minv = dinvs = 0).  With q_old: reduces z.q_old and sets the flexible-CG
+// coefficient st->beta = -(z.q_old) / (p_old.q_old) (0 without a previous
+// step).
 __global__ void k_net_output(const double* __restrict__ r, const double* __restrict__ minv,
-                             const double* __restrict__ dinvs, const __nv_bfloat16* __restrict__ Y,
-                             int ystride, CgState* st, double scale_mul, double* __restrict__ z,
-                             const double* __restrict__ q_old, double* partials, int64_t nn) {
+                             const double* __restrict__ dinvs, const float* __restrict__ feat,
+                             const __nv_bfloat16* __restrict__ Y, CgState* st, double scale_mul,
+                             double* __restrict__ z, const double* __restrict__ q_old,
+                             double* partials, int64_t nn) {
   if (st->status != HX_RUNNING) return;
   const double s = sqrt(st->rz * scale_mul);
   double zq = 0.0;
   for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn;
        n += (int64_t)gridDim.x * blockDim.x) {
+    const uint4 yy = *reinterpret_cast<const uint4*>(Y + n * 8);
+    const __nv_bfloat16* y = reinterpret_cast<const __nv_bfloat16*>(&yy);
+    const double fn = (double)feat[n];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const int64_t i = 3 * n + c;
-      const double zi = minv[i] * r[i] + s * dinvs[i] * (double)__bfloat162float(Y[n * ystride + c]);
+      const double t = (double)__bfloat162float(y[c]) + fn * (double)__bfloat162float(y[c + 3]);
+      const double zi = minv[i] * r[i] + s * dinvs[i] * t;
       z[i] = zi;
       if (q_old) zq += zi * q_old[i];
     }
@@ -360,40 +358,23 @@ __global__ void k_net_output(const double* __restrict__ r, const double* __restr
   }
 }
 
-// Training loss in the Jacobi-scaled space.  Input scaling s = |r~|_2/sqrt(nf)
-// (st->rz = r.M^-1 r).  target = s^-1 D^1/2 e - s^-1 D^-1/2 r (what Jacobi
-// misses); loss = sum |NN - target|^2 / nf; D = dLoss/dNN (16 channels).
-__global__ void k_net_loss(const double* __restrict__ r, const double* __restrict__ e,
-                           const double* __restrict__ dinvs, const __nv_bfloat16* __restrict__ Y,
-                           const CgState* st, double scale_mul, double inv_nf,
-                           __nv_bfloat16* __restrict__ D, double* partials, CgState* rst,
-                           double* out, int64_t nn) {
-  const double inv_s = 1.0 / fmax(sqrt(st->rz * scale_mul), 1e-300);
-  double loss = 0.0;
-  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn;
-       n += (int64_t)gridDim.x * blockDim.x) {
-    __align__(16) __nv_bfloat16 v[16];
-#pragma unroll
-    for (int c = 0; c < 16; ++c) v[c] = __float2bfloat16_rn(0.f);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const int64_t i = 3 * n + c;
-      const double di = dinvs[i];
-      double t = 0.0, y = 0.0;
-      if (di > 0.0) {
-        t = (e[i] / di - r[i] * di) * inv_s;
-        y = (double)__bfloat162float(Y[n * 16 + c]);
-      }
-      const double d = y - t;
-      loss += d * d;
-      v[c] = __float2bfloat16_rn((float)(2.0 * d * inv_nf));
-    }
-    uint4* dst = reinterpret_cast<uint4*>(D + n * 16);
-    dst[0] = *reinterpret_cast<uint4*>(&v[0]);
-    dst[1] = *reinterpret_cast<uint4*>(&v[8]);
+// Energy-norm training loss.  With z the preconditioned vector and
+// d = z - e:  loss = d.Ad / e.Ae, e.Ae = e.r.  Reduces [d.q, e.r] (q = A d)
+// into st->aux[0] = e.r and out[0] = loss.
+__global__ void k_net_aloss(const double* __restrict__ d, const double* __restrict__ q,
+                            const double* __restrict__ e, const double* __restrict__ r,
+                            int64_t n, double* partials, CgState* st, double* out) {
+  double dq = 0.0, er = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    dq += d[i] * q[i];
+    er += e[i] * r[i];
   }
-  double vv[1] = {loss * inv_nf};
-  if (grid_reduce<1>(vv, partials, &rst->ticket[TK_AUX]) && threadIdx.x == 0) out[0] = vv[0];
+  double v[2] = {dq, er};
+  if (grid_reduce<2>(v, partials, &st->ticket[TK_AUX2]) && threadIdx.x == 0) {
+    st->aux[0] = v[1];
+    out[0] = v[1] > 0.0 ? v[0] / v[1] : 0.0;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -408,32 +389,26 @@ size_t conv_num_tiles(const GridN& g) {
   return (size_t)d.x * d.y * d.z;
 }
 
-void launch_conv3(cudaStream_t s, int cout, int epi, const __nv_bfloat16* X, __nv_bfloat16* Y,
-                  const __nv_bfloat16* W, const float* bias, const __nv_bfloat16* M,
-                  const GridN& g) {
+void launch_conv3(cudaStream_t s, int cout, const __nv_bfloat16* X, __nv_bfloat16* Y,
+                  const __nv_bfloat16* W, const GridN& g) {
   const size_t smem = sizeof(ConvSmem);
-  static bool cfg[6] = {false, false, false, false, false, false};
-#define HX_CONV_CASE(CO, EP, IDX)                                                          \
-  if (cout == CO && epi == EP) {                                                           \
-    if (!cfg[IDX]) {                                                                       \
-      HX_CUDA(cudaFuncSetAttribute(k_conv3<CO, EP>,                                        \
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
-      cfg[IDX] = true;                                                                     \
-    }                                                                                      \
-    k_conv3<CO, EP><<<conv_grid(g), NTHREADS, smem, s>>>(X, Y, W, bias, M, g);            \
-    HX_CHECK_LAUNCH();                                                                     \
-    return;                                                                                \
+  static bool cfg[2] = {false, false};
+  if (cout != 16 && cout != 8) throw Error{HX_BAD_ARG, "unsupported conv configuration"};
+  const int idx = cout == 16 ? 0 : 1;
+  if (!cfg[idx]) {
+    HX_CUDA(cudaFuncSetAttribute(cout == 16 ? k_conv3<16> : k_conv3<8>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    cfg[idx] = true;
   }
-  HX_CONV_CASE(16, 0, 0)
-  HX_CONV_CASE(16, 1, 1)
-  HX_CONV_CASE(16, 2, 2)
-  HX_CONV_CASE(8, 1, 3)
-#undef HX_CONV_CASE
-  throw Error{HX_BAD_ARG, "unsupported conv configuration"};
+  if (cout == 16)
+    k_conv3<16><<<conv_grid(g), NTHREADS, smem, s>>>(X, Y, W, g);
+  else
+    k_conv3<8><<<conv_grid(g), NTHREADS, smem, s>>>(X, Y, W, g);
+  HX_CHECK_LAUNCH();
 }
 
 void launch_conv3_wgrad(cudaStream_t s, const __nv_bfloat16* X, const __nv_bfloat16* D,
-                        float* part, float* grad, const GridN& g) {
+                        float* part, float* grad, bool accumulate, const GridN& g) {
   const size_t smem = (HNODES + TX * TY * TZ) * C * sizeof(__nv_bfloat16);
   static bool cfg = false;
   if (!cfg) {
@@ -443,8 +418,9 @@ void launch_conv3_wgrad(cudaStream_t s, const __nv_bfloat16* X, const __nv_bfloa
   }
   k_conv3_wgrad<<<conv_grid(g), NTHREADS, smem, s>>>(X, D, part, g);
   HX_CHECK_LAUNCH();
-  const int len = 27 * 256 + 16;
-  k_reduce_parts<<<cdiv(len, 256), 256, 0, s>>>(part, (int)conv_num_tiles(g), len, grad);
+  const int len = 27 * 256;
+  k_reduce_parts<<<cdiv(len, 256), 256, 0, s>>>(part, (int)conv_num_tiles(g), len, grad,
+                                                accumulate ? 1 : 0);
   HX_CHECK_LAUNCH();
 }
 
@@ -461,16 +437,17 @@ void launch_pack_weights(cudaStream_t s, const float* w, __nv_bfloat16* wf, __nv
   HX_CHECK_LAUNCH();
 }
 
-void launch_net_input(cudaStream_t s, const double* r, const double* dinvs, const float* feat,
-                      const CgState* st, double scale_mul, __nv_bfloat16* X0, int64_t nn) {
-  k_net_input<<<vec_blocks(nn), 256, 0, s>>>(r, dinvs, feat, st, scale_mul, X0, nn);
+void launch_net_lift(cudaStream_t s, const double* v, const double* dinvs, const float* feat,
+                     const CgState* sst, const CgState* lst, int mode, double scale_mul,
+                     __nv_bfloat16* X, int64_t nn) {
+  k_net_lift<<<vec_blocks(nn), 256, 0, s>>>(v, dinvs, feat, sst, lst, mode, scale_mul, X, nn);
   HX_CHECK_LAUNCH();
 }
 
 void launch_net_output(cudaStream_t s, const double* r, const double* minv, const double* dinvs,
-                       const __nv_bfloat16* Y, int ystride, CgState* st, double scale_mul,
+                       const float* feat, const __nv_bfloat16* Y, CgState* st, double scale_mul,
                        double* z, const double* q_old, double* partials, int64_t nn) {
-  k_net_output<<<vec_blocks(nn), 256, 0, s>>>(r, minv, dinvs, Y, ystride, st, scale_mul, z, q_old,
+  k_net_output<<<vec_blocks(nn), 256, 0, s>>>(r, minv, dinvs, feat, Y, st, scale_mul, z, q_old,
                                               partials, nn);
   HX_CHECK_LAUNCH();
 }
@@ -514,11 +491,9 @@ void launch_rho_feature(cudaStream_t s, const double* fac, float* feat, const Gr
   HX_CHECK_LAUNCH();
 }
 
-void launch_net_loss(cudaStream_t s, const double* r, const double* e, const double* dinvs,
-                     const __nv_bfloat16* Y, const CgState* st, double scale_mul, double inv_nf,
-                     __nv_bfloat16* D, double* partials, CgState* rst, double* out, int64_t nn) {
-  k_net_loss<<<vec_blocks(nn), 256, 0, s>>>(r, e, dinvs, Y, st, scale_mul, inv_nf, D, partials,
-                                            rst, out, nn);
+void launch_net_aloss(cudaStream_t s, const double* d, const double* q, const double* e,
+                      const double* r, int64_t n, double* partials, CgState* st, double* out) {
+  k_net_aloss<<<vec_blocks(n), 256, 0, s>>>(d, q, e, r, n, partials, st, out);
   HX_CHECK_LAUNCH();
 }
 

@@ -199,8 +199,10 @@ struct hx_ctx {
     int step = 0;  // Adam steps taken
     hx::DevBuf<float> w, m, v, grad, part, feat;
     hx::DevBuf<unsigned char> live;
-    hx::DevBuf<__nv_bfloat16> wf, wb, x0, a1, a2, a3, y, da, db;
-    hx::DevBuf<double> dinvs, z, scal;
+    hx::DevBuf<__nv_bfloat16> wf, wb, x0, y, da, db;
+    hx::DevBuf<__nv_bfloat16> act[7];  // G activations A1 A2 A3 H, then G^T's B3 B2 B1
+    hx::DevBuf<double> dinvs, z, scal, facbuf;
+    const double* fac_last = nullptr;  // factors the operator inputs were built for
   } net;
 
   size_t partial_capacity() const { return d_partials.n; }

@@ -76,7 +76,8 @@ typedef struct hx_solve_opts {
   int32_t ref_retry;       /* 1: reference retry/shift-escalation semantics */
   int32_t divergence_checks; /* 1: explosion and 100x-over-best checks */
   int32_t verify_true_residual; /* 1: recompute ||b-Au|| in FP64 at the end */
-  int32_t reserved[6];
+  int32_t learned_no_fallback; /* 1: learned FCG without the Jacobi fallback */
+  int32_t reserved[5];
 } hx_solve_opts;
 
 typedef struct hx_solve_report {
@@ -270,22 +271,24 @@ HX_API hx_status hx_oc_update(hx_ctx *ctx, int32_t dtype, const void *x,
                               int32_t *steps);
 
 /* ---- learned preconditioner -----------------------------------------------------
- * No reference counterpart.  A 3D CNN on the node grid (4 conv3d layers,
- * 3x3x3, 4 -> 16 -> 16 -> 16 -> 3 channels, ReLU, BF16 weights and
- * activations, FP32 accumulation on the tensor cores) corrects the Jacobi
- * preconditioner: z = D^-1 r + s D^-1/2 NN(D^-1/2 r / s, density), with s the
- * RMS of D^-1/2 r.  hx_solve with preconditioner HX_PC_LEARNED applies it in
+ * No reference counterpart.  A 3D CNN G on the node grid (4 conv3d layers,
+ * 3x3x3, no bias, 6 -> 16 -> 16 -> 16 -> 16 channels, BF16 weights and
+ * activations, FP32 accumulation on the tensor cores) defines the
+ * preconditioner  z = D^-1/2 (I + E^T G^T G E) D^-1/2 r,  E the lifting
+ * v -> (v, density * v) per node and G^T the transposed convolutions.  It is
+ * symmetric positive definite for every choice of weights; zero weights
+ * give Jacobi.  hx_solve with preconditioner HX_PC_LEARNED applies it in
  * flexible CG (Notay, one stored direction) and falls back to Jacobi-PCG from
  * the current iterate on breakdown or stagnation (report->fallback_used).
  * Parameters: HX_NET_PARAMS floats, 4 layers of [27 taps][16 out][16 in]
- * weights followed by 16 biases; padding channels are forced to zero. */
-#define HX_NET_PARAMS (4 * (27 * 256 + 16))
+ * weights; the input channels >= 6 of the first layer are forced to zero. */
+#define HX_NET_PARAMS (4 * 27 * 256)
 HX_API hx_status hx_net_init(hx_ctx *ctx, uint64_t seed);
 HX_API hx_status hx_net_set_params(hx_ctx *ctx, const float *params);
 HX_API hx_status hx_net_get_params(hx_ctx *ctx, float *params);
-/* Forward and backward on an nx*ny*nz NODE grid from host arrays [node][16]
- * (FP32, rounded to BF16): y = network output (16 channels, the last layer
- * without ReLU), grads = dLoss/dparams for dLoss/dy = dy (gradient check). */
+/* y = G^T G x0 on an nx*ny*nz NODE grid from host arrays [node][16] (FP32,
+ * rounded to BF16; channels >= 6 of x0 and dy are ignored, those of y are
+ * zero) and grads = d<dy, y>/dparams (gradient check). */
 HX_API hx_status hx_net_forward_backward(hx_ctx *ctx, int32_t nx, int32_t ny,
                                          int32_t nz, const float *x0,
                                          const float *dy, float *y,
@@ -293,12 +296,17 @@ HX_API hx_status hx_net_forward_backward(hx_ctx *ctx, int32_t nx, int32_t ny,
 /* Operator inputs of the network (Jacobi scaling, density feature) for the
  * FP64 device factors `fac` on the current mesh and BCs. */
 HX_API hx_status hx_net_prepare(hx_ctx *ctx, const double *fac_dev);
-/* One Adam step on a residual/error pair (FP64 device vectors, grid
- * numbering) of the prepared operator; *loss = mean squared error in the
- * Jacobi-scaled space. */
+/* z = P r, the learned preconditioner of the prepared operator (FP64 device
+ * vectors, grid numbering); z = 0 when r vanishes on the free DOFs. */
+HX_API hx_status hx_net_apply(hx_ctx *ctx, const double *r_dev, double *z_dev);
+/* One Adam step on a residual (and error) of the prepared operator (FP64
+ * device vectors, grid numbering; r = f - K x, e = u* - x).  With z the
+ * preconditioned vector of r:  loss_kind 0: *loss = (z-e)^T K (z-e) / e^T K e
+ * (needs e);  loss_kind 1: *loss = |D^-1/2 (K z - r)|^2 / |D^-1/2 r|^2
+ * (e unused, may be NULL). */
 HX_API hx_status hx_net_train_step(hx_ctx *ctx, const double *r_dev,
                                    const double *e_dev, double lr,
-                                   double *loss);
+                                   int32_t loss_kind, double *loss);
 /* FP64 Jacobi-PCG from zero on (f, fac) storing the iterate every `every`
  * (even) iterations into snaps_dev[count][3*nodes] until rtol `tol`;
  * *taken = snapshots stored.  Training data for the network. */

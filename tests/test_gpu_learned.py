@@ -1,0 +1,191 @@
+"""The learned preconditioner P = D^-1/2 (I + E^T G^T G E) D^-1/2: the BF16
+tensor-core convolutions of G and G^T and the weight gradient checked
+against a CPU reference built on torch (FP32 arithmetic with the kernels'
+BF16 roundings of weights, activations and gradients); P symmetric positive
+definite; training on solver-generated residual/error pairs; flexible CG
+with the trained network against plain Jacobi-PCG; the fallback path."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+LP = 27 * 256
+NET_IN = 6
+
+
+def _bf(a):
+    import torch
+    return a.to(torch.bfloat16).to(torch.float32)
+
+
+def _torch_reference(params, dims, x0, dy):
+    """y = G^T G x0 and d<dy, y>/dW in torch (CPU, FP32), rounding to BF16
+    where the GPU kernels store BF16: every layer output, forward and
+    backward."""
+    import torch
+    import torch.nn.functional as F
+    nx, ny, nz = dims
+
+    def vol(a):  # [node][16] (x fastest) -> [1, 16, z, y, x]
+        return torch.from_numpy(a.reshape(nz, ny, nx, 16)).permute(3, 0, 1, 2)[None].float()
+
+    def unvol(t):
+        return t[0].permute(1, 2, 3, 0).reshape(-1, 16).numpy()
+
+    W = [_bf(torch.from_numpy(params[l * LP:(l + 1) * LP].reshape(27, 16, 16))
+             .permute(1, 2, 0).reshape(16, 16, 3, 3, 3)) for l in range(4)]  # [co][ci][kz][ky][kx]
+    conv = lambda x, l: _bf(F.conv3d(x, W[l], padding=1))
+    convT = lambda x, l: _bf(F.conv_transpose3d(x, W[l], padding=1))
+    wgrad = lambda X, D: torch.nn.grad.conv3d_weight(X, W[0].shape, D, padding=1)
+    a = [_bf(vol(x0))]
+    for l in range(4):
+        a.append(conv(a[-1], l))          # A1 A2 A3 H
+    b = {4: a[4]}
+    for l in (3, 2, 1, 0):
+        b[l] = convT(b[l + 1], l)         # B3 B2 B1 B0
+    gw = [torch.zeros_like(W[0]) for _ in range(4)]
+    e = _bf(vol(dy))
+    for l in range(4):                    # transposed uses: X = dLoss/dout, D = input
+        gw[l] += wgrad(e, b[l + 1])
+        e = conv(e, l)
+    for l in (3, 2, 1, 0):                # forward uses: X = input, D = dLoss/dout
+        gw[l] += wgrad(a[l], e)
+        if l > 0:
+            e = convT(e, l)
+    grads = np.concatenate([g.reshape(16, 16, 27).permute(2, 0, 1).reshape(-1).numpy()
+                            for g in gw])
+    return unvol(b[0]), grads
+
+
+def test_conv_stack_and_gradient_match_torch(ctx):
+    dims = (21, 11, 6)  # several 16x8x4 tiles, partial at every edge
+    nn_ = dims[0] * dims[1] * dims[2]
+    rng = np.random.default_rng(7)
+    ctx.net_init(seed=11)
+    p = ctx.net_get_params()
+    p = (p + rng.normal(0, 0.02, p.size).astype(np.float32))
+    ctx.net_set_params(p)
+    p = ctx.net_get_params()  # unused input channels forced to zero
+    assert not p.reshape(4, 27, 16, 16)[0, :, :, NET_IN:].any()
+    x0 = np.zeros((nn_, 16), np.float32)
+    x0[:, :NET_IN] = rng.standard_normal((nn_, NET_IN))
+    dy = np.zeros((nn_, 16), np.float32)
+    dy[:, :NET_IN] = rng.standard_normal((nn_, NET_IN))
+    y, g = ctx.net_forward_backward(dims, x0, dy)
+    yr, gr = _torch_reference(p, dims, x0, dy)
+    assert not y[:, NET_IN:].any()
+    assert np.abs(y - yr).max() <= 2e-2 * np.abs(yr).max()
+    assert np.abs(y - yr).mean() <= 2e-3 * np.abs(yr).max()
+    for l in range(4):
+        a, b = g[l * LP:(l + 1) * LP], gr[l * LP:(l + 1) * LP]
+        assert np.abs(a - b).max() <= 3e-2 * np.abs(b).max(), l
+        assert np.abs(a - b).mean() <= 3e-3 * np.abs(b).max(), l
+    assert np.isfinite(g).all()
+
+
+def _problem(ctx, hx, dims, seed):
+    import torch
+    W = hx.workloads
+    nodes, el, bc, f = W.cantilever(*dims)
+    ctx.set_grid(*dims)
+    ctx.set_material(1.0, 0.3)
+    ctx.set_bc(bc)
+    raw = W.raw_density(el.shape[0], seed)
+    rho_f, _ = ctx.filter(raw, 2.0, 0, 1e-5, 200)
+    fac = W.simp(W.map_density(rho_f, 1e-3))
+    dev = torch.device("cuda", 0)
+    return torch.from_numpy(f).to(dev), torch.from_numpy(fac).to(dev)
+
+
+def test_preconditioner_is_symmetric_positive_definite(ctx, hx):
+    import torch
+    dims = (24, 8, 8)
+    f_d, fac_d = _problem(ctx, hx, dims, seed=4)
+    ctx.solve_device(f_d.data_ptr(), fac_d.data_ptr(), torch.zeros_like(f_d).data_ptr(),
+                     opts=hx.default_opts(tol=1e-3))
+    ctx.net_init(seed=3)
+    p = ctx.net_get_params()
+    ctx.net_set_params(p * 3.0)  # a strong correction, far from Jacobi
+    ctx.net_prepare(fac_d.data_ptr())
+    g = torch.Generator(device="cpu").manual_seed(1)
+    bc = hx.workloads.cantilever(*dims, with_elements=False)[2]
+    free = torch.from_numpy(bc.reshape(-1) == 0).to(f_d.device)
+    r = [torch.randn(f_d.numel(), generator=g, dtype=torch.float64).to(f_d.device) * free
+         for _ in range(3)]
+    z = []
+    for v in r:
+        out = torch.empty_like(v)
+        ctx.net_apply(v.data_ptr(), out.data_ptr())
+        z.append(out)
+    for i in range(3):
+        assert float(r[i] @ z[i]) > 0
+        for j in range(i):
+            a, b = float(r[i] @ z[j]), float(r[j] @ z[i])
+            scale = np.sqrt(float(r[i] @ z[i]) * float(r[j] @ z[j]))
+            assert abs(a - b) <= 1e-2 * scale, (i, j, a, b)
+    # linearity in r (up to the BF16 roundings): P(2 r0 + r1) = 2 P r0 + P r1
+    out = torch.empty_like(r[0])
+    ctx.net_apply((2 * r[0] + r[1]).data_ptr(), out.data_ptr())
+    ref = 2 * z[0] + z[1]
+    assert float(torch.linalg.norm(out - ref) / torch.linalg.norm(ref)) < 2e-2
+    # zero residual -> zero
+    zero = torch.zeros_like(r[0])
+    ctx.net_apply(zero.data_ptr(), out.data_ptr())
+    assert not out.any()
+
+
+def test_training_reduces_loss_and_iterations(ctx, hx):
+    import torch
+    dims = (40, 12, 12)
+    f_d, fac_d = _problem(ctx, hx, dims, seed=3)
+    n = f_d.numel()
+    # reference solution and Jacobi-PCG snapshots
+    u_star = torch.zeros_like(f_d)
+    ctx.solve_device(f_d.data_ptr(), fac_d.data_ptr(), u_star.data_ptr(),
+                     opts=hx.default_opts(tol=1e-11, max_iter=100000))
+    base_iters = ctx.solve_device(f_d.data_ptr(), fac_d.data_ptr(),
+                                  torch.zeros_like(f_d).data_ptr(),
+                                  opts=hx.default_opts(tol=1e-6)).iterations
+    snaps = torch.zeros((64, n), dtype=torch.float64, device=f_d.device)
+    taken = ctx.pcg_snapshots(f_d.data_ptr(), fac_d.data_ptr(), 4, 64, 1e-8, snaps.data_ptr())
+    assert taken >= 8
+    ctx.net_init(seed=5)
+    ctx.net_prepare(fac_d.data_ptr())
+    r = torch.empty_like(f_d)
+    losses = []
+    rng = np.random.default_rng(0)
+    for step in range(1500):
+        k = int(rng.integers(taken))
+        ctx.residual_device(f_d.data_ptr(), fac_d.data_ptr(), snaps[k].data_ptr(), r.data_ptr())
+        e = (u_star - snaps[k]).contiguous()
+        losses.append(ctx.net_train_step(r.data_ptr(), e.data_ptr(), 1e-3))
+    first = np.mean(losses[:100])
+    last = np.mean(losses[-100:])
+    assert np.isfinite(losses).all() and last < first
+    # flexible CG with the trained network: converges on the true residual
+    u = torch.zeros_like(f_d)
+    rl = ctx.solve_device(f_d.data_ptr(), fac_d.data_ptr(), u.data_ptr(),
+                          opts=hx.default_opts(tol=1e-6, preconditioner=1, max_iter=20000,
+                                               learned_no_fallback=1))
+    assert rl.status == 0 and rl.true_rel_res < 1e-6
+    err = float(torch.linalg.norm(u - u_star) / torch.linalg.norm(u_star))
+    assert err < 1e-4
+    print(f"jacobi-pcg {base_iters} its; learned fcg {rl.iterations} its; "
+          f"loss {first:.3e} -> {last:.3e}")
+    # the gain: at least 1.5x fewer iterations than Jacobi-PCG
+    assert rl.iterations * 1.5 < base_iters
+
+
+def test_poisoned_network_falls_back_to_jacobi(ctx, hx):
+    import torch
+    dims = (24, 8, 8)
+    f_d, fac_d = _problem(ctx, hx, dims, seed=9)
+    ctx.net_init(seed=1)
+    p = ctx.net_get_params()
+    p[:] = 1e30  # the network now outputs inf/NaN
+    ctx.net_set_params(p)
+    u = torch.zeros_like(f_d)
+    rl = ctx.solve_device(f_d.data_ptr(), fac_d.data_ptr(), u.data_ptr(),
+                          opts=hx.default_opts(tol=1e-6, preconditioner=1, max_iter=20000))
+    assert rl.fallback_used == 1
+    assert rl.status == 0 and rl.true_rel_res < 1e-6
