@@ -18,7 +18,7 @@ HX_F32, HX_F64 = 0, 1
 HX_PREC_FP64, HX_PREC_MIXED32, HX_PREC_MIXED_BF16 = 0, 1, 2
 HX_PC_JACOBI, HX_PC_LEARNED, HX_PC_NONE = 0, 1, 2
 (HX_KERNEL_PCG_STEP_FP64, HX_KERNEL_PCG_UPDATE_FP64, HX_KERNEL_APPLY_FP64, HX_KERNEL_PCG_STEP_FP32,
- HX_KERNEL_FILTER_MATVEC) = range(5)
+ HX_KERNEL_FILTER_MATVEC, HX_KERNEL_CONV3, HX_KERNEL_NET_APPLY) = range(7)
 
 
 class SolveOpts(C.Structure):
@@ -88,6 +88,7 @@ PROTOTYPES = {
     "hx_net_prepare": (_i32, [_vp, _vp]),
     "hx_net_apply": (_i32, [_vp, _vp, _vp]),
     "hx_net_train_step": (_i32, [_vp, _vp, _vp, _dbl, _i32, C.POINTER(_dbl)]),
+    "hx_net_train_batch": (_i32, [_vp, _vp, _vp, _i32, _dbl, _i32, C.POINTER(_dbl)]),
     "hx_pcg_snapshots": (_i32, [_vp, _vp, _vp, _i32, _i32, _dbl, _vp, C.POINTER(_i32)]),
     "hx_residual_device": (_i32, [_vp, _vp, _vp, _vp, _vp]),
     "hx_element_energy": (_i32, [_vp, _i32, _vp, _vp]),
@@ -270,7 +271,7 @@ class Context:
         return ms.value
 
     # ---- learned preconditioner ----
-    NET_PARAMS = 4 * 27 * 256
+    NET_PARAMS = 3 * 4 * 27 * 256
 
     def net_init(self, seed=1):
         self.check(self.lib.hx_net_init(self.h, int(seed)), "hx_net_init")
@@ -306,6 +307,16 @@ class Context:
         self.check(self.lib.hx_net_train_step(self.h, C.c_void_p(r_ptr), C.c_void_p(e_ptr or 0),
                                               float(lr), int(loss_kind), C.byref(loss)),
                    "hx_net_train_step")
+        return loss.value
+
+    def net_train_batch(self, r_ptrs, e_ptrs, lr, loss_kind=0):
+        """One Adam step on the summed gradient of the pairs (device pointers)."""
+        k = len(r_ptrs)
+        ra = (C.c_void_p * k)(*[C.c_void_p(p) for p in r_ptrs])
+        ea = (C.c_void_p * k)(*[C.c_void_p(p) for p in e_ptrs]) if e_ptrs is not None else None
+        loss = C.c_double()
+        self.check(self.lib.hx_net_train_batch(self.h, ra, ea, k, float(lr), int(loss_kind),
+                                               C.byref(loss)), "hx_net_train_batch")
         return loss.value
 
     def pcg_snapshots(self, f_ptr, fac_ptr, every, count, tol, snaps_ptr):

@@ -815,12 +815,22 @@ HX_API hx_status hx_net_apply(hx_ctx* c, const double* r, double* z) {
 
 HX_API hx_status hx_net_train_step(hx_ctx* c, const double* r, const double* e, double lr,
                                    int32_t loss_kind, double* loss) {
+  return hx_net_train_batch(c, &r, e ? &e : nullptr, 1, lr, loss_kind, loss);
+}
+
+HX_API hx_status hx_net_train_batch(hx_ctx* c, const double* const* r, const double* const* e,
+                                    int32_t count, double lr, int32_t loss_kind, double* loss) {
   return guard(c, [&] {
     need_mesh(c);
-    HX_REQUIRE(r != nullptr, "null argument");
+    HX_REQUIRE(r != nullptr && count >= 1, "null argument or empty batch");
+    for (int i = 0; i < count; ++i) HX_REQUIRE(r[i] != nullptr, "null residual");
     HX_REQUIRE(lr > 0, "lr must be positive");
     HX_REQUIRE(loss_kind == 0 || loss_kind == 1, "loss_kind must be 0 or 1");
-    const double l = hx::net_train_step(c, r, e, lr, loss_kind);
+    if (loss_kind == 0) {
+      HX_REQUIRE(e != nullptr, "the energy loss needs the errors");
+      for (int i = 0; i < count; ++i) HX_REQUIRE(e[i] != nullptr, "null error");
+    }
+    const double l = hx::net_train_step(c, r, e, count, lr, loss_kind);
     if (loss) *loss = l;
     return HX_OK;
   });

@@ -290,13 +290,14 @@ __global__ void k_pack_weights(const float* __restrict__ w, __nv_bfloat16* __res
 // ---------------------------------------------------------------------------
 // Solver <-> network glue (node grid, interleaved FP64 vectors)
 // ---------------------------------------------------------------------------
-// The lifting E: X[n] = (k v~ (3 ch), k v~ * feat (3 ch), 0 ...), v~ = dinvs * v,
-// with the coefficient k of `mode`:  0: 1/s (network input, s the RMS of
-// D^-1/2 r);  1: 2 s / (e.r) (energy-loss gradient);  2: 2 s / (r.M^-1 r)
-// (residual-loss gradient).  s from sst->rz; e.r from lst->aux[0].
-__global__ void k_net_lift(const double* __restrict__ v, const double* __restrict__ dinvs,
-                           const float* __restrict__ feat, const CgState* sst, const CgState* lst,
-                           int mode, double scale_mul, __nv_bfloat16* __restrict__ X, int64_t nn) {
+// Scaled nodal field of a DOF vector: x[n][c] = k * dinvs[3n+c] * v[3n+c]
+// (FP32), with the coefficient k of `mode`:  0: 1/s (network input, s the
+// RMS of D^-1/2 r);  1: 2 s / (e.r) (energy-loss gradient);  2: 2 s /
+// (r.M^-1 r) (residual-loss gradient).  s from sst->rz; e.r from
+// lst->aux[0].
+__global__ void k_field_in(const double* __restrict__ v, const double* __restrict__ dinvs,
+                           const CgState* sst, const CgState* lst, int mode, double scale_mul,
+                           float* __restrict__ x, int64_t n) {
   const double s = sqrt(sst->rz * scale_mul);
   double k;
   if (mode == 0) {
@@ -305,15 +306,117 @@ __global__ void k_net_lift(const double* __restrict__ v, const double* __restric
     const double den = (mode == 1) ? lst->aux[0] : sst->rz;
     k = den > 0.0 ? 2.0 * s / den : 0.0;
   }
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    x[i] = (float)(k * dinvs[i] * v[i]);
+}
+
+// 1D full-weighting factor of fine offset d = j - 2i (|d| <= 1)
+__device__ __forceinline__ float fw(int d) { return d == 0 ? 1.f : 0.5f; }
+
+// Restriction to the next coarser node grid (coarse node i <-> fine node
+// 2i), full weighting (1/2, 1, 1/2) per axis, zero outside the grid:
+// out[i][c] = sum_d w(d) in[2i + d][c].  With `normalise`, divides by the
+// sum of the weights inside the grid (a weighted average; for features).
+template <int CH>
+__global__ void k_restrict(const float* __restrict__ in, float* __restrict__ out, GridN gf,
+                           GridN gc, int normalise) {
+  const int64_t nc = (int64_t)gc.nx * gc.ny * gc.nz;
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nc;
+       n += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(n % gc.nx);
+    const int64_t t = n / gc.nx;
+    const int j = (int)(t % gc.ny), k = (int)(t / gc.ny);
+    float acc[CH];
+#pragma unroll
+    for (int c = 0; c < CH; ++c) acc[c] = 0.f;
+    float wsum = 0.f;
+    for (int dz = -1; dz <= 1; ++dz) {
+      const int fz = 2 * k + dz;
+      if (fz < 0 || fz >= gf.nz) continue;
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int fy = 2 * j + dy;
+        if (fy < 0 || fy >= gf.ny) continue;
+        for (int dx = -1; dx <= 1; ++dx) {
+          const int fx = 2 * i + dx;
+          if (fx < 0 || fx >= gf.nx) continue;
+          const float w = fw(dz) * fw(dy) * fw(dx);
+          const int64_t f = ((int64_t)fz * gf.ny + fy) * gf.nx + fx;
+#pragma unroll
+          for (int c = 0; c < CH; ++c) acc[c] += w * in[f * CH + c];
+          wsum += w;
+        }
+      }
+    }
+    const float sc = (normalise && wsum > 0.f) ? 1.f / wsum : 1.f;
+#pragma unroll
+    for (int c = 0; c < CH; ++c) out[n * CH + c] = acc[c] * sc;
+  }
+}
+
+// Prolongation, the exact transpose of k_restrict (without normalisation):
+// fine[j][c] = (accumulate ? fine[j][c] : 0) + sum_{i: |j - 2i| <= 1} w(j - 2i) coarse[i][c].
+__global__ void k_prolong(const float* __restrict__ coarse, float* __restrict__ fine, GridN gf,
+                          GridN gc, int accumulate) {
+  const int64_t nf = (int64_t)gf.nx * gf.ny * gf.nz;
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nf;
+       n += (int64_t)gridDim.x * blockDim.x) {
+    const int fx = (int)(n % gf.nx);
+    const int64_t t = n / gf.nx;
+    const int fy = (int)(t % gf.ny), fz = (int)(t / gf.ny);
+    // per axis: the coarse nodes i with |f - 2i| <= 1: floor(f/2) and, for odd f, f/2 + 1
+    int ix[2], iy[2], iz[2];
+    float wx[2], wy[2], wz[2];
+    auto axis = [](int f, int nc, int (&i)[2], float (&w)[2]) {
+      if ((f & 1) == 0) {
+        i[0] = f >> 1; w[0] = 1.f; i[1] = 0; w[1] = 0.f;
+      } else {
+        i[0] = f >> 1; w[0] = 0.5f;
+        i[1] = (f >> 1) + 1; w[1] = (i[1] < nc) ? 0.5f : 0.f;
+        if (i[1] >= nc) i[1] = 0;
+      }
+      if (i[0] >= nc) { i[0] = 0; w[0] = 0.f; }
+    };
+    axis(fx, gc.nx, ix, wx);
+    axis(fy, gc.ny, iy, wy);
+    axis(fz, gc.nz, iz, wz);
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+#pragma unroll
+    for (int az = 0; az < 2; ++az)
+#pragma unroll
+      for (int ay = 0; ay < 2; ++ay)
+#pragma unroll
+        for (int ax = 0; ax < 2; ++ax) {
+          const float w = wz[az] * wy[ay] * wx[ax];
+          if (w == 0.f) continue;
+          const int64_t c = ((int64_t)iz[az] * gc.ny + iy[ay]) * gc.nx + ix[ax];
+          a0 += w * coarse[3 * c + 0];
+          a1 += w * coarse[3 * c + 1];
+          a2 += w * coarse[3 * c + 2];
+        }
+    if (accumulate) {
+      a0 += fine[3 * n + 0];
+      a1 += fine[3 * n + 1];
+      a2 += fine[3 * n + 2];
+    }
+    fine[3 * n + 0] = a0;
+    fine[3 * n + 1] = a1;
+    fine[3 * n + 2] = a2;
+  }
+}
+
+// The lifting E of a nodal field: X[n] = (x (3 ch), feat * x (3 ch), 0 ...) in BF16.
+__global__ void k_lift(const float* __restrict__ x, const float* __restrict__ feat,
+                       __nv_bfloat16* __restrict__ X, int64_t nn) {
   for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn;
        n += (int64_t)gridDim.x * blockDim.x) {
     __align__(16) __nv_bfloat16 o[16];
-    const double fn = (double)feat[n];
+    const float fn = feat[n];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const double t = k * dinvs[3 * n + c] * v[3 * n + c];
-      o[c] = __float2bfloat16_rn((float)t);
-      o[c + 3] = __float2bfloat16_rn((float)(t * fn));
+      const float t = x[3 * n + c];
+      o[c] = __float2bfloat16_rn(t);
+      o[c + 3] = __float2bfloat16_rn(t * fn);
     }
 #pragma unroll
     for (int c = 6; c < 16; ++c) o[c] = __float2bfloat16_rn(0.f);
@@ -323,32 +426,40 @@ __global__ void k_net_lift(const double* __restrict__ v, const double* __restric
   }
 }
 
-// z = M^-1 r + s * dinvs * E^T(Y), E^T(Y)_c = Y[c] + feat * Y[c + 3]
-// (Y: the network's 6-channel output with stride 8; masked DOFs have
-// minv = dinvs = 0).  With q_old: reduces z.q_old and sets the flexible-CG
-// coefficient st->beta = -(z.q_old) / (p_old.q_old) (0 without a previous
-// step).
-__global__ void k_net_output(const double* __restrict__ r, const double* __restrict__ minv,
-                             const double* __restrict__ dinvs, const float* __restrict__ feat,
-                             const __nv_bfloat16* __restrict__ Y, CgState* st, double scale_mul,
-                             double* __restrict__ z, const double* __restrict__ q_old,
-                             double* partials, int64_t nn) {
-  if (st->status != HX_RUNNING) return;
-  const double s = sqrt(st->rz * scale_mul);
-  double zq = 0.0;
+// Its transpose on the network output (6 channels, stride 8):
+// acc[n][c] (+)= Y[c] + feat * Y[c + 3].
+__global__ void k_unlift(const __nv_bfloat16* __restrict__ Y, const float* __restrict__ feat,
+                         float* __restrict__ acc, int accumulate, int64_t nn) {
   for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn;
        n += (int64_t)gridDim.x * blockDim.x) {
     const uint4 yy = *reinterpret_cast<const uint4*>(Y + n * 8);
     const __nv_bfloat16* y = reinterpret_cast<const __nv_bfloat16*>(&yy);
-    const double fn = (double)feat[n];
+    const float fn = feat[n];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const int64_t i = 3 * n + c;
-      const double t = (double)__bfloat162float(y[c]) + fn * (double)__bfloat162float(y[c + 3]);
-      const double zi = minv[i] * r[i] + s * dinvs[i] * t;
-      z[i] = zi;
-      if (q_old) zq += zi * q_old[i];
+      float t = __bfloat162float(y[c]) + fn * __bfloat162float(y[c + 3]);
+      if (accumulate) t += acc[3 * n + c];
+      acc[3 * n + c] = t;
     }
+  }
+}
+
+// z = M^-1 r + s * dinvs * t  (t: the correction field on the fine node grid,
+// FP32 [node][3]; masked DOFs have minv = dinvs = 0).  With q_old: reduces
+// z.q_old and sets the flexible-CG coefficient st->beta = -(z.q_old) /
+// (p_old.q_old) (0 without a previous step).
+__global__ void k_net_output(const double* __restrict__ r, const double* __restrict__ minv,
+                             const double* __restrict__ dinvs, const float* __restrict__ t,
+                             CgState* st, double scale_mul, double* __restrict__ z,
+                             const double* __restrict__ q_old, double* partials, int64_t n) {
+  if (st->status != HX_RUNNING) return;
+  const double s = sqrt(st->rz * scale_mul);
+  double zq = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double zi = minv[i] * r[i] + s * dinvs[i] * (double)t[i];
+    z[i] = zi;
+    if (q_old) zq += zi * q_old[i];
   }
   if (!q_old) return;
   double v[1] = {zq};
@@ -437,18 +548,47 @@ void launch_pack_weights(cudaStream_t s, const float* w, __nv_bfloat16* wf, __nv
   HX_CHECK_LAUNCH();
 }
 
-void launch_net_lift(cudaStream_t s, const double* v, const double* dinvs, const float* feat,
-                     const CgState* sst, const CgState* lst, int mode, double scale_mul,
-                     __nv_bfloat16* X, int64_t nn) {
-  k_net_lift<<<vec_blocks(nn), 256, 0, s>>>(v, dinvs, feat, sst, lst, mode, scale_mul, X, nn);
+void launch_field_in(cudaStream_t s, const double* v, const double* dinvs, const CgState* sst,
+                     const CgState* lst, int mode, double scale_mul, float* x, int64_t n) {
+  k_field_in<<<vec_blocks(n), 256, 0, s>>>(v, dinvs, sst, lst, mode, scale_mul, x, n);
+  HX_CHECK_LAUNCH();
+}
+
+void launch_restrict(cudaStream_t s, int ch, const float* in, float* out, const GridN& gf,
+                     const GridN& gc, bool normalise) {
+  const int64_t nc = (int64_t)gc.nx * gc.ny * gc.nz;
+  if (ch == 3)
+    k_restrict<3><<<vec_blocks(nc), 256, 0, s>>>(in, out, gf, gc, normalise ? 1 : 0);
+  else if (ch == 1)
+    k_restrict<1><<<vec_blocks(nc), 256, 0, s>>>(in, out, gf, gc, normalise ? 1 : 0);
+  else
+    throw Error{HX_BAD_ARG, "unsupported channel count"};
+  HX_CHECK_LAUNCH();
+}
+
+void launch_prolong(cudaStream_t s, const float* coarse, float* fine, const GridN& gf,
+                    const GridN& gc, bool accumulate) {
+  const int64_t nf = (int64_t)gf.nx * gf.ny * gf.nz;
+  k_prolong<<<vec_blocks(nf), 256, 0, s>>>(coarse, fine, gf, gc, accumulate ? 1 : 0);
+  HX_CHECK_LAUNCH();
+}
+
+void launch_lift(cudaStream_t s, const float* x, const float* feat, __nv_bfloat16* X, int64_t nn) {
+  k_lift<<<vec_blocks(nn), 256, 0, s>>>(x, feat, X, nn);
+  HX_CHECK_LAUNCH();
+}
+
+void launch_unlift(cudaStream_t s, const __nv_bfloat16* Y, const float* feat, float* acc,
+                   bool accumulate, int64_t nn) {
+  k_unlift<<<vec_blocks(nn), 256, 0, s>>>(Y, feat, acc, accumulate ? 1 : 0, nn);
   HX_CHECK_LAUNCH();
 }
 
 void launch_net_output(cudaStream_t s, const double* r, const double* minv, const double* dinvs,
-                       const float* feat, const __nv_bfloat16* Y, CgState* st, double scale_mul,
-                       double* z, const double* q_old, double* partials, int64_t nn) {
-  k_net_output<<<vec_blocks(nn), 256, 0, s>>>(r, minv, dinvs, feat, Y, st, scale_mul, z, q_old,
-                                              partials, nn);
+                       const float* t, CgState* st, double scale_mul, double* z,
+                       const double* q_old, double* partials, int64_t n) {
+  k_net_output<<<vec_blocks(n), 256, 0, s>>>(r, minv, dinvs, t, st, scale_mul, z, q_old,
+                                              partials, n);
   HX_CHECK_LAUNCH();
 }
 

@@ -12,7 +12,9 @@ struct GridN {  // node grid of the network (nodes per axis)
 
 constexpr int NET_LAYERS = 4;
 constexpr int NET_LAYER_PARAMS = 27 * 256;  // weights [27 taps][16 co][16 ci], no bias
-constexpr int NET_PARAMS = NET_LAYERS * NET_LAYER_PARAMS;
+constexpr int NET_NET_PARAMS = NET_LAYERS * NET_LAYER_PARAMS;  // one network
+constexpr int NET_NETS = 3;        // networks on node-grid levels 1 .. NET_NETS
+constexpr int NET_PARAMS = NET_NETS * NET_NET_PARAMS;
 constexpr int NET_IN = 6;  // live input channels: D^-1/2 r / s and the same times the density
 
 size_t conv_num_tiles(const GridN& g);
@@ -25,12 +27,22 @@ void launch_conv3_wgrad(cudaStream_t s, const __nv_bfloat16* X, const __nv_bfloa
 void launch_adam(cudaStream_t s, float* w, float* m, float* v, const float* grad,
                  const unsigned char* live, int n, float lr, int step);
 void launch_pack_weights(cudaStream_t s, const float* w, __nv_bfloat16* wf, __nv_bfloat16* wb);
-void launch_net_lift(cudaStream_t s, const double* v, const double* dinvs, const float* feat,
-                     const CgState* sst, const CgState* lst, int mode, double scale_mul,
-                     __nv_bfloat16* X, int64_t nn);
+// x = k D^-1/2 v as an FP32 nodal field [node][3] (k by mode: 0 network input,
+// 1 energy-loss gradient, 2 residual-loss gradient)
+void launch_field_in(cudaStream_t s, const double* v, const double* dinvs, const CgState* sst,
+                     const CgState* lst, int mode, double scale_mul, float* x, int64_t n);
+// full-weighting restriction fine -> coarse node grid (ch 3 or 1), and its transpose
+void launch_restrict(cudaStream_t s, int ch, const float* in, float* out, const GridN& gf,
+                     const GridN& gc, bool normalise);
+void launch_prolong(cudaStream_t s, const float* coarse, float* fine, const GridN& gf,
+                    const GridN& gc, bool accumulate);
+// lifting E: [node][3] FP32 -> [node][16] BF16 (x, feat * x), and its transpose
+void launch_lift(cudaStream_t s, const float* x, const float* feat, __nv_bfloat16* X, int64_t nn);
+void launch_unlift(cudaStream_t s, const __nv_bfloat16* Y, const float* feat, float* acc,
+                   bool accumulate, int64_t nn);
 void launch_net_output(cudaStream_t s, const double* r, const double* minv, const double* dinvs,
-                       const float* feat, const __nv_bfloat16* Y, CgState* st, double scale_mul,
-                       double* z, const double* q_old, double* partials, int64_t nn);
+                       const float* t, CgState* st, double scale_mul, double* z,
+                       const double* q_old, double* partials, int64_t n);
 void launch_net_aloss(cudaStream_t s, const double* d, const double* q, const double* e,
                       const double* r, int64_t n, double* partials, CgState* st, double* out);
 void launch_sqrt(cudaStream_t s, const double* a, double* b, int64_t n);

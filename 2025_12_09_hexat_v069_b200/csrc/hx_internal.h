@@ -193,14 +193,17 @@ struct hx_ctx {
 
   int64_t launches = 0;  // kernels launched on behalf of this context
 
-  // convolutional preconditioner network (see hx_net.cu)
+  // convolutional preconditioner networks (see hx_net.cu)
   struct Net {
     bool ready = false;
     int step = 0;  // Adam steps taken
-    hx::DevBuf<float> w, m, v, grad, part, feat;
+    hx::DevBuf<float> w, m, v, grad, part;
     hx::DevBuf<unsigned char> live;
-    hx::DevBuf<__nv_bfloat16> wf, wb, x0, y, da, db;
-    hx::DevBuf<__nv_bfloat16> act[7];  // G activations A1 A2 A3 H, then G^T's B3 B2 B1
+    hx::DevBuf<__nv_bfloat16> wf, wb, da, db, tmp[2];
+    struct Level {  // one node-grid level (0 = the mesh's node grid)
+      hx::DevBuf<float> x, acc, gx, feat;  // [node][3] fields, [node] feature
+      hx::DevBuf<__nv_bfloat16> x0, y, act[7];  // network input, output, training activations
+    } lv[4];
     hx::DevBuf<double> dinvs, z, scal, facbuf;
     const double* fac_last = nullptr;  // factors the operator inputs were built for
   } net;

@@ -688,6 +688,8 @@ hx_status time_kernel(hx_ctx* c, int kernel, int reps, double* avg_ms) {
                                           c->f_compat_last);
     const Grid fg = c->fg;
     body = [&, F, fg] { launch_filter_matvec(c->stream, c->f_p.p, c->f_q.p, fg, F, st, c->d_partials.p); };
+  } else if (kernel == HX_KERNEL_CONV3 || kernel == HX_KERNEL_NET_APPLY) {
+    body = net_time_body(c, kernel == HX_KERNEL_CONV3 ? 0 : 1);
   } else {
     throw Error{HX_BAD_ARG, "unknown kernel id"};
   }

@@ -26,9 +26,13 @@ void net_set_params(hx_ctx* c, const float* params);
 void net_get_params(hx_ctx* c, float* params);
 void net_forward_backward(hx_ctx* c, int nx, int ny, int nz, const float* x0, const float* dy,
                           float* y, float* grads);
-double net_train_step(hx_ctx* c, const double* r, const double* e, double lr, int loss_kind);
+double net_train_step(hx_ctx* c, const double* const* r, const double* const* e, int count,
+                      double lr, int loss_kind);
 void net_prepare(hx_ctx* c, const double* fac);
 void net_apply_vec(hx_ctx* c, const double* r, double* z);
+// Timing bodies on the prepared network: 0 = one 16 -> 16 conv layer on the
+// node grid, 1 = one preconditioner application (lift, 8 layers, output).
+std::function<void()> net_time_body(hx_ctx* c, int which);
 CgState solve_learned(hx_ctx* c, const double* fac, const double* b, double* x, bool warm,
                       double shift, const hx_solve_opts& o, double t0, bool* timed_out,
                       int* fallback, int* iters_out);

@@ -1,0 +1,126 @@
+"""Training and loading of the learned preconditioner.
+
+The network and its training kernels live in the library (hx_net_*); this
+module drives them.  It generates residual/error pairs from the library's
+own Jacobi-PCG, on seeded problems built like the scale workload:
+cantilever clamp, line load, i.i.d. uniform element densities smoothed by
+the Helmholtz filter (r = 3), mapped to [1e-3, 1], SIMP p = 3.  Per problem:
+  1. solve to rtol 1e-11 for u*;
+  2. record `snaps` Jacobi-PCG iterates x_k spread over a solve to rtol 1e-8;
+  3. take `steps` Adam steps, each on the summed gradient of `batch` random
+     pairs r = b - K x_k, e = u* - x_k (energy-norm loss).
+The trained parameters are stored as a float32 .npy of HX_NET_PARAMS values.
+"""
+import os
+
+import numpy as np
+
+from . import workloads as W
+
+WEIGHTS_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights")
+DEFAULT_WEIGHTS = os.path.join(WEIGHTS_DIR, "spd_cnn_128x64x64.npy")
+
+
+def problem(ctx, dims, seed, radius=3.0):
+    """(f, fac) device tensors of one seeded problem; sets the grid and BCs."""
+    import torch
+    nx, ny, nz = dims
+    _, _, bc, f = W.cantilever(nx, ny, nz, with_elements=False)
+    ctx.set_grid(nx, ny, nz)
+    ctx.set_material(1.0, 0.3)
+    ctx.set_bc(bc)
+    raw = W.raw_density(nx * ny * nz, seed)
+    rho_f, _ = ctx.filter(raw, radius, 0, 1e-5, 200)
+    fac = W.simp(W.map_density(rho_f, 1e-3), 3.0, 1.0, 1e-9)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    return torch.from_numpy(f).to(dev), torch.from_numpy(fac).to(dev)
+
+
+def _solve(ctx, hx, f, fac, **kw):
+    import torch
+    u = torch.zeros_like(f)
+    rep = ctx.solve_device(f.data_ptr(), fac.data_ptr(), u.data_ptr(),
+                           opts=hx.default_opts(**kw), ok=(0, 1, 3, 4, 9))
+    return u, rep
+
+
+def train(ctx, dims=(128, 64, 64), problems=20, snaps=128, steps=100, batch=8,
+          lr=(3e-4, 1e-4), seed0=1000, init_seed=5, log=None):
+    """Train from a fresh initialisation; returns (params, losses).  The
+    learning rate steps from lr[0] to lr[1] halfway through."""
+    import importlib
+    import torch
+    hx = importlib.import_module(__package__)
+    ctx.net_init(seed=init_seed)
+    losses = []
+    rng = np.random.default_rng(seed0)
+    total = problems * steps
+    for p in range(problems):
+        f, fac = problem(ctx, dims, seed0 + p)
+        n = f.numel()
+        u_star, _ = _solve(ctx, hx, f, fac, tol=1e-11, max_iter=1000000)
+        _, rj = _solve(ctx, hx, f, fac, tol=1e-8, max_iter=1000000)
+        every = max(2, 2 * int(np.ceil(rj.iterations / (2.0 * snaps))))
+        X = torch.zeros((snaps, n), dtype=torch.float64, device=f.device)
+        taken = ctx.pcg_snapshots(f.data_ptr(), fac.data_ptr(), every, snaps, 1e-8, X.data_ptr())
+        ctx.net_prepare(fac.data_ptr())
+        R = torch.empty((batch, n), dtype=torch.float64, device=f.device)
+        E = torch.empty_like(R)
+        for s in range(steps):
+            ks = rng.integers(taken, size=batch)
+            for b, k in enumerate(ks):
+                ctx.residual_device(f.data_ptr(), fac.data_ptr(), X[k].data_ptr(), R[b].data_ptr())
+                torch.sub(u_star, X[k], out=E[b])
+            torch.cuda.current_stream().synchronize()
+            rate = lr[0] if len(losses) < total // 2 else lr[1]
+            losses.append(ctx.net_train_batch([R[b].data_ptr() for b in range(batch)],
+                                              [E[b].data_ptr() for b in range(batch)], rate, 0))
+        if log:
+            log(f"problem {p}: jacobi {rj.iterations} its to 1e-8, {taken} snapshots, "
+                f"loss {np.mean(losses[-steps:]):.4f}")
+        del X, R, E
+    return ctx.net_get_params(), np.array(losses)
+
+
+def save_params(path, params):
+    os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+    np.save(path, np.asarray(params, np.float32))
+
+
+def load_params(path=DEFAULT_WEIGHTS):
+    p = np.load(path)
+    if p.dtype != np.float32 or p.ndim != 1:
+        raise ValueError(f"{path}: expected a flat float32 array")
+    return p
+
+
+def load_into(ctx, path=DEFAULT_WEIGHTS):
+    """Load trained parameters into the context's network."""
+    ctx.net_set_params(load_params(path))
+
+
+def main(argv=None):
+    """Regenerate the default weights: python -m <package>.learned [--out PATH]."""
+    import argparse
+    import importlib
+    import time
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--out", default=DEFAULT_WEIGHTS)
+    ap.add_argument("--problems", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--batch", type=int, default=8)
+    ap.add_argument("--lr", type=float, default=3e-4)
+    a = ap.parse_args(argv)
+    hx = importlib.import_module(__package__)
+    t0 = time.time()
+    with hx.Context(0) as ctx:
+        params, losses = train(ctx, problems=a.problems, steps=a.steps, batch=a.batch,
+                               lr=(a.lr, a.lr / 3),
+                               log=lambda m: print(f"[{time.time() - t0:.0f}s] {m}", flush=True))
+    save_params(a.out, params)
+    print(f"{len(losses)} Adam steps, loss {losses[:50].mean():.4f} -> {losses[-50:].mean():.4f}; "
+          f"saved {a.out}")
+
+
+if __name__ == "__main__":
+    main()

@@ -271,24 +271,28 @@ HX_API hx_status hx_oc_update(hx_ctx *ctx, int32_t dtype, const void *x,
                               int32_t *steps);
 
 /* ---- learned preconditioner -----------------------------------------------------
- * No reference counterpart.  A 3D CNN G on the node grid (4 conv3d layers,
- * 3x3x3, no bias, 6 -> 16 -> 16 -> 16 -> 16 channels, BF16 weights and
- * activations, FP32 accumulation on the tensor cores) defines the
- * preconditioner  z = D^-1/2 (I + E^T G^T G E) D^-1/2 r,  E the lifting
- * v -> (v, density * v) per node and G^T the transposed convolutions.  It is
- * symmetric positive definite for every choice of weights; zero weights
- * give Jacobi.  hx_solve with preconditioner HX_PC_LEARNED applies it in
- * flexible CG (Notay, one stored direction) and falls back to Jacobi-PCG from
- * the current iterate on breakdown or stagnation (report->fallback_used).
- * Parameters: HX_NET_PARAMS floats, 4 layers of [27 taps][16 out][16 in]
- * weights; the input channels >= 6 of the first layer are forced to zero. */
-#define HX_NET_PARAMS (4 * 27 * 256)
+ * No reference counterpart.  z = D^-1/2 (I + sum_l R_l^T E_l^T G_l^T G_l E_l R_l) D^-1/2 r
+ * for l = 1, 2, 3: R_l restricts a nodal field to node-grid level l (each
+ * level halves the grid, full weighting) and R_l^T is its exact transpose;
+ * E_l lifts a field to 6 channels (x, density * x); G_l is a 3D CNN of 4
+ * conv3d layers (3x3x3, no bias, 6 -> 16 -> 16 -> 16 -> 16 channels, BF16
+ * weights and activations, FP32 accumulation on the tensor cores) and G_l^T
+ * its transposed convolutions.  Symmetric positive definite for every choice
+ * of weights; zero weights give Jacobi.  hx_solve with preconditioner
+ * HX_PC_LEARNED applies it in flexible CG (Notay, one stored direction) and
+ * falls back to Jacobi-PCG from the current iterate on breakdown or
+ * stagnation (report->fallback_used).
+ * Parameters: HX_NET_PARAMS floats, the 3 networks one after the other, each
+ * 4 layers of [27 taps][16 out][16 in] weights; input channels >= 6 of each
+ * first layer are forced to zero. */
+#define HX_NET_PARAMS (3 * 4 * 27 * 256)
 HX_API hx_status hx_net_init(hx_ctx *ctx, uint64_t seed);
 HX_API hx_status hx_net_set_params(hx_ctx *ctx, const float *params);
 HX_API hx_status hx_net_get_params(hx_ctx *ctx, float *params);
-/* y = G^T G x0 on an nx*ny*nz NODE grid from host arrays [node][16] (FP32,
- * rounded to BF16; channels >= 6 of x0 and dy are ignored, those of y are
- * zero) and grads = d<dy, y>/dparams (gradient check). */
+/* y = G^T G x0 with the FIRST network on an nx*ny*nz NODE grid from host
+ * arrays [node][16] (FP32, rounded to BF16; channels >= 6 of x0 and dy are
+ * ignored, those of y are zero) and grads = d<dy, y>/dparams (HX_NET_PARAMS
+ * values, zero for the other networks; gradient check). */
 HX_API hx_status hx_net_forward_backward(hx_ctx *ctx, int32_t nx, int32_t ny,
                                          int32_t nz, const float *x0,
                                          const float *dy, float *y,
@@ -307,6 +311,12 @@ HX_API hx_status hx_net_apply(hx_ctx *ctx, const double *r_dev, double *z_dev);
 HX_API hx_status hx_net_train_step(hx_ctx *ctx, const double *r_dev,
                                    const double *e_dev, double lr,
                                    int32_t loss_kind, double *loss);
+/* The same over a batch: the gradients of `count` pairs (arrays of device
+ * pointers; e_devs may be NULL for loss_kind 1) are summed before one Adam
+ * step; *loss = their mean loss. */
+HX_API hx_status hx_net_train_batch(hx_ctx *ctx, const double *const *r_devs,
+                                    const double *const *e_devs, int32_t count,
+                                    double lr, int32_t loss_kind, double *loss);
 /* FP64 Jacobi-PCG from zero on (f, fac) storing the iterate every `every`
  * (even) iterations into snaps_dev[count][3*nodes] until rtol `tol`;
  * *taken = snapshots stored.  Training data for the network. */
@@ -329,7 +339,9 @@ enum {
   HX_KERNEL_PCG_UPDATE_FP64 = 1, /* r update + r.z, r.r reductions */
   HX_KERNEL_APPLY_FP64 = 2,      /* plain K.x */
   HX_KERNEL_PCG_STEP_FP32 = 3,
-  HX_KERNEL_FILTER_MATVEC = 4
+  HX_KERNEL_FILTER_MATVEC = 4,
+  HX_KERNEL_CONV3 = 5,           /* one 16 -> 16 BF16 conv3d layer on the node grid */
+  HX_KERNEL_NET_APPLY = 6        /* one learned-preconditioner application */
 };
 HX_API hx_status hx_time_kernel(hx_ctx *ctx, int32_t kernel, int32_t reps,
                                 double *avg_ms);

@@ -1,15 +1,19 @@
-"""The learned preconditioner P = D^-1/2 (I + E^T G^T G E) D^-1/2: the BF16
-tensor-core convolutions of G and G^T and the weight gradient checked
-against a CPU reference built on torch (FP32 arithmetic with the kernels'
-BF16 roundings of weights, activations and gradients); P symmetric positive
-definite; training on solver-generated residual/error pairs; flexible CG
-with the trained network against plain Jacobi-PCG; the fallback path."""
+"""The learned preconditioner
+P = D^-1/2 (I + sum_l R_l^T E_l^T G_l^T G_l E_l R_l) D^-1/2  (levels 1-3):
+the BF16 tensor-core convolutions of G and G^T and the weight gradient, and
+the whole application of P, checked against a CPU reference built on torch
+(FP32 arithmetic with the kernels' BF16 roundings of weights, activations
+and gradients); P symmetric positive definite; training on solver-generated
+residual/error pairs; flexible CG with the trained networks against plain
+Jacobi-PCG; the fallback path."""
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
 
 LP = 27 * 256
+NP = 4 * LP       # one network
+NETS = 3          # networks on node-grid levels 1..3
 NET_IN = 6
 
 
@@ -18,10 +22,29 @@ def _bf(a):
     return a.to(torch.bfloat16).to(torch.float32)
 
 
+def _weights(params, k):
+    """BF16-rounded conv weights of network k as torch [co][ci][kz][ky][kx]."""
+    import torch
+    return [_bf(torch.from_numpy(params[k * NP + l * LP:k * NP + (l + 1) * LP].reshape(27, 16, 16))
+                .permute(1, 2, 0).reshape(16, 16, 3, 3, 3)) for l in range(4)]
+
+
+def _gtg(W, x):
+    """G^T G x with BF16 rounding of every layer output (x: [1, 16, z, y, x])."""
+    import torch.nn.functional as F
+    a = [x]
+    for l in range(4):
+        a.append(_bf(F.conv3d(a[-1], W[l], padding=1)))
+    b = {4: a[4]}
+    for l in (3, 2, 1, 0):
+        b[l] = _bf(F.conv_transpose3d(b[l + 1], W[l], padding=1))
+    return a, b
+
+
 def _torch_reference(params, dims, x0, dy):
-    """y = G^T G x0 and d<dy, y>/dW in torch (CPU, FP32), rounding to BF16
-    where the GPU kernels store BF16: every layer output, forward and
-    backward."""
+    """y = G^T G x0 and d<dy, y>/dW for network 0 in torch (CPU, FP32),
+    rounding to BF16 where the GPU kernels store BF16: every layer output,
+    forward and backward."""
     import torch
     import torch.nn.functional as F
     nx, ny, nz = dims
@@ -32,17 +55,11 @@ def _torch_reference(params, dims, x0, dy):
     def unvol(t):
         return t[0].permute(1, 2, 3, 0).reshape(-1, 16).numpy()
 
-    W = [_bf(torch.from_numpy(params[l * LP:(l + 1) * LP].reshape(27, 16, 16))
-             .permute(1, 2, 0).reshape(16, 16, 3, 3, 3)) for l in range(4)]  # [co][ci][kz][ky][kx]
+    W = _weights(params, 0)
     conv = lambda x, l: _bf(F.conv3d(x, W[l], padding=1))
     convT = lambda x, l: _bf(F.conv_transpose3d(x, W[l], padding=1))
     wgrad = lambda X, D: torch.nn.grad.conv3d_weight(X, W[0].shape, D, padding=1)
-    a = [_bf(vol(x0))]
-    for l in range(4):
-        a.append(conv(a[-1], l))          # A1 A2 A3 H
-    b = {4: a[4]}
-    for l in (3, 2, 1, 0):
-        b[l] = convT(b[l + 1], l)         # B3 B2 B1 B0
+    a, b = _gtg(W, _bf(vol(x0)))
     gw = [torch.zeros_like(W[0]) for _ in range(4)]
     e = _bf(vol(dy))
     for l in range(4):                    # transposed uses: X = dLoss/dout, D = input
@@ -66,7 +83,7 @@ def test_conv_stack_and_gradient_match_torch(ctx):
     p = (p + rng.normal(0, 0.02, p.size).astype(np.float32))
     ctx.net_set_params(p)
     p = ctx.net_get_params()  # unused input channels forced to zero
-    assert not p.reshape(4, 27, 16, 16)[0, :, :, NET_IN:].any()
+    assert not p.reshape(NETS, 4, 27, 16, 16)[:, 0, :, :, NET_IN:].any()
     x0 = np.zeros((nn_, 16), np.float32)
     x0[:, :NET_IN] = rng.standard_normal((nn_, NET_IN))
     dy = np.zeros((nn_, 16), np.float32)
@@ -80,7 +97,7 @@ def test_conv_stack_and_gradient_match_torch(ctx):
         a, b = g[l * LP:(l + 1) * LP], gr[l * LP:(l + 1) * LP]
         assert np.abs(a - b).max() <= 3e-2 * np.abs(b).max(), l
         assert np.abs(a - b).mean() <= 3e-3 * np.abs(b).max(), l
-    assert np.isfinite(g).all()
+    assert np.isfinite(g).all() and not g[NP:].any()
 
 
 def _problem(ctx, hx, dims, seed):
@@ -95,6 +112,92 @@ def _problem(ctx, hx, dims, seed):
     fac = W.simp(W.map_density(rho_f, 1e-3))
     dev = torch.device("cuda", 0)
     return torch.from_numpy(f).to(dev), torch.from_numpy(fac).to(dev)
+
+
+def _restrict(x, normalise=False):
+    """Full weighting (1/2, 1, 1/2 per axis) onto the next coarser node grid."""
+    import torch
+    import torch.nn.functional as F
+    w1 = torch.tensor([0.5, 1.0, 0.5])
+    k = (w1[:, None, None] * w1[None, :, None] * w1[None, None, :])[None, None]
+    C = x.shape[1]
+    out = F.conv3d(x, k.expand(C, 1, 3, 3, 3).to(x.dtype), stride=2, padding=1, groups=C)
+    if normalise:
+        out = out / F.conv3d(torch.ones_like(x[:, :1]), k.to(x.dtype), stride=2, padding=1)
+    return out
+
+
+def _prolong(x, fine_shape):
+    """Exact transpose of _restrict (no normalisation)."""
+    import torch
+    import torch.nn.functional as F
+    w1 = torch.tensor([0.5, 1.0, 0.5])
+    k = (w1[:, None, None] * w1[None, :, None] * w1[None, None, :])[None, None]
+    C = x.shape[1]
+    op = tuple(fine_shape[i] - 2 * x.shape[2 + i] + 1 for i in range(3))
+    return F.conv_transpose3d(x, k.expand(C, 1, 3, 3, 3).to(x.dtype), stride=2, padding=1,
+                              output_padding=op, groups=C)
+
+
+def _torch_precond(params, dims, fac, minv, r):
+    """P r restated in torch from the preconditioner's definition."""
+    import torch
+    nx, ny, nz = dims
+    nz1, ny1, nx1 = nz + 1, ny + 1, nx + 1
+    dinvs = np.sqrt(minv)
+    n = r.size
+    s = np.sqrt(float(r @ (minv * r)) / n)
+    x = torch.from_numpy((dinvs * r / s).astype(np.float32)).reshape(nz1, ny1, nx1, 3)
+    x = x.permute(3, 0, 1, 2)[None]
+    # nodal density feature: mean over the node's elements of clip((log10 f + 9) / 9)
+    v = np.clip((np.log10(np.maximum(fac, 1e-12)) + 9.0) / 9.0, 0.0, 1.0).reshape(nz, ny, nx)
+    vp = np.pad(v, 1)
+    cp = np.pad(np.ones_like(v), 1)
+    ssum = sum(vp[a:a + nz1, b:b + ny1, c:c + nx1] for a in (0, 1) for b in (0, 1) for c in (0, 1))
+    cnt = sum(cp[a:a + nz1, b:b + ny1, c:c + nx1] for a in (0, 1) for b in (0, 1) for c in (0, 1))
+    feat = [torch.from_numpy((ssum / cnt).astype(np.float32))[None, None]]
+    xs = [x]
+    for l in range(1, NETS + 1):
+        feat.append(_restrict(feat[-1], True))
+        xs.append(_restrict(xs[-1]))
+    acc = None
+    for l in range(NETS, 0, -1):
+        X0 = torch.zeros((1, 16) + xs[l].shape[2:])
+        X0[:, :3] = _bf(xs[l])
+        X0[:, 3:6] = _bf(xs[l] * feat[l])
+        _, b = _gtg(_weights(params, l - 1), X0)
+        t = b[0][:, :3] + feat[l] * b[0][:, 3:6]
+        acc = t if acc is None else t + _prolong(acc, xs[l].shape[2:])
+    acc = _prolong(acc, xs[0].shape[2:])
+    corr = acc[0].permute(1, 2, 3, 0).reshape(-1).double().numpy()
+    return minv * r + s * dinvs * corr, minv * r
+
+
+def test_full_preconditioner_matches_torch(ctx, hx):
+    import torch
+    dims = (22, 9, 7)  # odd and even node counts on the levels
+    f_d, fac_d = _problem(ctx, hx, dims, seed=6)
+    ctx.solve_device(f_d.data_ptr(), fac_d.data_ptr(), torch.zeros_like(f_d).data_ptr(),
+                     opts=hx.default_opts(tol=1e-2))
+    ctx.net_init(seed=21)
+    p = ctx.net_get_params()
+    rng = np.random.default_rng(2)
+    ctx.net_set_params(p * 2.0 + rng.normal(0, 0.01, p.size).astype(np.float32))
+    p = ctx.net_get_params()
+    ctx.net_prepare(fac_d.data_ptr())
+    fac = fac_d.cpu().numpy()
+    bc = hx.workloads.cantilever(*dims, with_elements=False)[2].reshape(-1)
+    diag = ctx.diagonal(fac, f_d.numel())
+    minv = np.where(bc > 0, 0.0, 1.0 / diag)
+    r = rng.standard_normal(f_d.numel()) * (bc == 0)
+    z = torch.empty_like(f_d)
+    ctx.net_apply(torch.from_numpy(r).to(f_d.device).data_ptr(), z.data_ptr())
+    z = z.cpu().numpy()
+    zr, jac = _torch_precond(p, dims, fac, minv, r)
+    corr = np.linalg.norm(zr - jac)
+    assert corr > 0.1 * np.linalg.norm(jac)  # the networks contribute
+    assert np.linalg.norm(z - zr) <= 2e-2 * corr
+    assert np.array_equal(z[bc > 0], np.zeros(int((bc > 0).sum())))
 
 
 def test_preconditioner_is_symmetric_positive_definite(ctx, hx):
@@ -189,3 +292,50 @@ def test_poisoned_network_falls_back_to_jacobi(ctx, hx):
                           opts=hx.default_opts(tol=1e-6, preconditioner=1, max_iter=20000))
     assert rl.fallback_used == 1
     assert rl.status == 0 and rl.true_rel_res < 1e-6
+
+
+def test_batch_step_sums_single_gradients(ctx, hx):
+    """A batch of two copies of one pair: same loss as the single step, and
+    the Adam step of the summed gradient equals the single one (Adam is
+    invariant to the gradient's scale up to its epsilon)."""
+    import torch
+    dims = (20, 8, 6)
+    f_d, fac_d = _problem(ctx, hx, dims, seed=12)
+    x = torch.zeros_like(f_d)
+    ctx.solve_device(f_d.data_ptr(), fac_d.data_ptr(), x.data_ptr(),
+                     opts=hx.default_opts(tol=1e-2))
+    u_star = torch.zeros_like(f_d)
+    ctx.solve_device(f_d.data_ptr(), fac_d.data_ptr(), u_star.data_ptr(),
+                     opts=hx.default_opts(tol=1e-10, max_iter=100000))
+    r = torch.empty_like(f_d)
+    ctx.residual_device(f_d.data_ptr(), fac_d.data_ptr(), x.data_ptr(), r.data_ptr())
+    e = (u_star - x).contiguous()
+    ctx.net_init(seed=4)
+    ctx.net_prepare(fac_d.data_ptr())
+    l1 = ctx.net_train_step(r.data_ptr(), e.data_ptr(), 1e-3)
+    p1 = ctx.net_get_params()
+    ctx.net_init(seed=4)
+    l2 = ctx.net_train_batch([r.data_ptr(), r.data_ptr()], [e.data_ptr(), e.data_ptr()], 1e-3)
+    p2 = ctx.net_get_params()
+    assert l1 == l2
+    assert np.abs(p1 - p2).max() <= 1e-6 * np.abs(p1).max()
+
+
+def test_shipped_weights_gain_on_unseen_problem(ctx, hx):
+    """The committed networks (trained on 128x64x64 problems) on an unseen
+    seeded problem of another size: FCG converges on the true residual in
+    well under half of Jacobi-PCG's iterations."""
+    import torch
+    from importlib import import_module
+    learned = import_module(hx.__name__ + ".learned")
+    f_d, fac_d = learned.problem(ctx, (96, 48, 48), seed=77)
+    rj = ctx.solve_device(f_d.data_ptr(), fac_d.data_ptr(), torch.zeros_like(f_d).data_ptr(),
+                          opts=hx.default_opts(tol=1e-6, max_iter=100000))
+    learned.load_into(ctx)
+    u = torch.zeros_like(f_d)
+    rl = ctx.solve_device(f_d.data_ptr(), fac_d.data_ptr(), u.data_ptr(),
+                          opts=hx.default_opts(tol=1e-6, preconditioner=1, max_iter=100000))
+    print(f"96x48x48: jacobi-pcg {rj.iterations} its; learned fcg {rl.iterations} its "
+          f"(fallback {rl.fallback_used})")
+    assert rl.status == 0 and rl.true_rel_res < 1e-6 and rl.fallback_used == 0
+    assert rl.iterations * 2 < rj.iterations
