@@ -1,21 +1,16 @@
 // hx_cnn.cu -- 3D convolutional preconditioner network on the node grid:
-// BF16 implicit-GEMM conv3d (3x3x3, 16 input channels, no bias) on the
-// tensor cores with FP32 accumulation, its transpose (the backward-data
-// pass), the weight gradient, Adam, and the input/output assembly around a
-// Krylov solver.
+// the weight gradient of the BF16 conv3d layers (3x3x3, 16 channels, no
+// bias; the convolution itself is in hx_conv_tc.cu), Adam, the grid
+// transfers between levels, and the input/output assembly around a Krylov
+// solver.
 //
 // Activations are channels-last BF16, [node][16] (32 bytes per node, node
-// numbering of the grid).  A conv layer is a GEMM per CTA tile: M = 512
-// nodes (16 x 8 x 4), N = output channels, K = 27 taps x 16 channels; each
-// warp owns four 16-node x-rows and issues one m16n8k16 MMA per (row, tap,
-// 8 output channels).  The input tile with its one-node halo (18 x 10 x 6
-// nodes) and the layer's weights are staged with 16-byte cp.async; the A
-// fragment of a shifted tap is loaded with ldmatrix from the shifted rows,
-// the 16-byte halves of each node are XOR-swizzled so the 8 rows of a
-// matrix hit distinct banks.  The backward-data pass is the same kernel with
-// the taps flipped and each tap's weights transposed; the weight gradient
-// is a per-CTA tensor-core reduction over the tile's nodes (one tap per
-// warp at a time) summed across CTAs in a fixed order.
+// numbering of the grid).  The weight gradient of a layer is a per-CTA
+// tensor-core reduction (mma.sync m16n8k16) over a 16 x 8 x 4 node tile:
+// the input tile with its one-node halo (18 x 10 x 6 nodes) and the output
+// gradient tile are staged with 16-byte cp.async, the 16-byte halves of each
+// node XOR-swizzled so that the 8 rows of an ldmatrix hit distinct banks;
+// one tap per warp at a time; partials summed across CTAs in a fixed order.
 #include <cuda_bf16.h>
 
 #include "hx_cnn.h"
@@ -40,19 +35,9 @@ __device__ __forceinline__ void cp16(unsigned dst, const void* src, bool ok) {
 __device__ __forceinline__ void cp_commit_wait() {
   asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::);
 }
-__device__ __forceinline__ void ldsm_x4(unsigned addr, unsigned (&r)[4]) {
-  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-               : "r"(addr));
-}
 __device__ __forceinline__ void ldsm_x4_t(unsigned addr, unsigned (&r)[4]) {
   asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-               : "r"(addr));
-}
-__device__ __forceinline__ void ldsm_x2(unsigned addr, unsigned (&r)[2]) {
-  asm volatile("ldmatrix.sync.aligned.m8n8.x2.shared.b16 {%0,%1}, [%2];\n"
-               : "=r"(r[0]), "=r"(r[1])
                : "r"(addr));
 }
 __device__ __forceinline__ void mma16816(float (&d)[4], const unsigned (&a)[4], unsigned b0,
@@ -69,108 +54,7 @@ __device__ __forceinline__ unsigned swz(int row, int h) {
   return (unsigned)(row * 32 + ((h ^ ((row >> 2) & 1)) << 4));
 }
 
-struct ConvSmem {
-  __nv_bfloat16 x[HNODES * C];  // 34,560 B
-  __nv_bfloat16 w[27 * 16 * C]; // 13,824 B, per tap [co][ci]
-};
-
-// Stage the input tile (with halo) and the layer weights.
-__device__ __forceinline__ void stage_tile(ConvSmem& sm, const __nv_bfloat16* __restrict__ X,
-                                           const __nv_bfloat16* __restrict__ W, int cout,
-                                           const GridN& g, int x0, int y0, int z0) {
-  const unsigned xb = su32(sm.x), wb = su32(sm.w);
-  for (int ch = threadIdx.x; ch < HNODES * 2; ch += NTHREADS) {
-    const int node = ch >> 1, h = ch & 1;
-    const int hx = node % HX_, r = node / HX_;
-    const int hy = r % HY, hz = r / HY;
-    const int gx = x0 - 1 + hx, gy = y0 - 1 + hy, gz = z0 - 1 + hz;
-    const bool ok = gx >= 0 && gy >= 0 && gz >= 0 && gx < g.nx && gy < g.ny && gz < g.nz;
-    const int64_t gn = ok ? ((int64_t)gz * g.ny + gy) * g.nx + gx : 0;
-    cp16(xb + swz(node, h), X + gn * C + h * 8, ok);
-  }
-  for (int ch = threadIdx.x; ch < 27 * cout * 2; ch += NTHREADS) {
-    const int row = ch >> 1, h = ch & 1;  // row = tap * cout + co
-    const int tap = row / cout, co = row - tap * cout;
-    cp16(wb + swz(tap * 16 + co, h), W + ((int64_t)tap * 16 + co) * C + h * 8, true);
-  }
-  cp_commit_wait();
-  __syncthreads();
-}
-
 }  // namespace
-
-// ---------------------------------------------------------------------------
-// Convolution and its transpose (zero padding at the grid boundary):
-// Y[n, co] = sum_{tap, ci} X[n + off(tap), ci] * W[tap][co][ci]
-// The transpose is this kernel on the flipped, per-tap transposed weights
-// (k_pack_weights).  COUT: 16 or 8 output channels (stored with stride COUT).
-// ---------------------------------------------------------------------------
-template <int COUT>
-__global__ void __launch_bounds__(NTHREADS) k_conv3(const __nv_bfloat16* __restrict__ X,
-                                                    __nv_bfloat16* __restrict__ Y,
-                                                    const __nv_bfloat16* __restrict__ W,
-                                                    GridN g) {
-  constexpr int NT = COUT / 8;
-  extern __shared__ __align__(128) unsigned char smraw[];
-  ConvSmem& sm = *reinterpret_cast<ConvSmem*>(smraw);
-  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = blockIdx.z * TZ;
-  stage_tile(sm, X, W, COUT, g, x0, y0, z0);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const unsigned xb = su32(sm.x), wb = su32(sm.w);
-  float acc[4][NT][4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int nt = 0; nt < NT; ++nt)
-#pragma unroll
-      for (int k = 0; k < 4; ++k) acc[i][nt][k] = 0.f;
-  // A rows this lane addresses: node x = (mi&1)*8 + lane%8, half = mi>>1
-  const int mi = lane >> 3;
-  const int ax = ((mi & 1) << 3) + (lane & 7), ah = mi >> 1;
-  for (int tap = 0; tap < 27; ++tap) {
-    const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
-    unsigned b[4];
-    if (COUT == 16) {
-      const int co = ((mi >> 1) << 3) + (lane & 7), h = mi & 1;
-      ldsm_x4(wb + swz(tap * 16 + co, h), b);
-    } else {
-      unsigned b2[2];
-      const int co = lane & 7, h = (lane >> 3) & 1;
-      ldsm_x2(wb + swz(tap * 16 + co, h), b2);
-      b[0] = b2[0];
-      b[1] = b2[1];
-    }
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int row = warp * 4 + i;  // 32 x-rows: y = row % 8, z = row / 8
-      const int hy = (row & 7) + 1 + dy, hz = (row >> 3) + 1 + dz;
-      const int hx = ax + 1 + dx;
-      unsigned a[4];
-      ldsm_x4(xb + swz((hz * HY + hy) * HX_ + hx, ah), a);
-      mma16816(acc[i][0], a, b[0], b[1]);
-      if (NT == 2) mma16816(acc[i][NT - 1], a, b[2], b[3]);
-    }
-  }
-  // epilogue: lane holds nodes x = lane/4 and lane/4 + 8, channels 2t, 2t+1
-  const int gq = lane >> 2, tq = lane & 3;
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int row = warp * 4 + i;
-    const int gy = y0 + (row & 7), gz = z0 + (row >> 3);
-#pragma unroll
-    for (int half = 0; half < 2; ++half) {
-      const int gx = x0 + gq + half * 8;
-      if (gx >= g.nx || gy >= g.ny || gz >= g.nz) continue;
-      const int64_t node = ((int64_t)gz * g.ny + gy) * g.nx + gx;
-#pragma unroll
-      for (int nt = 0; nt < NT; ++nt) {
-        const int co = nt * 8 + 2 * tq;
-        *reinterpret_cast<__nv_bfloat162*>(Y + node * COUT + co) =
-            __floats2bfloat162_rn(acc[i][nt][2 * half], acc[i][nt][2 * half + 1]);
-      }
-    }
-  }
-}
 
 // ---------------------------------------------------------------------------
 // Weight-gradient partials of one CTA tile:
@@ -275,44 +159,50 @@ __global__ void k_adam(float* __restrict__ w, float* __restrict__ m, float* __re
   w[k] -= lr * (mk / c1) / (sqrtf(vk / c2) + eps);
 }
 
-// Master FP32 parameters of one layer -> BF16 weights [27][16][16] and the
-// flipped/transposed weights [27][16 ci][16 co] of its backward-data pass.
+// Master FP32 parameters of one layer (W[tap][co][ci]) -> the BF16 B
+// operands of the tensor-core convolution, in its shared-memory order
+// [tap][plane][row][8] (plane = which 8 of the 16 reduced channels):
+// wf for the convolution (row = co, reduced over ci) and wb for its
+// transpose (tap flipped, row = ci, reduced over co).
 __global__ void k_pack_weights(const float* __restrict__ w, __nv_bfloat16* __restrict__ wf,
                                __nv_bfloat16* __restrict__ wb) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= 27 * 256) return;
   const int tap = k / 256, co = (k / 16) % 16, ci = k % 16;
   const __nv_bfloat16 v = __float2bfloat16_rn(w[k]);
-  wf[k] = v;
-  wb[(26 - tap) * 256 + ci * 16 + co] = v;
+  wf[((tap * 2 + (ci >> 3)) * 16 + co) * 8 + (ci & 7)] = v;
+  wb[(((26 - tap) * 2 + (co >> 3)) * 16 + ci) * 8 + (co & 7)] = v;
 }
 
 // ---------------------------------------------------------------------------
 // Solver <-> network glue (node grid, interleaved FP64 vectors)
 // ---------------------------------------------------------------------------
-// Scaled nodal field of a DOF vector: x[n][c] = k * dinvs[3n+c] * v[3n+c]
-// (FP32), with the coefficient k of `mode`:  0: 1/s (network input, s the
-// RMS of D^-1/2 r);  1: 2 s / (e.r) (energy-loss gradient);  2: 2 s /
-// (r.M^-1 r) (residual-loss gradient).  s from sst->rz; e.r from
-// lst->aux[0].
-__global__ void k_field_in(const double* __restrict__ v, const double* __restrict__ dinvs,
-                           const CgState* sst, const CgState* lst, int mode, double scale_mul,
-                           float* __restrict__ x, int64_t n) {
-  const double s = sqrt(sst->rz * scale_mul);
-  double k;
-  if (mode == 0) {
-    k = 1.0 / fmax(s, 1e-300);
-  } else {
-    const double den = (mode == 1) ? lst->aux[0] : sst->rz;
-    k = den > 0.0 ? 2.0 * s / den : 0.0;
-  }
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x)
-    x[i] = (float)(k * dinvs[i] * v[i]);
-}
-
 // 1D full-weighting factor of fine offset d = j - 2i (|d| <= 1)
 __device__ __forceinline__ float fw(int d) { return d == 0 ? 1.f : 0.5f; }
+
+// Per axis, the coarse nodes i with |f - 2i| <= 1 and their weights
+// (floor(f/2), and for odd f also f/2 + 1; weight 0 past the coarse grid).
+__device__ __forceinline__ void prolong_axis(int f, int nc, int (&i)[2], float (&w)[2]) {
+  if ((f & 1) == 0) {
+    i[0] = f >> 1;
+    w[0] = 1.f;
+    i[1] = 0;
+    w[1] = 0.f;
+  } else {
+    i[0] = f >> 1;
+    w[0] = 0.5f;
+    i[1] = (f >> 1) + 1;
+    w[1] = 0.5f;
+    if (i[1] >= nc) {
+      i[1] = 0;
+      w[1] = 0.f;
+    }
+  }
+  if (i[0] >= nc) {
+    i[0] = 0;
+    w[0] = 0.f;
+  }
+}
 
 // Restriction to the next coarser node grid (coarse node i <-> fine node
 // 2i), full weighting (1/2, 1, 1/2) per axis, zero outside the grid:
@@ -354,6 +244,58 @@ __global__ void k_restrict(const float* __restrict__ in, float* __restrict__ out
   }
 }
 
+// Coefficient k of the scaled field x = k D^-1/2 v of `mode`:  0: 1/s
+// (network input, s the RMS of D^-1/2 r);  1: 2 s / (e.r) (energy-loss
+// gradient);  2: 2 s / (r.M^-1 r) (residual-loss gradient).  s from
+// sst->rz; e.r from lst->aux[0].
+__device__ __forceinline__ double field_coef(const CgState* sst, const CgState* lst, int mode,
+                                             double scale_mul) {
+  const double s = sqrt(sst->rz * scale_mul);
+  if (mode == 0) return 1.0 / fmax(s, 1e-300);
+  const double den = (mode == 1) ? lst->aux[0] : sst->rz;
+  return den > 0.0 ? 2.0 * s / den : 0.0;
+}
+
+// Level-1 field of a DOF vector in one pass: out = R (k D^-1/2 v) with
+// D^-1/2 = sqrt(minv) (0 on fixed DOFs), R the full-weighting restriction
+// of k_restrict; the scaled field on the mesh's node grid is never stored.
+// T: the precision of the solver's vectors; the field is FP32 (it feeds the
+// BF16 network), so it is formed in FP32 whatever T is.
+template <typename T>
+__global__ void k_restrict_dof(const T* __restrict__ v, const T* __restrict__ minv,
+                               const CgState* sst, const CgState* lst, int mode, double scale_mul,
+                               float* __restrict__ out, GridN gf, GridN gc) {
+  const double kc = field_coef(sst, lst, mode, scale_mul);
+  const int64_t nc = (int64_t)gc.nx * gc.ny * gc.nz;
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nc;
+       n += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(n % gc.nx);
+    const int64_t t = n / gc.nx;
+    const int j = (int)(t % gc.ny), k = (int)(t / gc.ny);
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+    for (int dz = -1; dz <= 1; ++dz) {
+      const int fz = 2 * k + dz;
+      if (fz < 0 || fz >= gf.nz) continue;
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int fy = 2 * j + dy;
+        if (fy < 0 || fy >= gf.ny) continue;
+        for (int dx = -1; dx <= 1; ++dx) {
+          const int fx = 2 * i + dx;
+          if (fx < 0 || fx >= gf.nx) continue;
+          const float w = fw(dz) * fw(dy) * fw(dx);
+          const int64_t f = 3 * (((int64_t)fz * gf.ny + fy) * gf.nx + fx);
+          a0 += w * sqrtf((float)minv[f + 0]) * (float)v[f + 0];
+          a1 += w * sqrtf((float)minv[f + 1]) * (float)v[f + 1];
+          a2 += w * sqrtf((float)minv[f + 2]) * (float)v[f + 2];
+        }
+      }
+    }
+    out[3 * n + 0] = (float)kc * a0;
+    out[3 * n + 1] = (float)kc * a1;
+    out[3 * n + 2] = (float)kc * a2;
+  }
+}
+
 // Prolongation, the exact transpose of k_restrict (without normalisation):
 // fine[j][c] = (accumulate ? fine[j][c] : 0) + sum_{i: |j - 2i| <= 1} w(j - 2i) coarse[i][c].
 __global__ void k_prolong(const float* __restrict__ coarse, float* __restrict__ fine, GridN gf,
@@ -364,22 +306,11 @@ __global__ void k_prolong(const float* __restrict__ coarse, float* __restrict__ 
     const int fx = (int)(n % gf.nx);
     const int64_t t = n / gf.nx;
     const int fy = (int)(t % gf.ny), fz = (int)(t / gf.ny);
-    // per axis: the coarse nodes i with |f - 2i| <= 1: floor(f/2) and, for odd f, f/2 + 1
     int ix[2], iy[2], iz[2];
     float wx[2], wy[2], wz[2];
-    auto axis = [](int f, int nc, int (&i)[2], float (&w)[2]) {
-      if ((f & 1) == 0) {
-        i[0] = f >> 1; w[0] = 1.f; i[1] = 0; w[1] = 0.f;
-      } else {
-        i[0] = f >> 1; w[0] = 0.5f;
-        i[1] = (f >> 1) + 1; w[1] = (i[1] < nc) ? 0.5f : 0.f;
-        if (i[1] >= nc) i[1] = 0;
-      }
-      if (i[0] >= nc) { i[0] = 0; w[0] = 0.f; }
-    };
-    axis(fx, gc.nx, ix, wx);
-    axis(fy, gc.ny, iy, wy);
-    axis(fz, gc.nz, iz, wz);
+    prolong_axis(fx, gc.nx, ix, wx);
+    prolong_axis(fy, gc.ny, iy, wy);
+    prolong_axis(fz, gc.nz, iz, wz);
     float a0 = 0.f, a1 = 0.f, a2 = 0.f;
 #pragma unroll
     for (int az = 0; az < 2; ++az)
@@ -444,22 +375,53 @@ __global__ void k_unlift(const __nv_bfloat16* __restrict__ Y, const float* __res
   }
 }
 
-// z = M^-1 r + s * dinvs * t  (t: the correction field on the fine node grid,
-// FP32 [node][3]; masked DOFs have minv = dinvs = 0).  With q_old: reduces
+// z = M^-1 r + s D^-1/2 (R^T t)  with t the level-1 correction field (FP32
+// [node][3]), R^T the prolongation of k_prolong computed on the fly and
+// D^-1/2 = sqrt(minv) (masked DOFs have minv = 0).  With q_old: reduces
 // z.q_old and sets the flexible-CG coefficient st->beta = -(z.q_old) /
-// (p_old.q_old) (0 without a previous step).
-__global__ void k_net_output(const double* __restrict__ r, const double* __restrict__ minv,
-                             const double* __restrict__ dinvs, const float* __restrict__ t,
-                             CgState* st, double scale_mul, double* __restrict__ z,
-                             const double* __restrict__ q_old, double* partials, int64_t n) {
+// (p_old.q_old) (0 without a previous step).  T: vector precision.
+template <typename T>
+__global__ void k_net_output(const T* __restrict__ r, const T* __restrict__ minv,
+                             const float* __restrict__ t, GridN gf, GridN gc, CgState* st,
+                             double scale_mul, T* __restrict__ z, const T* __restrict__ q_old,
+                             double* partials) {
   if (st->status != HX_RUNNING) return;
   const double s = sqrt(st->rz * scale_mul);
+  const int64_t nf = (int64_t)gf.nx * gf.ny * gf.nz;
   double zq = 0.0;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const double zi = minv[i] * r[i] + s * dinvs[i] * (double)t[i];
-    z[i] = zi;
-    if (q_old) zq += zi * q_old[i];
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nf;
+       n += (int64_t)gridDim.x * blockDim.x) {
+    const int fx = (int)(n % gf.nx);
+    const int64_t tt = n / gf.nx;
+    const int fy = (int)(tt % gf.ny), fz = (int)(tt / gf.ny);
+    int ix[2], iy[2], iz[2];
+    float wx[2], wy[2], wz[2];
+    prolong_axis(fx, gc.nx, ix, wx);
+    prolong_axis(fy, gc.ny, iy, wy);
+    prolong_axis(fz, gc.nz, iz, wz);
+    float a[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int az = 0; az < 2; ++az)
+#pragma unroll
+      for (int ay = 0; ay < 2; ++ay)
+#pragma unroll
+        for (int ax = 0; ax < 2; ++ax) {
+          const float w = wz[az] * wy[ay] * wx[ax];
+          if (w == 0.f) continue;
+          const int64_t c = 3 * (((int64_t)iz[az] * gc.ny + iy[ay]) * gc.nx + ix[ax]);
+          a[0] += w * t[c + 0];
+          a[1] += w * t[c + 1];
+          a[2] += w * t[c + 2];
+        }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int64_t i = 3 * n + c;
+      // the correction is BF16-accurate: its scale sqrt(minv) in FP32
+      const double m = (double)minv[i];
+      const T zi = (T)(m * (double)r[i] + s * (double)(sqrtf((float)minv[i]) * a[c]));
+      z[i] = zi;
+      if (q_old) zq += (double)zi * (double)q_old[i];
+    }
   }
   if (!q_old) return;
   double v[1] = {zq};
@@ -500,24 +462,6 @@ size_t conv_num_tiles(const GridN& g) {
   return (size_t)d.x * d.y * d.z;
 }
 
-void launch_conv3(cudaStream_t s, int cout, const __nv_bfloat16* X, __nv_bfloat16* Y,
-                  const __nv_bfloat16* W, const GridN& g) {
-  const size_t smem = sizeof(ConvSmem);
-  static bool cfg[2] = {false, false};
-  if (cout != 16 && cout != 8) throw Error{HX_BAD_ARG, "unsupported conv configuration"};
-  const int idx = cout == 16 ? 0 : 1;
-  if (!cfg[idx]) {
-    HX_CUDA(cudaFuncSetAttribute(cout == 16 ? k_conv3<16> : k_conv3<8>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    cfg[idx] = true;
-  }
-  if (cout == 16)
-    k_conv3<16><<<conv_grid(g), NTHREADS, smem, s>>>(X, Y, W, g);
-  else
-    k_conv3<8><<<conv_grid(g), NTHREADS, smem, s>>>(X, Y, W, g);
-  HX_CHECK_LAUNCH();
-}
-
 void launch_conv3_wgrad(cudaStream_t s, const __nv_bfloat16* X, const __nv_bfloat16* D,
                         float* part, float* grad, bool accumulate, const GridN& g) {
   const size_t smem = (HNODES + TX * TY * TZ) * C * sizeof(__nv_bfloat16);
@@ -548,11 +492,21 @@ void launch_pack_weights(cudaStream_t s, const float* w, __nv_bfloat16* wf, __nv
   HX_CHECK_LAUNCH();
 }
 
-void launch_field_in(cudaStream_t s, const double* v, const double* dinvs, const CgState* sst,
-                     const CgState* lst, int mode, double scale_mul, float* x, int64_t n) {
-  k_field_in<<<vec_blocks(n), 256, 0, s>>>(v, dinvs, sst, lst, mode, scale_mul, x, n);
+template <typename T>
+void launch_restrict_dof(cudaStream_t s, const T* v, const T* minv, const CgState* sst,
+                         const CgState* lst, int mode, double scale_mul, float* out,
+                         const GridN& gf, const GridN& gc) {
+  const int64_t nc = (int64_t)gc.nx * gc.ny * gc.nz;
+  k_restrict_dof<T><<<vec_blocks(nc), 256, 0, s>>>(v, minv, sst, lst, mode, scale_mul, out, gf,
+                                                   gc);
   HX_CHECK_LAUNCH();
 }
+template void launch_restrict_dof<double>(cudaStream_t, const double*, const double*,
+                                          const CgState*, const CgState*, int, double, float*,
+                                          const GridN&, const GridN&);
+template void launch_restrict_dof<float>(cudaStream_t, const float*, const float*, const CgState*,
+                                         const CgState*, int, double, float*, const GridN&,
+                                         const GridN&);
 
 void launch_restrict(cudaStream_t s, int ch, const float* in, float* out, const GridN& gf,
                      const GridN& gc, bool normalise) {
@@ -584,24 +538,21 @@ void launch_unlift(cudaStream_t s, const __nv_bfloat16* Y, const float* feat, fl
   HX_CHECK_LAUNCH();
 }
 
-void launch_net_output(cudaStream_t s, const double* r, const double* minv, const double* dinvs,
-                       const float* t, CgState* st, double scale_mul, double* z,
-                       const double* q_old, double* partials, int64_t n) {
-  k_net_output<<<vec_blocks(n), 256, 0, s>>>(r, minv, dinvs, t, st, scale_mul, z, q_old,
-                                              partials, n);
+template <typename T>
+void launch_net_output(cudaStream_t s, const T* r, const T* minv, const float* t, const GridN& gf,
+                       const GridN& gc, CgState* st, double scale_mul, T* z, const T* q_old,
+                       double* partials) {
+  const int64_t nf = (int64_t)gf.nx * gf.ny * gf.nz;
+  k_net_output<T><<<vec_blocks(nf), 256, 0, s>>>(r, minv, t, gf, gc, st, scale_mul, z, q_old,
+                                                 partials);
   HX_CHECK_LAUNCH();
 }
-
-// dinvs = sqrt(minv) (the Jacobi scaling D^-1/2 on free DOFs, 0 elsewhere)
-__global__ void k_sqrt(const double* __restrict__ a, double* __restrict__ b, int64_t n) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x)
-    b[i] = sqrt(a[i]);
-}
-void launch_sqrt(cudaStream_t s, const double* a, double* b, int64_t n) {
-  k_sqrt<<<vec_blocks(n), 256, 0, s>>>(a, b, n);
-  HX_CHECK_LAUNCH();
-}
+template void launch_net_output<double>(cudaStream_t, const double*, const double*, const float*,
+                                        const GridN&, const GridN&, CgState*, double, double*,
+                                        const double*, double*);
+template void launch_net_output<float>(cudaStream_t, const float*, const float*, const float*,
+                                       const GridN&, const GridN&, CgState*, double, float*,
+                                       const float*, double*);
 
 // Density feature of a node: mean over its elements of (log10 f + 9) / 9,
 // clamped to [0, 1] (f = stiffness factor, 1e-9 .. 1 under SIMP).

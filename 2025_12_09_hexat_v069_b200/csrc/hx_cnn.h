@@ -19,18 +19,21 @@ constexpr int NET_IN = 6;  // live input channels: D^-1/2 r / s and the same tim
 
 size_t conv_num_tiles(const GridN& g);
 // plain convolution (or, with the packed transposed weights, its transpose)
+// on the tcgen05 tensor cores; *err is set when a CTA's bounded wait ran out
 void launch_conv3(cudaStream_t s, int cout, const __nv_bfloat16* X, __nv_bfloat16* Y,
-                  const __nv_bfloat16* W, const GridN& g);
+                  const __nv_bfloat16* W, const GridN& g, int* err);
 // grad (+)= dW of one layer from the per-CTA partials
 void launch_conv3_wgrad(cudaStream_t s, const __nv_bfloat16* X, const __nv_bfloat16* D,
                         float* part, float* grad, bool accumulate, const GridN& g);
 void launch_adam(cudaStream_t s, float* w, float* m, float* v, const float* grad,
                  const unsigned char* live, int n, float lr, int step);
 void launch_pack_weights(cudaStream_t s, const float* w, __nv_bfloat16* wf, __nv_bfloat16* wb);
-// x = k D^-1/2 v as an FP32 nodal field [node][3] (k by mode: 0 network input,
-// 1 energy-loss gradient, 2 residual-loss gradient)
-void launch_field_in(cudaStream_t s, const double* v, const double* dinvs, const CgState* sst,
-                     const CgState* lst, int mode, double scale_mul, float* x, int64_t n);
+// level-1 field R (k D^-1/2 v) of a DOF vector, D^-1/2 = sqrt(minv) (k by
+// mode: 0 network input, 1 energy-loss gradient, 2 residual-loss gradient)
+template <typename T>
+void launch_restrict_dof(cudaStream_t s, const T* v, const T* minv, const CgState* sst,
+                         const CgState* lst, int mode, double scale_mul, float* out,
+                         const GridN& gf, const GridN& gc);
 // full-weighting restriction fine -> coarse node grid (ch 3 or 1), and its transpose
 void launch_restrict(cudaStream_t s, int ch, const float* in, float* out, const GridN& gf,
                      const GridN& gc, bool normalise);
@@ -40,12 +43,13 @@ void launch_prolong(cudaStream_t s, const float* coarse, float* fine, const Grid
 void launch_lift(cudaStream_t s, const float* x, const float* feat, __nv_bfloat16* X, int64_t nn);
 void launch_unlift(cudaStream_t s, const __nv_bfloat16* Y, const float* feat, float* acc,
                    bool accumulate, int64_t nn);
-void launch_net_output(cudaStream_t s, const double* r, const double* minv, const double* dinvs,
-                       const float* t, CgState* st, double scale_mul, double* z,
-                       const double* q_old, double* partials, int64_t n);
+// z = M^-1 r + s D^-1/2 R^T t  (t: level-1 correction), with the FCG beta from q_old
+template <typename T>
+void launch_net_output(cudaStream_t s, const T* r, const T* minv, const float* t, const GridN& gf,
+                       const GridN& gc, CgState* st, double scale_mul, T* z, const T* q_old,
+                       double* partials);
 void launch_net_aloss(cudaStream_t s, const double* d, const double* q, const double* e,
                       const double* r, int64_t n, double* partials, CgState* st, double* out);
-void launch_sqrt(cudaStream_t s, const double* a, double* b, int64_t n);
 void launch_rho_feature(cudaStream_t s, const double* fac, float* feat, const Grid& g);
 
 }  // namespace hx

@@ -1,0 +1,324 @@
+// hx_conv_tc.cu -- 3x3x3 conv3d (16 input channels, BF16, no bias) on the
+// 5th-generation tensor cores: tcgen05.mma with operands in shared memory,
+// staged by TMA, and the FP32 accumulators in tensor memory (TMEM).
+//
+// Y[n, co] = sum_{tap, ci} X[n + off(tap), ci] * W[tap][co][ci]   (zero padding)
+// The transpose (backward-data pass) is the same kernel on the flipped,
+// per-tap transposed weights.
+//
+// One CTA (4 warps) computes an 8 x 16 x 4 node tile.  Implicit GEMM per
+// z-slice: M = 128 nodes (8 x by 16 y), N = 16 output channels, K = 27 taps
+// x 16 channels, as 27 MMAs of M128 N16 K16 accumulating in 16 TMEM columns
+// (4 slices: 64 columns).
+//
+// Shared-memory layout.  An MMA operand descriptor (no swizzle, K-major)
+// addresses 8-row core matrices whose rows are 16 bytes apart; the stride
+// between consecutive core matrices (SBO) and between the two 8-channel
+// halves of K (LBO) are descriptor fields.  The input tile with its one-node
+// halo (10 x 18 x 6 nodes) is staged as two planes of 8 channels, 16 bytes
+// per node, x fastest: node (z, y, x) at ((z * 18 + y) * 10 + x) * 16.  The
+// 128 rows of z-slice z for tap (dz, dy, dx) are then 16 core matrices, one
+// per y, of 8 consecutive x: core matrix j starts at node
+// ((z + 1 + dz) * 18 + 1 + dy + j) * 10 + 1 + dx, i.e. a fixed start plus
+// j * 160 bytes (SBO = 160).  Every tap is a start address in the same
+// staged tile, so one TMA tile load per plane (box 8 ch x 10 x 18 x 6 from
+// the [z][y][x][16 ch] activation tensor; coordinates outside the grid read
+// as zero) stages all the operands.  Row m of the accumulator is node
+// (x0 + m % 8, y0 + m / 8).  The weights are staged as [tap][plane][co][8 ci]
+// (the B operand, N = 16 rows).
+//
+// One tile per CTA; with 48 KB of shared memory 4 CTAs share an SM, so the
+// loads of some overlap the MMAs and epilogues of others (a persistent
+// variant with a 2-stage load ring, at 2 CTAs per SM, measured slower).
+// Thread 0 issues the tile's TMA loads and the bulk copy of the layer's
+// weights (pre-packed in this order) on one mbarrier, then the 108 MMAs
+// and a tcgen05.commit on a second.  Every wait is bounded; on timeout the
+// CTA records it in *err, waits (bounded) for its own loads, frees its TMEM
+// and returns, and the host reports the error.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+#include "hx_cnn.h"
+
+namespace hx {
+
+namespace {
+
+constexpr int TX = 8, TY = 16, TZ = 4;
+constexpr int BX = TX + 2, BY = TY + 2, BZ = TZ + 2;          // staged box with halo
+constexpr int BOX_NODES = BX * BY * BZ;                       // 1080
+constexpr int PLANE_BYTES = BOX_NODES * 16;                   // 17280
+constexpr int X_BYTES = 2 * PLANE_BYTES;                      // 34560: [plane]
+constexpr int W_BYTES = 27 * 2 * 16 * 16;                     // 13824: [tap][plane][co]
+constexpr int SMEM_BYTES = X_BYTES + W_BYTES + 64;            // + barriers, TMEM address
+constexpr int NTHREADS = 128;
+constexpr int TMEM_COLS = 64;                                 // TZ slices x 16 columns
+constexpr uint32_t TMA_BYTES = (uint32_t)X_BYTES;
+constexpr long long WAIT_LIMIT = 1ll << 20;                   // polls before giving up
+
+static_assert(TX == 8 && TX * TY == 128, "a z-slice is 16 core matrices of 8 x-nodes");
+static_assert(PLANE_BYTES % 128 == 0, "TMA destinations 128-byte aligned");
+static_assert(TZ * 16 <= TMEM_COLS, "accumulators fit the allocation");
+
+// Shared-memory matrix descriptor (tcgen05): no swizzle, K-major.  Fields in
+// 16-byte units: start address [0,14), leading byte offset (between the two
+// 8-element K halves) [16,30), stride byte offset (between 8-row groups)
+// [32,46); version 1 [46,48); base offset 0; layout type 0 (no swizzle).
+__host__ __device__ constexpr uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor, kind::f16: D FP32 [4,6) = 1, A BF16 [7,10) = 1,
+// B BF16 [10,13) = 1, both K-major, N >> 3 at [17,23), M >> 4 at [24,29).
+__host__ __device__ constexpr uint32_t instr_desc(int m, int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) |
+         ((uint32_t)(m >> 4) << 24);
+}
+
+static_assert(instr_desc(128, 16) == 0x08040490u, "instruction descriptor encoding");
+static_assert(smem_desc(0x400, 17280, 160) ==
+                  ((1ull << 46) | (10ull << 32) | (1080ull << 16) | 0x40ull),
+              "shared-memory descriptor encoding");
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t phase) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred P1;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, P1;\n\t}"
+      : "=r"(done)
+      : "r"(bar), "r"(phase)
+      : "memory");
+  return done != 0;
+}
+
+// bounded wait; false when the limit was reached
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
+  for (long long i = 0; i < WAIT_LIMIT; ++i)
+    if (mbar_try_wait(bar, phase)) return true;
+  return false;
+}
+
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map, uint32_t bar,
+                                            int c0, int c1, int c2, int c3) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4, %5, %6}], [%2];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_f16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                         uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   bar)
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+}  // namespace
+
+template <int COUT>
+__global__ void __launch_bounds__(NTHREADS) k_conv3_tc(const __grid_constant__ CUtensorMap xmap,
+                                                       const __nv_bfloat16* __restrict__ W,
+                                                       __nv_bfloat16* __restrict__ Y, GridN g,
+                                                       int* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned char* xs = smem;                        // [plane][1080 nodes][16 B]
+  unsigned char* ws = smem + X_BYTES;              // [tap][plane][16 co][16 B]
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + X_BYTES + W_BYTES);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2);
+  int* fail = reinterpret_cast<int*>(bars + 2) + 1;
+  const uint32_t load_bar = smem_u32(&bars[0]), mma_bar = smem_u32(&bars[1]);
+  const uint32_t xb = smem_u32(xs), wsb = smem_u32(ws);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = blockIdx.z * TZ;
+
+  if (warp == 0) {  // TMEM for the 4 accumulators
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (threadIdx.x == 0) {
+    mbar_init(load_bar, 1);
+    mbar_init(mma_bar, 1);
+    *fail = 0;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // barriers visible to TMA
+    // the input tile (two 8-channel planes) and the layer's weights on one barrier
+    mbar_expect_tx(load_bar, TMA_BYTES + W_BYTES);
+    for (int h = 0; h < 2; ++h)
+      tma_load_4d(xb + (uint32_t)(h * PLANE_BYTES), &xmap, load_bar, h * 8, x0 - 1, y0 - 1,
+                  z0 - 1);
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(wsb),
+        "l"(W), "r"(W_BYTES), "r"(load_bar)
+        : "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  if (threadIdx.x == 0) {
+    if (!mbar_wait(load_bar, 0)) {
+      *fail = 1;
+      atomicExch(err, 1);
+      mbar_wait(load_bar, 0);  // give the loads in flight another bounded chance
+    } else {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      // descriptors: a fixed part plus the start address (16-byte units, low
+      // bits), so each of the 108 MMAs adds a compile-time offset
+      const uint64_t a0 = smem_desc(xb, PLANE_BYTES, BX * 16);
+      const uint64_t b0 = smem_desc(wsb, 256, 128);
+      constexpr uint32_t idesc = instr_desc(128, 16);
+#pragma unroll
+      for (int z = 0; z < TZ; ++z) {
+#pragma unroll
+        for (int tap = 0; tap < 27; ++tap) {
+          const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+          const uint32_t a_off = (uint32_t)(((z + 1 + dz) * BY + 1 + dy) * BX + 1 + dx);
+          umma_f16(tmem + (uint32_t)(z * 16), a0 + a_off, b0 + (uint32_t)(tap * 32), idesc,
+                   tap > 0 ? 1u : 0u);
+        }
+      }
+      umma_commit(mma_bar);
+    }
+  }
+  __syncthreads();
+  bool ok = *fail == 0;
+  if (ok && !mbar_wait(mma_bar, 0)) {
+    ok = false;
+    atomicExch(err, 1);
+  }
+  if (ok) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const int m = warp * 32 + lane;  // accumulator row = TMEM lane
+    const int gx = x0 + (m & 7), gy = y0 + (m >> 3);
+#pragma unroll
+    for (int z = 0; z < TZ; ++z) {
+      float v[16];
+      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(z * 16), v);
+      const int gz = z0 + z;
+      if (gx < g.nx && gy < g.ny && gz < g.nz) {
+        const int64_t node = ((int64_t)gz * g.ny + gy) * g.nx + gx;
+        uint32_t o[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const __nv_bfloat162 h2 = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+          o[i] = *reinterpret_cast<const uint32_t*>(&h2);
+        }
+        uint4* dst = reinterpret_cast<uint4*>(Y + node * COUT);
+        dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
+        if (COUT == 16) dst[1] = make_uint4(o[4], o[5], o[6], o[7]);
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(TMEM_COLS)
+                 : "memory");
+}
+
+namespace {
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    else
+      cudaGetLastError();
+  });
+  return fn;
+}
+
+// Tensor map of an activation tensor [nz][ny][nx][16 ch] BF16 with the
+// staging box (8 ch, 10 x, 18 y, 6 z).
+CUtensorMap activation_map(const __nv_bfloat16* X, const GridN& g) {
+  auto fn = encode_fn();
+  HX_REQUIRE(fn != nullptr, "cuTensorMapEncodeTiled is not available from the driver");
+  HX_REQUIRE((reinterpret_cast<uintptr_t>(X) & 15) == 0, "activations must be 16-byte aligned");
+  CUtensorMap map;
+  const cuuint64_t dims[4] = {16, (cuuint64_t)g.nx, (cuuint64_t)g.ny, (cuuint64_t)g.nz};
+  const cuuint64_t strides[3] = {32, (cuuint64_t)g.nx * 32, (cuuint64_t)g.nx * g.ny * 32};
+  const cuuint32_t box[4] = {8, BX, BY, BZ};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  const CUresult r =
+      fn(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16*>(X), dims, strides,
+         box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+         CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  HX_REQUIRE(r == CUDA_SUCCESS, "cuTensorMapEncodeTiled failed");
+  return map;
+}
+
+}  // namespace
+
+void launch_conv3(cudaStream_t s, int cout, const __nv_bfloat16* X, __nv_bfloat16* Y,
+                  const __nv_bfloat16* W, const GridN& g, int* err) {
+  HX_REQUIRE(cout == 16 || cout == 8, "unsupported conv configuration");
+  HX_REQUIRE(err != nullptr, "conv error flag missing");
+  static bool cfg[2] = {false, false};
+  const int idx = cout == 16 ? 0 : 1;
+  if (!cfg[idx]) {
+    HX_CUDA(cudaFuncSetAttribute(cout == 16 ? k_conv3_tc<16> : k_conv3_tc<8>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+    cfg[idx] = true;
+  }
+  const CUtensorMap map = activation_map(X, g);
+  const dim3 grid((unsigned)cdiv(g.nx, TX), (unsigned)cdiv(g.ny, TY), (unsigned)cdiv(g.nz, TZ));
+  if (cout == 16)
+    k_conv3_tc<16><<<grid, NTHREADS, SMEM_BYTES, s>>>(map, W, Y, g, err);
+  else
+    k_conv3_tc<8><<<grid, NTHREADS, SMEM_BYTES, s>>>(map, W, Y, g, err);
+  HX_CHECK_LAUNCH();
+}
+
+}  // namespace hx

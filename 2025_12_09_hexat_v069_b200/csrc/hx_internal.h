@@ -204,8 +204,11 @@ struct hx_ctx {
       hx::DevBuf<float> x, acc, gx, feat;  // [node][3] fields, [node] feature
       hx::DevBuf<__nv_bfloat16> x0, y, act[7];  // network input, output, training activations
     } lv[4];
-    hx::DevBuf<double> dinvs, z, scal, facbuf;
+    hx::DevBuf<double> z, scal, facbuf;
+    hx::DevBuf<float> z32, s32;  // mixed-precision FCG: preconditioned vector, scratch
+    hx::DevBuf<int> err;         // set by a conv CTA whose bounded wait ran out
     const double* fac_last = nullptr;  // factors the operator inputs were built for
+    int64_t prepared_dofs = -1;        // DOF count of the mesh they were built on
   } net;
 
   size_t partial_capacity() const { return d_partials.n; }

@@ -28,6 +28,7 @@
 // always judged on the residual, and the solve falls back to Jacobi-PCG
 // from the current iterate when FCG breaks down or stalls.
 #include <cmath>
+#include <limits>
 #include <cstring>
 #include <utility>
 #include <vector>
@@ -66,6 +67,22 @@ void net_alloc_params(hx_ctx* c) {
   N.wf.ensure(NET_PARAMS);
   N.wb.ensure(NET_PARAMS);
   N.scal.ensure(8);
+  if (N.err.n == 0) {
+    N.err.ensure(1);
+    HX_CUDA(cudaMemsetAsync(N.err.p, 0, sizeof(int), c->stream));
+  }
+}
+
+// Throws if a conv kernel reported a wait that ran out (and clears the flag).
+void check_conv_error(hx_ctx* c) {
+  if (c->net.err.n == 0) return;
+  int e = 0;
+  HX_CUDA(cudaMemcpyAsync(&e, c->net.err.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  HX_CUDA(cudaStreamSynchronize(c->stream));
+  if (e != 0) {
+    HX_CUDA(cudaMemsetAsync(c->net.err.p, 0, sizeof(int), c->stream));
+    throw Error{HX_CUDA_ERROR, "tensor-core convolution: a bounded wait ran out"};
+  }
 }
 
 void net_pack(hx_ctx* c) {
@@ -100,20 +117,18 @@ void net_buffers(hx_ctx* c, bool train) {
   const size_t a1 = (size_t)nodes_of(g1) * 16;
   N.tmp[0].ensure(a1);
   N.tmp[1].ensure(a1);
-  for (int l = 0; l <= NET_NETS; ++l) {
+  N.lv[0].feat.ensure((size_t)nodes_of(level_grid(c->g, 0)));  // only the feature on level 0
+  for (int l = 1; l <= NET_NETS; ++l) {
     const size_t nl = (size_t)nodes_of(level_grid(c->g, l));
     auto& L = N.lv[l];
     L.x.ensure(nl * 3);
     L.acc.ensure(nl * 3);
     L.feat.ensure(nl);
-    if (l >= 1) {
-      L.x0.ensure(nl * 16);
-      L.y.ensure(nl * 8);
-    }
+    L.x0.ensure(nl * 16);
+    L.y.ensure(nl * 8);
     if (train) {
       L.gx.ensure(nl * 3);
-      if (l >= 1)
-        for (auto& a : L.act) a.ensure(nl * 16);
+      for (auto& a : L.act) a.ensure(nl * 16);
     }
   }
   if (train) {
@@ -130,23 +145,25 @@ const __nv_bfloat16* adj_w(const hx_ctx* c, int k, int l) { return c->net.wb.p +
 void stack_apply(hx_ctx* c, int k, const GridN& g, const __nv_bfloat16* x0, __nv_bfloat16* y) {
   __nv_bfloat16* u = c->net.tmp[0].p;
   __nv_bfloat16* v = c->net.tmp[1].p;
-  launch_conv3(c->stream, 16, x0, u, fwd_w(c, k, 0), g);  // A1
-  launch_conv3(c->stream, 16, u, v, fwd_w(c, k, 1), g);   // A2
-  launch_conv3(c->stream, 16, v, u, fwd_w(c, k, 2), g);   // A3
-  launch_conv3(c->stream, 16, u, v, fwd_w(c, k, 3), g);   // H = G x0
-  launch_conv3(c->stream, 16, v, u, adj_w(c, k, 3), g);   // B3
-  launch_conv3(c->stream, 16, u, v, adj_w(c, k, 2), g);   // B2
-  launch_conv3(c->stream, 16, v, u, adj_w(c, k, 1), g);   // B1
-  launch_conv3(c->stream, 8, u, y, adj_w(c, k, 0), g);    // B0 = G^T H (6 live channels)
+  launch_conv3(c->stream, 16, x0, u, fwd_w(c, k, 0), g, c->net.err.p);  // A1
+  launch_conv3(c->stream, 16, u, v, fwd_w(c, k, 1), g, c->net.err.p);   // A2
+  launch_conv3(c->stream, 16, v, u, fwd_w(c, k, 2), g, c->net.err.p);   // A3
+  launch_conv3(c->stream, 16, u, v, fwd_w(c, k, 3), g, c->net.err.p);   // H = G x0
+  launch_conv3(c->stream, 16, v, u, adj_w(c, k, 3), g, c->net.err.p);   // B3
+  launch_conv3(c->stream, 16, u, v, adj_w(c, k, 2), g, c->net.err.p);   // B2
+  launch_conv3(c->stream, 16, v, u, adj_w(c, k, 1), g, c->net.err.p);   // B1
+  launch_conv3(c->stream, 8, u, y, adj_w(c, k, 0), g, c->net.err.p);    // B0 = G^T H, 6 channels
 }
 
 // y = G_k^T G_k x0 keeping every activation: act = A1 A2 A3 H B3 B2 B1.
 void stack_forward_train(hx_ctx* c, int k, const GridN& g, const __nv_bfloat16* x0,
                          DevBuf<__nv_bfloat16>* act, __nv_bfloat16* y) {
-  launch_conv3(c->stream, 16, x0, act[0].p, fwd_w(c, k, 0), g);
-  for (int l = 1; l < 4; ++l) launch_conv3(c->stream, 16, act[l - 1].p, act[l].p, fwd_w(c, k, l), g);
-  for (int l = 3; l >= 1; --l) launch_conv3(c->stream, 16, act[6 - l].p, act[7 - l].p, adj_w(c, k, l), g);
-  launch_conv3(c->stream, 8, act[6].p, y, adj_w(c, k, 0), g);
+  launch_conv3(c->stream, 16, x0, act[0].p, fwd_w(c, k, 0), g, c->net.err.p);
+  for (int l = 1; l < 4; ++l)
+    launch_conv3(c->stream, 16, act[l - 1].p, act[l].p, fwd_w(c, k, l), g, c->net.err.p);
+  for (int l = 3; l >= 1; --l)
+    launch_conv3(c->stream, 16, act[6 - l].p, act[7 - l].p, adj_w(c, k, l), g, c->net.err.p);
+  launch_conv3(c->stream, 8, act[6].p, y, adj_w(c, k, 0), g, c->net.err.p);
 }
 
 // Gradients of network k into N.grad from da = dLoss/dB0 (16-channel
@@ -165,7 +182,8 @@ void stack_backward_train(hx_ctx* c, int k, const GridN& g, const __nv_bfloat16*
   const __nv_bfloat16* bin[4] = {act[6].p, act[5].p, act[4].p, act[3].p};
   for (int l = 0; l < 4; ++l) {
     launch_conv3_wgrad(c->stream, e0, bin[l], N.part.p, grad + l * LP, accumulate, g);
-    launch_conv3(c->stream, 16, e0, e1, fwd_w(c, k, l), g);  // E_{l+1}; l = 3: dLoss/dH
+    // E_{l+1}; l = 3: dLoss/dH
+    launch_conv3(c->stream, 16, e0, e1, fwd_w(c, k, l), g, c->net.err.p);
     std::swap(e0, e1);
   }
   // forward uses: layer l maps A_l (x0 for l = 0) to A_{l+1} (H for l = 3)
@@ -173,19 +191,27 @@ void stack_backward_train(hx_ctx* c, int k, const GridN& g, const __nv_bfloat16*
   for (int l = 3; l >= 0; --l) {
     launch_conv3_wgrad(c->stream, ain[l], e0, N.part.p, grad + l * LP, true, g);
     if (l > 0) {
-      launch_conv3(c->stream, 16, e0, e1, adj_w(c, k, l), g);
+      launch_conv3(c->stream, 16, e0, e1, adj_w(c, k, l), g, c->net.err.p);
       std::swap(e0, e1);
     }
   }
 }
 
-// lv[0].acc = sum_l R_l^T E_l^T G_l^T G_l E_l R_l lv[0].x  (coarsest level
-// first: acc_l = E_l^T y_l + R^T acc_{l+1}).  `train` keeps the activations.
-void precond_correction(hx_ctx* c, bool train) {
+// z = M^-1 r + s D^-1/2 sum_l R_l^T E_l^T G_l^T G_l E_l R_l (D^-1/2 r / s).
+// The mesh-grid passes are fused: the level-1 field is restricted straight
+// from r (k_restrict_dof) and the level-1 correction is prolongated inside
+// the output kernel, so no field is stored on the mesh's node grid.  The
+// levels run coarsest first: acc_l = E_l^T y_l + R^T acc_{l+1}.  `train`
+// keeps the activations; q_old: FCG beta reduction (see k_net_output).
+// T: precision of r, minv, z, q_old (the solver's vectors).
+template <typename T>
+void precond_z(hx_ctx* c, const T* r, const T* minv, CgState* st, double scale_mul, T* z,
+               const T* q_old, bool train) {
   auto& N = c->net;
   GridN gl[NET_NETS + 1];
   for (int l = 0; l <= NET_NETS; ++l) gl[l] = level_grid(c->g, l);
-  for (int l = 1; l <= NET_NETS; ++l)
+  launch_restrict_dof<T>(c->stream, r, minv, st, nullptr, 0, scale_mul, N.lv[1].x.p, gl[0], gl[1]);
+  for (int l = 2; l <= NET_NETS; ++l)
     launch_restrict(c->stream, 3, N.lv[l - 1].x.p, N.lv[l].x.p, gl[l - 1], gl[l], false);
   for (int l = NET_NETS; l >= 1; --l) {
     auto& L = N.lv[l];
@@ -198,7 +224,8 @@ void precond_correction(hx_ctx* c, bool train) {
     launch_unlift(c->stream, L.y.p, L.feat.p, L.acc.p, false, nl);
     if (l < NET_NETS) launch_prolong(c->stream, N.lv[l + 1].acc.p, L.acc.p, gl[l], gl[l + 1], true);
   }
-  launch_prolong(c->stream, N.lv[1].acc.p, N.lv[0].acc.p, gl[0], gl[1], false);
+  launch_net_output<T>(c->stream, r, minv, N.lv[1].acc.p, gl[0], gl[1], st, scale_mul, z, q_old,
+                       c->d_partials.p);
 }
 
 // Jacobi scaling and density features of the current operator (after a
@@ -208,8 +235,6 @@ void net_operator_inputs(hx_ctx* c, const double* fac) {
   const int64_t n = c->g.dofs();
   HX_REQUIRE(c->d_minv.n >= (size_t)n, "no Jacobi data: run a solve on this grid first");
   net_buffers(c, false);
-  N.dinvs.ensure(n);
-  launch_sqrt(c->stream, c->d_minv.p, N.dinvs.p, n);
   launch_rho_feature(c->stream, fac, N.lv[0].feat.p, c->g);
   for (int l = 1; l <= NET_NETS; ++l)
     launch_restrict(c->stream, 1, N.lv[l - 1].feat.p, N.lv[l].feat.p, level_grid(c->g, l - 1),
@@ -220,11 +245,12 @@ void net_operator_inputs(hx_ctx* c, const double* fac) {
     HX_CUDA(cudaMemcpyAsync(fb, fac, c->g.elems() * sizeof(double), cudaMemcpyDeviceToDevice,
                             c->stream));
   N.fac_last = fb;
+  N.prepared_dofs = n;
 }
 
 void require_prepared(hx_ctx* c) {
   HX_REQUIRE(c->net.ready, "network not initialised");
-  HX_REQUIRE(c->net.dinvs.n >= (size_t)c->g.dofs() && c->net.fac_last != nullptr,
+  HX_REQUIRE(c->net.fac_last != nullptr && c->net.prepared_dofs == c->g.dofs(),
              "no operator inputs: call hx_net_prepare after a solve");
 }
 
@@ -307,6 +333,7 @@ void net_forward_backward(hx_ctx* c, int nx, int ny, int nz, const float* x0, co
   for (int64_t n = 0; n < nn; ++n)
     for (int ch = 0; ch < 16; ++ch)
       y[n * 16 + ch] = ch < 8 ? __bfloat162float(hy[n * 8 + ch]) : 0.f;
+  check_conv_error(c);
 }
 
 // Loss of one residual (and error) of the current operator; with `grad`,
@@ -323,12 +350,9 @@ double net_loss_grad(hx_ctx* c, const double* r, const double* e, int loss_kind,
   HX_CUDA(cudaMemsetAsync(s3, 0, sizeof(CgState), c->stream));
   launch_cg_init<double>(c->stream, r, nullptr, c->d_minv.p, zscr, pscr, n, s3, c->d_partials.p);
   const double scale_mul = 1.0 / (double)n;
-  launch_field_in(c->stream, r, N.dinvs.p, s3, nullptr, 0, scale_mul, N.lv[0].x.p, n);
-  precond_correction(c, true);
   double* z = N.z.ensure(n);
   double* q = c->d_q.ensure(n);
-  launch_net_output(c->stream, r, c->d_minv.p, N.dinvs.p, N.lv[0].acc.p, s3, scale_mul, z,
-                    nullptr, nullptr, n);
+  precond_z<double>(c, r, c->d_minv.p, s3, scale_mul, z, nullptr, true);
   HX_CUDA(cudaMemsetAsync(s2, 0, sizeof(CgState), c->stream));
   bool host_ratio = false;
   const double* gvec = nullptr;  // dLoss/dz up to the coefficient of the mode
@@ -357,8 +381,9 @@ double net_loss_grad(hx_ctx* c, const double* r, const double* e, int loss_kind,
   }
   // dLoss/d(correction at level l) = R_l (s D^-1/2 dLoss/dz); each network's
   // output gradient is its lifting E_l
-  launch_field_in(c->stream, gvec, N.dinvs.p, s3, s2, mode, scale_mul, N.lv[0].gx.p, n);
-  for (int l = 1; l <= NET_NETS; ++l)
+  launch_restrict_dof<double>(c->stream, gvec, c->d_minv.p, s3, s2, mode, scale_mul, N.lv[1].gx.p,
+                      level_grid(g, 0), level_grid(g, 1));
+  for (int l = 2; l <= NET_NETS; ++l)
     launch_restrict(c->stream, 3, N.lv[l - 1].gx.p, N.lv[l].gx.p, level_grid(g, l - 1),
                     level_grid(g, l), false);
   for (int l = 1; l <= NET_NETS; ++l) {
@@ -393,7 +418,7 @@ double net_train_step(hx_ctx* c, const double* const* r, const double* const* e,
   N.step += 1;
   launch_adam(c->stream, N.w.p, N.m.p, N.v.p, N.grad.p, N.live.p, NET_PARAMS, (float)lr, N.step);
   net_pack(c);
-  HX_CUDA(cudaStreamSynchronize(c->stream));
+  check_conv_error(c);
   return sum / count;
 }
 
@@ -402,7 +427,6 @@ void net_prepare(hx_ctx* c, const double* fac) { net_operator_inputs(c, fac); }
 // z = P r with the prepared operator (FP64 device vectors, grid numbering).
 void net_apply_vec(hx_ctx* c, const double* r, double* z) {
   require_prepared(c);
-  auto& N = c->net;
   const int64_t n = c->g.dofs();
   net_buffers(c, false);
   ensure_workspace(c);
@@ -418,11 +442,8 @@ void net_apply_vec(hx_ctx* c, const double* r, double* z) {
   }
   HX_REQUIRE(st.status == HX_RUNNING && st.rz > 0.0, "r is not finite");
   const double scale_mul = 1.0 / (double)n;
-  launch_field_in(c->stream, r, N.dinvs.p, s3, nullptr, 0, scale_mul, N.lv[0].x.p, n);
-  precond_correction(c, false);
-  launch_net_output(c->stream, r, c->d_minv.p, N.dinvs.p, N.lv[0].acc.p, s3, scale_mul, z,
-                    nullptr, nullptr, n);
-  HX_CUDA(cudaStreamSynchronize(c->stream));
+  precond_z<double>(c, r, c->d_minv.p, s3, scale_mul, z, nullptr, false);
+  check_conv_error(c);
 }
 
 std::function<void()> net_time_body(hx_ctx* c, int which) {
@@ -437,7 +458,8 @@ std::function<void()> net_time_body(hx_ctx* c, int which) {
     HX_CUDA(cudaMemsetAsync(N.tmp[0].p, 0, (size_t)nodes_of(g1) * 16 * sizeof(__nv_bfloat16),
                             c->stream));
     return [c, g1] {
-      launch_conv3(c->stream, 16, c->net.tmp[0].p, c->net.tmp[1].p, fwd_w(c, 0, 1), g1);
+      launch_conv3(c->stream, 16, c->net.tmp[0].p, c->net.tmp[1].p, fwd_w(c, 0, 1), g1,
+                   c->net.err.p);
     };
   }
   // the state of slot 3 holds r.M^-1 r of the last solve's residual
@@ -447,12 +469,8 @@ std::function<void()> net_time_body(hx_ctx* c, int which) {
                          c->d_aux2.ensure(n), n, s3, c->d_partials.p);
   double* z = N.z.ensure(n);
   return [c, s3, z, n] {
-    auto& M = c->net;
     const double scale_mul = 1.0 / (double)n;
-    launch_field_in(c->stream, c->d_r.p, M.dinvs.p, s3, nullptr, 0, scale_mul, M.lv[0].x.p, n);
-    precond_correction(c, false);
-    launch_net_output(c->stream, c->d_r.p, c->d_minv.p, M.dinvs.p, M.lv[0].acc.p, s3, scale_mul,
-                      z, nullptr, nullptr, n);
+    precond_z<double>(c, c->d_r.p, c->d_minv.p, s3, scale_mul, z, nullptr, false);
   };
 }
 
@@ -461,9 +479,9 @@ std::function<void()> net_time_body(hx_ctx* c, int which) {
 // BF16 network).  Falls back to Jacobi-PCG from the current iterate when
 // FCG breaks down, diverges, or stalls.
 // ---------------------------------------------------------------------------
-CgState solve_learned(hx_ctx* c, const double* fac, const double* b, double* x, bool warm,
-                      double shift, const hx_solve_opts& o, double t0, bool* timed_out,
-                      int* fallback, int* iters_out) {
+static CgState learned_fcg(hx_ctx* c, const double* fac, const double* b, double* x, bool warm,
+                          double shift, const hx_solve_opts& o, double t0, bool* timed_out,
+                          int* fallback, int* iters_out) {
   HX_REQUIRE(c->net.ready, "learned preconditioner requested but no network is loaded");
   auto& N = c->net;
   const Grid& g = c->g;
@@ -493,10 +511,7 @@ CgState solve_learned(hx_ctx* c, const double* fac, const double* b, double* x, 
   *iters_out = 0;
   if (s0.status != HX_RUNNING || o.max_iter <= 0) return s0;
   auto one = [&](double* pin, double* pout) {
-    launch_field_in(c->stream, r, N.dinvs.p, st, nullptr, 0, scale_mul, N.lv[0].x.p, n);
-    precond_correction(c, false);
-    launch_net_output(c->stream, r, minv, N.dinvs.p, N.lv[0].acc.p, st, scale_mul, z, q,
-                      c->d_partials.p, n);
+    precond_z<double>(c, r, minv, st, scale_mul, z, q, false);
     launch_fcg_step<double>(c->stream, pin, pout, z, r, x, q, fac, c->d_nmask.p, g, c->K, shift,
                             st, c->d_partials.p);
     launch_cg_update2<double>(c->stream, r, q, minv, n, st, c->d_partials.p);
@@ -510,23 +525,20 @@ CgState solve_learned(hx_ctx* c, const double* fac, const double* b, double* x, 
   int best_it = 0;
   CgState sf{};
   bool stalled = false;
-  // Run in batches, checking between them for stagnation: no 10% gain on
-  // the best residual within max(500, iterations / 4) iterations.  (CG
+  // One graph, checked between launches for stagnation: no 10% gain on the
+  // best residual within max(500, iterations / 4) iterations.  (CG
   // residuals are not monotone and on hard problems halve only every few
   // hundred iterations, so a tighter test would misfire.)
-  for (;;) {
-    sf = run_batched(c, 0, reps, body, o.wall_limit_ms, t0, timed_out, 1);
-    if (sf.rel_res < 0.9 * best) {
-      best = sf.rel_res;
-      best_it = sf.iter;
+  auto keep_going = [&](const CgState& sv) {
+    if (sv.rel_res < 0.9 * best) {
+      best = sv.rel_res;
+      best_it = sv.iter;
     }
-    if (sf.status != HX_RUNNING || *timed_out) break;
-    const int window = std::max(500, sf.iter / 4);
-    if (!o.learned_no_fallback && sf.iter - best_it > window) {
-      stalled = true;
-      break;
-    }
-  }
+    stalled = !o.learned_no_fallback && sv.iter - best_it > std::max(500, sv.iter / 4);
+    return !stalled;
+  };
+  sf = run_batched(c, 0, reps, body, o.wall_limit_ms, t0, timed_out, 0, keep_going);
+  if (sf.status != HX_RUNNING) stalled = false;
   // pending x += alpha p of the last completed iteration
   if (sf.status != HX_ST_BREAKDOWN && sf.iter > 0) {
     double* pk = ((sf.iter - 1) % 2 == 0) ? P0 : P1;
@@ -547,6 +559,191 @@ CgState solve_learned(hx_ctx* c, const double* fac, const double* b, double* x, 
                                  auto_batch(g, o.check_every), o.wall_limit_ms, t0, timed_out);
   *iters_out += sj.iter;
   return sj;
+}
+
+// ---------------------------------------------------------------------------
+// Mixed precision learned FCG.  The FCG iteration (preconditioner, fused
+// step, residual update) runs on FP32 vectors and the FP32 operator, with
+// FP64 reductions, and accumulates its correction in d32.  Reliable updates
+// as in solve_mixed: after each batch (which also ends when the recursive
+// residual has dropped by opts.inner_tol since the last replacement, or
+// claims convergence) d32 is folded into the FP64 x, the true residual
+// b - (K+sI)x is recomputed in FP64 and replaces the FP32 one, and the
+// iteration resumes with the same direction: p_old, q_old = K p_old and
+// p_old.q_old are kept, so the next flexible-CG coefficient is formed as
+// usual; alpha = 0 so the folded step is not applied twice.  Convergence is
+// judged only on the FP64 true residual.  Falls back to mixed Jacobi-PCG
+// from the current iterate when FCG breaks down or stalls (stagnation is
+// measured on the true residual).
+// ---------------------------------------------------------------------------
+static CgState learned_fcg_mixed(hx_ctx* c, const double* fac, const double* b, double* x,
+                                 bool warm, double shift, const hx_solve_opts& o, double t0,
+                                 bool* timed_out, int* fallback, int* iters_out) {
+  HX_REQUIRE(c->net.ready, "learned preconditioner requested but no network is loaded");
+  auto& N = c->net;
+  const Grid& g = c->g;
+  const int64_t n = g.dofs(), ne = g.elems();
+  net_operator_inputs(c, fac);
+  float* fac32 = c->d_fac32.ensure(ne);
+  float* minv32 = c->d_minv32.ensure(n);
+  float* r32 = c->d_r32.ensure(n);
+  float* P0 = c->d_p32.ensure(n);
+  float* P1 = c->d_p32b.ensure(n);
+  float* q32 = c->d_q32.ensure(n);
+  float* d32 = c->d_x32.ensure(n);
+  float* z32 = N.z32.ensure(n);
+  float* s32 = N.s32.ensure(n);  // scratch output of cg_init
+  double* q = c->d_q.ensure(n);
+  launch_convert<float, double>(c->stream, fac32, fac, ne);
+  launch_convert<float, double>(c->stream, minv32, c->d_minv.p, n);
+  const ElemCoef<float> K32 = to_float(c->K);
+  const float sh32 = (float)shift;
+  CgState* so = c->d_state.p;      // FP64 outer: ||b||, true residual
+  CgState* si = c->d_state.p + 1;  // FP32 FCG iteration
+  const double scale_mul = 1.0 / (double)n;
+  *fallback = 0;
+  *iters_out = 0;
+  // ||b||
+  CgState s = fresh_state(o.tol, std::numeric_limits<int>::max(), 1, false, false);
+  put_state(c, 3, CgState{});
+  launch_dot(c->stream, b, b, n, c->d_state.p + 3, c->d_partials.p, c->d_scalars.p);
+  double bb = 0;
+  HX_CUDA(cudaMemcpyAsync(&bb, c->d_scalars.p, sizeof(double), cudaMemcpyDeviceToHost,
+                          c->stream));
+  HX_CUDA(cudaStreamSynchronize(c->stream));
+  s.bnorm = std::sqrt(bb);
+  if (s.bnorm == 0.0) {
+    launch_fill_zero(c->stream, x, n * sizeof(double));
+    s.status = HX_ST_ZERO_RHS;
+    s.rel_res = 0;
+    return s;
+  }
+  put_state(c, 0, s);
+  if (!warm) launch_fill_zero(c->stream, x, n * sizeof(double));
+  // true residual of the initial guess -> r32 = r / ||b||
+  if (warm)
+    launch_matvec<double>(c->stream, 0, x, q, fac, c->d_nmask.p, g, c->K, shift,
+                          c->d_state.p + 3, c->d_partials.p, nullptr);
+  else
+    launch_fill_zero(c->stream, q, n * sizeof(double));
+  launch_ir_residual(c->stream, b, q, r32, n, so, c->d_partials.p);
+  CgState so_h = get_state(c, 0);
+  if (so_h.status != HX_RUNNING || o.max_iter <= 0) return so_h;
+  // FP32 iteration state: rz, rr of the replaced residual; no previous
+  // direction (p_old = q_old = 0, pq = 0 gives beta = 0, alpha = 0)
+  const double delta = (o.inner_tol > 0 && o.inner_tol < 1) ? o.inner_tol : 0.1;
+  put_state(c, 1, fresh_state(o.tol, o.max_iter, 1, false, false));
+  launch_fill_zero(c->stream, d32, n * sizeof(float));
+  launch_fill_zero(c->stream, P1, n * sizeof(float));
+  launch_fill_zero(c->stream, q32, n * sizeof(float));
+  launch_cg_init<float>(c->stream, r32, nullptr, minv32, r32, s32, n, si, c->d_partials.p);
+  CgState st = get_state(c, 1);
+  st.bnorm = 1.0;
+  st.alpha = 0.0;
+  st.beta = 0.0;
+  st.pq = 0.0;
+  st.aux[1] = delta;
+  st.aux[2] = st.rr;
+  st.max_iter = o.max_iter;
+  put_state(c, 1, st);
+  const int reps = std::max(1, auto_batch(g, o.check_every) / 2);
+  int parity = 0;  // which P buffer holds p_{k-1}: P1 when parity == 0
+  double best = so_h.rel_res;
+  int best_it = 0;
+  bool stalled = false;
+  CgState sf{};
+  for (;;) {
+    float* Pin = parity ? P0 : P1;
+    float* Pout = parity ? P1 : P0;
+    auto one = [&](float* pi, float* po) {
+      precond_z<float>(c, r32, minv32, si, scale_mul, z32, q32, false);
+      launch_fcg_step<float>(c->stream, pi, po, z32, r32, d32, q32, fac32, c->d_nmask.p, g, K32,
+                             sh32, si, c->d_partials.p);
+      launch_cg_update2<float>(c->stream, r32, q32, minv32, n, si, c->d_partials.p);
+    };
+    auto body = [&]() {
+      one(Pin, Pout);
+      one(Pout, Pin);
+    };
+    // a batch ends on a reliable-update pause, convergence, failure, or
+    // stagnation of the recursive residual (relative to ||b||, as the true
+    // one) by the test of solve_learned
+    auto keep_going = [&](const CgState& sv) {
+      if (sv.rel_res < 0.9 * best) {
+        best = sv.rel_res;
+        best_it = sv.iter;
+      }
+      stalled = !o.learned_no_fallback && sv.iter - best_it > std::max(500, sv.iter / 4);
+      return !stalled;
+    };
+    const int it_before = st.iter;
+    sf = run_batched(c, 1, reps, body, o.wall_limit_ms, t0, timed_out, 0, keep_going);
+    const int done = sf.iter - it_before;
+    *iters_out += done;
+    float* pk = (done % 2 == 1) ? Pout : Pin;  // p of the last completed iteration
+    if (done % 2 == 1) parity ^= 1;
+    if (sf.status != HX_ST_BREAKDOWN && done > 0)
+      launch_axpy_state<float>(c->stream, d32, d32, pk, n, si, 0);  // pending step
+    // fold the FP32 correction into x and replace the residual in FP64
+    launch_ir_correct(c->stream, x, d32, n, so);
+    launch_fill_zero(c->stream, d32, n * sizeof(float));
+    launch_matvec<double>(c->stream, 0, x, q, fac, c->d_nmask.p, g, c->K, shift,
+                          c->d_state.p + 3, c->d_partials.p, nullptr);
+    launch_ir_residual(c->stream, b, q, r32, n, so, c->d_partials.p);
+    so_h = get_state(c, 0);
+    so_h.iter = *iters_out;
+    if (so_h.status != HX_RUNNING) return so_h;  // converged on the true residual (or non-finite)
+    const bool broke = sf.status == HX_ST_BREAKDOWN || sf.status == HX_ST_NONFINITE ||
+                       sf.status == HX_ST_DIVERGED;
+    if (sf.status != HX_RUNNING) stalled = false;
+    if (*timed_out || broke || stalled || *iters_out >= o.max_iter) break;
+    // resume: rz, rr of the replaced residual; p_old, q_old, pq kept; alpha = 0
+    st = get_state(c, 1);
+    launch_cg_init<float>(c->stream, r32, nullptr, minv32, r32, s32, n, si, c->d_partials.p);
+    CgState s2 = get_state(c, 1);
+    s2.bnorm = 1.0;
+    s2.alpha = 0.0;
+    s2.beta = st.beta;
+    s2.pq = st.pq;
+    s2.iter = sf.iter;
+    s2.aux[1] = delta;
+    s2.aux[2] = s2.rr;
+    s2.max_iter = o.max_iter;
+    s2.status = HX_RUNNING;
+    put_state(c, 1, s2);
+    st = s2;
+  }
+  const bool broke = sf.status == HX_ST_BREAKDOWN || sf.status == HX_ST_NONFINITE ||
+                     sf.status == HX_ST_DIVERGED;
+  if (*timed_out || o.learned_no_fallback || !(broke || stalled)) {
+    so_h.status = broke ? sf.status : HX_ST_MAXITER;
+    return so_h;
+  }
+  // fallback: mixed Jacobi-PCG warm-started from the current iterate
+  *fallback = 1;
+  hx_solve_opts oj = o;
+  oj.max_iter = std::max(1, o.max_iter - *iters_out);
+  int inner = 0;
+  CgState sj = solve_mixed(c, fac, b, x, true, shift, oj, t0, timed_out, &inner);
+  *iters_out += inner;
+  return sj;
+}
+
+CgState solve_learned(hx_ctx* c, const double* fac, const double* b, double* x, bool warm,
+                      double shift, const hx_solve_opts& o, double t0, bool* timed_out,
+                      int* fallback, int* iters_out) {
+  const CgState s = learned_fcg(c, fac, b, x, warm, shift, o, t0, timed_out, fallback, iters_out);
+  check_conv_error(c);
+  return s;
+}
+
+CgState solve_learned_mixed(hx_ctx* c, const double* fac, const double* b, double* x, bool warm,
+                            double shift, const hx_solve_opts& o, double t0, bool* timed_out,
+                            int* fallback, int* iters_out) {
+  const CgState s =
+      learned_fcg_mixed(c, fac, b, x, warm, shift, o, t0, timed_out, fallback, iters_out);
+  check_conv_error(c);
+  return s;
 }
 
 // FP64 Jacobi-PCG from zero, storing x every `every` iterations (at most

@@ -486,6 +486,10 @@ template void launch_fcg_step<double>(cudaStream_t, const double*, double*, cons
                                       const double*, double*, double*, const double*,
                                       const uint8_t*, const Grid&, const ElemCoef<double>&,
                                       double, CgState*, double*);
+template void launch_fcg_step<float>(cudaStream_t, const float*, float*, const float*,
+                                     const float*, float*, float*, const float*, const uint8_t*,
+                                     const Grid&, const ElemCoef<float>&, float, CgState*,
+                                     double*);
 
 template void launch_matvec<double>(cudaStream_t, int, const double*, double*, const double*,
                                     const uint8_t*, const Grid&, const ElemCoef<double>&, double,

@@ -124,7 +124,8 @@ CgState get_state(hx_ctx* c, int slot) {
 // wall-clock limit is hit, or after `max_launches` graph launches (0: no
 // limit).  Returns the final state.
 CgState run_batched(hx_ctx* c, int slot, int reps, const std::function<void()>& body,
-                    double wall_limit_ms, double t0, bool* timed_out, int max_launches) {
+                    double wall_limit_ms, double t0, bool* timed_out, int max_launches,
+                    const std::function<bool(const CgState&)>& keep_going) {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   const int64_t before = launch_counter();
@@ -151,6 +152,7 @@ CgState run_batched(hx_ctx* c, int slot, int reps, const std::function<void()>& 
       st = get_state(c, slot);
       if (st.status != HX_RUNNING) break;
       if (max_launches > 0 && nl >= max_launches) break;
+      if (keep_going && !keep_going(st)) break;
       if (wall_limit_ms > 0 && now_ms() - t0 > wall_limit_ms) {
         *timed_out = true;
         break;
@@ -292,9 +294,9 @@ static double true_residual(hx_ctx* c, const double* fac, const double* b, const
 // FP32 residual with it and resumes with the same search direction (no
 // restart).  Convergence is judged only on the FP64 true residual.
 // ---------------------------------------------------------------------------
-static CgState solve_mixed(hx_ctx* c, const double* fac, const double* b, double* x, bool warm,
-                           double shift, const hx_solve_opts& o, double t0, bool* timed_out,
-                           int* inner_total) {
+CgState solve_mixed(hx_ctx* c, const double* fac, const double* b, double* x, bool warm,
+                    double shift, const hx_solve_opts& o, double t0, bool* timed_out,
+                    int* inner_total) {
   const Grid& g = c->g;
   const int64_t n = g.dofs(), ne = g.elems();
   float* fac32 = c->d_fac32.ensure(ne);
@@ -438,8 +440,9 @@ hx_status solve_grid(hx_ctx* c, const double* f, const double* fac, double* u,
   HX_REQUIRE(o.tol > 0, "tol must be > 0");
   HX_REQUIRE(o.preconditioner == HX_PC_JACOBI || o.preconditioner == HX_PC_LEARNED,
              "unknown preconditioner");
-  HX_REQUIRE(o.preconditioner != HX_PC_LEARNED || o.precision == HX_PREC_FP64,
-             "the learned preconditioner runs with FP64 vectors");
+  HX_REQUIRE(o.preconditioner != HX_PC_LEARNED || o.precision == HX_PREC_FP64 ||
+                 o.precision == HX_PREC_MIXED32,
+             "the learned preconditioner runs with FP64 or FP32 (mixed) vectors");
   ensure_workspace(c);
   if (c->bc_dirty) upload_bc(c);
   const Grid& g = c->g;
@@ -475,7 +478,12 @@ hx_status solve_grid(hx_ctx* c, const double* f, const double* fac, double* u,
     CgState st{};
     if (o.preconditioner == HX_PC_LEARNED) {
       int fb = 0, its = 0;
-      st = solve_learned(c, fac, b, u, warm, shift, o, t0, &timed_out, &fb, &its);
+      if (o.precision == HX_PREC_FP64) {
+        st = solve_learned(c, fac, b, u, warm, shift, o, t0, &timed_out, &fb, &its);
+      } else {
+        st = solve_learned_mixed(c, fac, b, u, warm, shift, o, t0, &timed_out, &fb, &its);
+        R.refinements = c->h_state[0].iter;
+      }
       total_iters += its;
       R.fallback_used = fb;
     } else if (o.precision == HX_PREC_FP64) {

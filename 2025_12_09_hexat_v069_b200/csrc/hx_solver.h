@@ -11,8 +11,13 @@ CgState fresh_state(double tol, int max_iter, int check_every, bool divchecks, b
 void put_state(hx_ctx* c, int slot, const CgState& s);
 CgState get_state(hx_ctx* c, int slot);
 int auto_batch(const Grid& g, int check_every);
+// Capture `reps` x body into one CUDA graph and launch it until the state of
+// `slot` leaves HX_RUNNING, `max_launches` (> 0) launches were made, the wall
+// limit passed, or keep_going (if given) returns false for the state read
+// after a launch.
 CgState run_batched(hx_ctx* c, int slot, int reps, const std::function<void()>& body,
-                    double wall_limit_ms, double t0, bool* timed_out, int max_launches);
+                    double wall_limit_ms, double t0, bool* timed_out, int max_launches,
+                    const std::function<bool(const CgState&)>& keep_going = {});
 // node masks, diagonal, shift and M^-1 (FP64) for `fac`; returns max diag
 double jacobi_setup_public(hx_ctx* c, const double* fac, double shift_factor, double* shift_out);
 template <typename T>
@@ -36,6 +41,12 @@ std::function<void()> net_time_body(hx_ctx* c, int which);
 CgState solve_learned(hx_ctx* c, const double* fac, const double* b, double* x, bool warm,
                       double shift, const hx_solve_opts& o, double t0, bool* timed_out,
                       int* fallback, int* iters_out);
+CgState solve_learned_mixed(hx_ctx* c, const double* fac, const double* b, double* x, bool warm,
+                            double shift, const hx_solve_opts& o, double t0, bool* timed_out,
+                            int* fallback, int* iters_out);
+CgState solve_mixed(hx_ctx* c, const double* fac, const double* b, double* x, bool warm,
+                    double shift, const hx_solve_opts& o, double t0, bool* timed_out,
+                    int* inner_total);
 int pcg_snapshots(hx_ctx* c, const double* f, const double* fac, int every, int count,
                   double tol, double* snaps);
 void ensure_workspace(hx_ctx* c);

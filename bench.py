@@ -238,6 +238,8 @@ def run_ours(args):
     }
     if tuple(args.dims) != DIMS:
         out["config"]["workload"] = f"profiling case {tuple(args.dims)} (not the C1 workload)"
+    if rank == 0 and ws == 1 and not args.no_variants:
+        out["variants"] = variants(hx, ctx, f, fac, f_d, fac_d, u_d, lib_stream)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline and tuple(args.dims) == DIMS:
         out["cpu_baseline"] = cpu_baseline(hx, iters, args.cpu_iters)
     if rank == 0:
@@ -245,6 +247,54 @@ def run_ours(args):
     ctx.close()
     if ws > 1:
         dist.destroy_process_group()
+
+
+def variants(hx, ctx, f, fac, f_d, fac_d, u64_d, lib_stream):
+    """The solver forms on the same workload, each timed once on the device
+    after one untimed run: FP64 and mixed (FP32 in FP64 reliable updates)
+    Jacobi-PCG, and flexible CG with the shipped learned preconditioner in
+    FP64 and mixed.  Errors of u, compliance f.u and max von Mises stress
+    against the FP64 Jacobi-PCG solution u64 (the timed solve's result)."""
+    import importlib
+    import torch
+    learned = importlib.import_module(hx.__name__ + ".learned")
+    learned.load_into(ctx)
+    u64 = u64_d.cpu().numpy()
+    c64 = float(f @ u64)
+    vm64 = ctx.stress(u64, fac, 1.0, 0.3)[1]
+    vmax64 = float(np.max(vm64))
+    forms = {"fp64_jacobi": dict(precision=0, preconditioner=0),
+             "mixed32_jacobi": dict(precision=1, preconditioner=0),
+             "fp64_learned_fcg": dict(precision=0, preconditioner=1),
+             "mixed32_learned_fcg": dict(precision=1, preconditioner=1)}
+    out = {}
+    u = torch.zeros_like(u64_d)
+    for name, kw in forms.items():
+        opts = hx.default_opts(tol=1e-6, max_iter=100000, **kw)
+        ctx.solve_device(f_d.data_ptr(), fac_d.data_ptr(), u.data_ptr(), opts=opts)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(lib_stream)
+        rep = ctx.solve_device(f_d.data_ptr(), fac_d.data_ptr(), u.data_ptr(), opts=opts)
+        e1.record(lib_stream)
+        e1.synchronize()
+        uh = u.cpu().numpy()
+        vm = ctx.stress(uh, fac, 1.0, 0.3)[1]
+        out[name] = {
+            "s_per_solve": e0.elapsed_time(e1) / 1e3, "iterations": rep.iterations,
+            "true_rel_res": rep.true_rel_res, "fallback": rep.fallback_used,
+            "refinements": rep.refinements,
+            "u_rel_err": float(np.linalg.norm(uh - u64) / np.linalg.norm(u64)),
+            "compliance_rel_err": abs(float(f @ uh) - c64) / abs(c64),
+            "max_von_mises_rel_err": abs(float(np.max(vm)) - vmax64) / vmax64,
+            "von_mises_rel_err_l2": float(np.linalg.norm(vm - vm64) / np.linalg.norm(vm64))}
+    base = out["fp64_jacobi"]["s_per_solve"]
+    for v in out.values():
+        v["speedup_vs_fp64_jacobi"] = base / v["s_per_solve"]
+    out["_note"] = ("learned forms use the shipped networks trained on 128x64x64 problems; "
+                    "errors against the FP64 Jacobi-PCG solution at rtol 1e-6")
+    return out
 
 
 def _cpu_threads():
@@ -326,6 +376,8 @@ def main():
     ap.add_argument("--precision", type=int, default=0, help="0 fp64, 1 mixed32")
     ap.add_argument("--cpu-iters", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-variants", action="store_true",
+                    help="skip the mixed / learned solver forms")
     ap.add_argument("--dims", type=int, nargs=3, default=list(DIMS),
                     help="grid size; other than 320 160 160 only for profiling")
     args = ap.parse_args()

@@ -284,8 +284,9 @@ HXO_API int hxo_cg_solve(int64_t nN, int64_t nE, const int32_t *elem,
   double *p = (double *)malloc(((size_t)nf + 1) * sizeof(double));
   double *ap = (double *)malloc(((size_t)nf + 1) * sizeof(double));
   double *df = (double *)malloc(((size_t)nf + 1) * sizeof(double));
-  double *full = (double *)calloc((size_t)ndof, sizeof(double));
-  double *yfull = (double *)malloc((size_t)ndof * sizeof(double));
+  const size_t nd = (size_t)(ndof > 0 ? ndof : 1);
+  double *full = (double *)calloc(nd, sizeof(double));
+  double *yfull = (double *)malloc(nd * sizeof(double));
 
   hxo_diagonal(nN, nE, elem, ke, factor, diag);
   double maxd = -INFINITY;
