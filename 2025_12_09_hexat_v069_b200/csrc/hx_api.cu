@@ -329,6 +329,11 @@ HX_API void hx_destroy(hx_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->h_state) cudaFreeHost(c->h_state);
+  for (int i = 0; i < 2; ++i) {
+    if (c->net.side[i]) cudaStreamDestroy(c->net.side[i]);
+    if (c->net.ev_join[i]) cudaEventDestroy(c->net.ev_join[i]);
+  }
+  if (c->net.ev_fork) cudaEventDestroy(c->net.ev_fork);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }

@@ -269,9 +269,9 @@ __global__ void k_restrict_dof(const T* __restrict__ v, const T* __restrict__ mi
   const int64_t nc = (int64_t)gc.nx * gc.ny * gc.nz;
   for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nc;
        n += (int64_t)gridDim.x * blockDim.x) {
-    const int i = (int)(n % gc.nx);
-    const int64_t t = n / gc.nx;
-    const int j = (int)(t % gc.ny), k = (int)(t / gc.ny);
+    const unsigned un = (unsigned)n, t = un / (unsigned)gc.nx;
+    const int i = (int)(un - t * (unsigned)gc.nx);
+    const int j = (int)(t % (unsigned)gc.ny), k = (int)(t / (unsigned)gc.ny);
     float a0 = 0.f, a1 = 0.f, a2 = 0.f;
     for (int dz = -1; dz <= 1; ++dz) {
       const int fz = 2 * k + dz;
@@ -391,9 +391,9 @@ __global__ void k_net_output(const T* __restrict__ r, const T* __restrict__ minv
   double zq = 0.0;
   for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nf;
        n += (int64_t)gridDim.x * blockDim.x) {
-    const int fx = (int)(n % gf.nx);
-    const int64_t tt = n / gf.nx;
-    const int fy = (int)(tt % gf.ny), fz = (int)(tt / gf.ny);
+    const unsigned un = (unsigned)n, tt = un / (unsigned)gf.nx;
+    const int fx = (int)(un - tt * (unsigned)gf.nx);
+    const int fy = (int)(tt % (unsigned)gf.ny), fz = (int)(tt / (unsigned)gf.ny);
     int ix[2], iy[2], iz[2];
     float wx[2], wy[2], wz[2];
     prolong_axis(fx, gc.nx, ix, wx);

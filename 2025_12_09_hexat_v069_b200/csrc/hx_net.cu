@@ -42,6 +42,7 @@ namespace {
 
 constexpr int LP = NET_LAYER_PARAMS;
 constexpr int NP = NET_NET_PARAMS;
+static_assert(NET_NETS >= 1 && NET_NETS <= 3, "one side stream per level beyond the first");
 
 GridN level_grid(const Grid& g, int l) {
   GridN a{g.nxn, g.nyn, g.nzn};
@@ -131,6 +132,15 @@ void net_buffers(hx_ctx* c, bool train) {
       for (auto& a : L.act) a.ensure(nl * 16);
     }
   }
+  for (int l = 2; l <= NET_NETS; ++l)
+    for (auto& b : N.lv[l].pp) b.ensure((size_t)nodes_of(level_grid(c->g, l)) * 16);
+  if (!N.ev_fork) {
+    HX_CUDA(cudaEventCreateWithFlags(&N.ev_fork, cudaEventDisableTiming));
+    for (int i = 0; i < 2; ++i) {
+      HX_CUDA(cudaStreamCreateWithFlags(&N.side[i], cudaStreamNonBlocking));
+      HX_CUDA(cudaEventCreateWithFlags(&N.ev_join[i], cudaEventDisableTiming));
+    }
+  }
   if (train) {
     N.da.ensure(a1);
     N.db.ensure(a1);
@@ -141,18 +151,18 @@ void net_buffers(hx_ctx* c, bool train) {
 const __nv_bfloat16* fwd_w(const hx_ctx* c, int k, int l) { return c->net.wf.p + k * NP + l * LP; }
 const __nv_bfloat16* adj_w(const hx_ctx* c, int k, int l) { return c->net.wb.p + k * NP + l * LP; }
 
-// y = G_k^T G_k x0 on grid g through the two ping-pong buffers (application).
-void stack_apply(hx_ctx* c, int k, const GridN& g, const __nv_bfloat16* x0, __nv_bfloat16* y) {
-  __nv_bfloat16* u = c->net.tmp[0].p;
-  __nv_bfloat16* v = c->net.tmp[1].p;
-  launch_conv3(c->stream, 16, x0, u, fwd_w(c, k, 0), g, c->net.err.p);  // A1
-  launch_conv3(c->stream, 16, u, v, fwd_w(c, k, 1), g, c->net.err.p);   // A2
-  launch_conv3(c->stream, 16, v, u, fwd_w(c, k, 2), g, c->net.err.p);   // A3
-  launch_conv3(c->stream, 16, u, v, fwd_w(c, k, 3), g, c->net.err.p);   // H = G x0
-  launch_conv3(c->stream, 16, v, u, adj_w(c, k, 3), g, c->net.err.p);   // B3
-  launch_conv3(c->stream, 16, u, v, adj_w(c, k, 2), g, c->net.err.p);   // B2
-  launch_conv3(c->stream, 16, v, u, adj_w(c, k, 1), g, c->net.err.p);   // B1
-  launch_conv3(c->stream, 8, u, y, adj_w(c, k, 0), g, c->net.err.p);    // B0 = G^T H, 6 channels
+// y = G_k^T G_k x0 on grid g through the ping-pong buffers u, v, on stream s.
+void stack_apply(hx_ctx* c, cudaStream_t s, int k, const GridN& g, const __nv_bfloat16* x0,
+                 __nv_bfloat16* y, __nv_bfloat16* u, __nv_bfloat16* v) {
+  int* err = c->net.err.p;
+  launch_conv3(s, 16, x0, u, fwd_w(c, k, 0), g, err);  // A1
+  launch_conv3(s, 16, u, v, fwd_w(c, k, 1), g, err);   // A2
+  launch_conv3(s, 16, v, u, fwd_w(c, k, 2), g, err);   // A3
+  launch_conv3(s, 16, u, v, fwd_w(c, k, 3), g, err);   // H = G x0
+  launch_conv3(s, 16, v, u, adj_w(c, k, 3), g, err);   // B3
+  launch_conv3(s, 16, u, v, adj_w(c, k, 2), g, err);   // B2
+  launch_conv3(s, 16, v, u, adj_w(c, k, 1), g, err);   // B1
+  launch_conv3(s, 8, u, y, adj_w(c, k, 0), g, err);    // B0 = G^T H, 6 channels
 }
 
 // y = G_k^T G_k x0 keeping every activation: act = A1 A2 A3 H B3 B2 B1.
@@ -213,15 +223,33 @@ void precond_z(hx_ctx* c, const T* r, const T* minv, CgState* st, double scale_m
   launch_restrict_dof<T>(c->stream, r, minv, st, nullptr, 0, scale_mul, N.lv[1].x.p, gl[0], gl[1]);
   for (int l = 2; l <= NET_NETS; ++l)
     launch_restrict(c->stream, 3, N.lv[l - 1].x.p, N.lv[l].x.p, gl[l - 1], gl[l], false);
+  if (train) {
+    for (int l = NET_NETS; l >= 1; --l) {
+      auto& L = N.lv[l];
+      launch_lift(c->stream, L.x.p, L.feat.p, L.x0.p, nodes_of(gl[l]));
+      stack_forward_train(c, l - 1, gl[l], L.x0.p, L.act, L.y.p);
+    }
+  } else {
+    // the networks of levels 2.. on side streams, level 1 on the main one
+    // (fork/join by events; inside a stream capture these become parallel
+    // branches of the graph)
+    HX_CUDA(cudaEventRecord(N.ev_fork, c->stream));
+    for (int l = 2; l <= NET_NETS; ++l) {
+      cudaStream_t ss = N.side[l - 2];
+      auto& L = N.lv[l];
+      HX_CUDA(cudaStreamWaitEvent(ss, N.ev_fork, 0));
+      launch_lift(ss, L.x.p, L.feat.p, L.x0.p, nodes_of(gl[l]));
+      stack_apply(c, ss, l - 1, gl[l], L.x0.p, L.y.p, L.pp[0].p, L.pp[1].p);
+      HX_CUDA(cudaEventRecord(N.ev_join[l - 2], ss));
+    }
+    auto& L1 = N.lv[1];
+    launch_lift(c->stream, L1.x.p, L1.feat.p, L1.x0.p, nodes_of(gl[1]));
+    stack_apply(c, c->stream, 0, gl[1], L1.x0.p, L1.y.p, N.tmp[0].p, N.tmp[1].p);
+    for (int l = 2; l <= NET_NETS; ++l) HX_CUDA(cudaStreamWaitEvent(c->stream, N.ev_join[l - 2], 0));
+  }
   for (int l = NET_NETS; l >= 1; --l) {
     auto& L = N.lv[l];
-    const int64_t nl = nodes_of(gl[l]);
-    launch_lift(c->stream, L.x.p, L.feat.p, L.x0.p, nl);
-    if (train)
-      stack_forward_train(c, l - 1, gl[l], L.x0.p, L.act, L.y.p);
-    else
-      stack_apply(c, l - 1, gl[l], L.x0.p, L.y.p);
-    launch_unlift(c->stream, L.y.p, L.feat.p, L.acc.p, false, nl);
+    launch_unlift(c->stream, L.y.p, L.feat.p, L.acc.p, false, nodes_of(gl[l]));
     if (l < NET_NETS) launch_prolong(c->stream, N.lv[l + 1].acc.p, L.acc.p, gl[l], gl[l + 1], true);
   }
   launch_net_output<T>(c->stream, r, minv, N.lv[1].acc.p, gl[0], gl[1], st, scale_mul, z, q_old,

@@ -44,7 +44,7 @@ def _solve(ctx, hx, f, fac, **kw):
     return u, rep
 
 
-def train(ctx, dims=(128, 64, 64), problems=20, snaps=128, steps=100, batch=8,
+def train(ctx, dims=(128, 64, 64), problems=60, snaps=128, steps=200, batch=8,
           lr=(3e-4, 1e-4), seed0=1000, init_seed=5, log=None):
     """Train from a fresh initialisation; returns (params, losses).  The
     learning rate steps from lr[0] to lr[1] halfway through."""
@@ -106,8 +106,8 @@ def main(argv=None):
     import time
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
-    ap.add_argument("--problems", type=int, default=20)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--problems", type=int, default=60)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--batch", type=int, default=8)
     ap.add_argument("--lr", type=float, default=3e-4)
     a = ap.parse_args(argv)
