@@ -87,6 +87,13 @@ PROTOTYPES = {
     "hx_net_forward_backward": (_i32, [_vp, _i32, _i32, _i32, _vp, _vp, _vp, _vp]),
     "hx_net_prepare": (_i32, [_vp, _vp]),
     "hx_net_apply": (_i32, [_vp, _vp, _vp]),
+    "hx_simp_device": (_i32, [_vp, _vp, _dbl, _dbl, _dbl, _vp]),
+    "hx_sensitivity_device": (_i32, [_vp, _vp, _vp, _dbl, _dbl, _dbl, _vp]),
+    "hx_compliance_device": (_i32, [_vp, _vp, _vp, C.POINTER(_dbl)]),
+    "hx_oc_update_device": (_i32, [_vp, _vp, _vp, _vp, _dbl, _dbl, _vp, C.POINTER(_dbl),
+                                   C.POINTER(_i32)]),
+    "hx_stress_pnorm": (_i32, [_vp, _i32, _vp, _vp, _dbl, _dbl, _dbl, C.POINTER(_dbl),
+                               C.POINTER(_dbl)]),
     "hx_net_train_step": (_i32, [_vp, _vp, _vp, _dbl, _i32, C.POINTER(_dbl)]),
     "hx_net_train_batch": (_i32, [_vp, _vp, _vp, _i32, _dbl, _i32, C.POINTER(_dbl)]),
     "hx_pcg_snapshots": (_i32, [_vp, _vp, _vp, _i32, _i32, _dbl, _vp, C.POINTER(_i32)]),
@@ -363,6 +370,41 @@ class Context:
                                       _ptr(pr), _ptr(vm), _ptr(vo), _ptr(l1), _ptr(dr)),
                    "hx_stress")
         return pr, vm, vo, l1, dr
+
+    # ---- device-resident loop pieces (device pointers, grid numbering) ----
+    def simp_device(self, rho_ptr, fac_ptr, p=3.0, e0=1.0, emin=1e-9):
+        self.check(self.lib.hx_simp_device(self.h, C.c_void_p(rho_ptr), p, e0, emin,
+                                           C.c_void_p(fac_ptr)), "hx_simp_device")
+
+    def sensitivity_device(self, rho_ptr, u_ptr, dc_ptr, p=3.0, e0=1.0, emin=1e-9):
+        self.check(self.lib.hx_sensitivity_device(self.h, C.c_void_p(rho_ptr), C.c_void_p(u_ptr),
+                                                  p, e0, emin, C.c_void_p(dc_ptr)),
+                   "hx_sensitivity_device")
+
+    def compliance_device(self, f_ptr, u_ptr):
+        c = C.c_double()
+        self.check(self.lib.hx_compliance_device(self.h, C.c_void_p(f_ptr), C.c_void_p(u_ptr),
+                                                 C.byref(c)), "hx_compliance_device")
+        return c.value
+
+    def oc_update_device(self, x_ptr, dc_ptr, xnew_ptr, volfrac, move, dv_ptr=None):
+        lam, steps = C.c_double(), C.c_int32()
+        self.check(self.lib.hx_oc_update_device(self.h, C.c_void_p(x_ptr), C.c_void_p(dc_ptr),
+                                                C.c_void_p(dv_ptr or 0), float(volfrac),
+                                                float(move), C.c_void_p(xnew_ptr),
+                                                C.byref(lam), C.byref(steps)),
+                   "hx_oc_update_device")
+        return lam.value, steps.value
+
+    def stress_pnorm(self, u, density, E, nu, P=8.0):
+        """(sigma_PN, max von Mises) of displacement u (host array)."""
+        u = np.ascontiguousarray(u)
+        density = np.ascontiguousarray(density, dtype=u.dtype)
+        pn, vmax = C.c_double(), C.c_double()
+        self.check(self.lib.hx_stress_pnorm(self.h, _dtype_code(u), _ptr(u), _ptr(density), E, nu,
+                                            float(P), C.byref(pn), C.byref(vmax)),
+                   "hx_stress_pnorm")
+        return pn.value, vmax.value
 
     def compliance(self, f, u):
         f = np.ascontiguousarray(f)

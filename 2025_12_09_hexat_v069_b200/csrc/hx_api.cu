@@ -679,6 +679,36 @@ HX_API hx_status hx_stress(hx_ctx* c, int32_t dt, const void* u, const void* den
   });
 }
 
+HX_API hx_status hx_stress_pnorm(hx_ctx* c, int32_t dt, const void* u, const void* density,
+                                 double E, double nu, double P, double* pnorm, double* vmax) {
+  return guard(c, [&] {
+    need_mesh(c);
+    check_dtype(dt);
+    HX_REQUIRE(u && density && pnorm, "null argument");
+    HX_REQUIRE(P >= 1.0 && std::isfinite(P), "P must be >= 1");
+    hx::ensure_workspace(c);
+    const int64_t ne = c->g.elems(), n = c->g.dofs();
+    double* du = c->d_x.ensure(n);
+    double* dd = c->d_fac.ensure(ne);
+    double* pr = c->d_aux0.ensure(3 * ne);
+    double* vmv = c->d_aux1.ensure(ne);
+    double* vo = c->d_aux2.ensure(6 * ne);
+    double* l1v = c->d_aux3.ensure(ne);
+    double* dv = c->d_aux4.ensure(3 * ne);
+    up_nodes3(c, dt, u, du);
+    if (!identity(c)) HX_CUDA(cudaMemsetAsync(dd, 0, ne * sizeof(double), c->stream));
+    up_elems(c, dt, density, dd);
+    hx::launch_stress(c->stream, du, dd, E, nu, c->g, c->h[0], c->h[1], c->h[2], pr, vmv, vo,
+                      l1v, dv);
+    hx::put_state(c, 3, hx::CgState{});
+    hx::launch_pnorm(c->stream, vmv, ne, P, c->d_state.p + 3, c->d_partials.p);
+    const hx::CgState st = hx::get_state(c, 3);
+    *pnorm = st.aux[0] > 0.0 ? st.aux[0] * std::pow(st.aux[1], 1.0 / P) : 0.0;
+    if (vmax) *vmax = st.aux[0];
+    return HX_OK;
+  });
+}
+
 HX_API hx_status hx_compute_stress_field(hx_ctx* c, const float* nodes, int64_t nN,
                                          const int64_t* elements, int64_t nE, const float* U,
                                          float E, float nu, const float* density,
@@ -758,6 +788,75 @@ HX_API hx_status hx_oc_update(hx_ctx* c, int32_t dt, const void* x, const void* 
     download(c, dt, dxn, none, ne, ne, 1, xnew);
     if (lambda) *lambda = c->h_state[3].aux[2];
     if (steps) *steps = c->h_state[3].iter;
+    return HX_OK;
+  });
+}
+
+// ---- device-resident pieces of the optimisation loop (grid numbering) ----
+static void need_grid_numbering(hx_ctx* c) {
+  need_mesh(c);
+  HX_REQUIRE(identity(c), "device-array entry points need a grid mesh (hx_set_grid)");
+}
+
+HX_API hx_status hx_simp_device(hx_ctx* c, const double* rho, double p, double e0, double emin,
+                                double* fac) {
+  return guard(c, [&] {
+    need_grid_numbering(c);
+    HX_REQUIRE(rho && fac, "null argument");
+    HX_REQUIRE(p >= 1.0 && e0 > emin && emin >= 0.0, "bad SIMP parameters");
+    hx::launch_simp(c->stream, rho, p, e0, emin, fac, c->g.elems(), false);
+    HX_CUDA(cudaStreamSynchronize(c->stream));
+    return HX_OK;
+  });
+}
+
+HX_API hx_status hx_sensitivity_device(hx_ctx* c, const double* rho, const double* u, double p,
+                                       double e0, double emin, double* dc) {
+  return guard(c, [&] {
+    need_grid_numbering(c);
+    HX_REQUIRE(rho && u && dc, "null argument");
+    HX_REQUIRE(p >= 1.0 && e0 > emin && emin >= 0.0, "bad SIMP parameters");
+    hx::launch_energy(c->stream, u, c->g, c->K, dc);
+    hx::launch_simp(c->stream, rho, p, e0, emin, dc, c->g.elems(), true);
+    HX_CUDA(cudaStreamSynchronize(c->stream));
+    return HX_OK;
+  });
+}
+
+HX_API hx_status hx_compliance_device(hx_ctx* c, const double* f, const double* u, double* out) {
+  return guard(c, [&] {
+    need_grid_numbering(c);
+    HX_REQUIRE(f && u && out, "null argument");
+    hx::ensure_workspace(c);
+    hx::put_state(c, 3, hx::CgState{});
+    hx::launch_dot(c->stream, f, u, c->g.dofs(), c->d_state.p + 3, c->d_partials.p,
+                   c->d_scalars.p);
+    HX_CUDA(cudaMemcpyAsync(out, c->d_scalars.p, sizeof(double), cudaMemcpyDeviceToHost,
+                            c->stream));
+    HX_CUDA(cudaStreamSynchronize(c->stream));
+    return HX_OK;
+  });
+}
+
+HX_API hx_status hx_oc_update_device(hx_ctx* c, const double* x, const double* dc,
+                                     const double* dv, double volfrac, double move, double* xnew,
+                                     double* lambda, int32_t* steps) {
+  return guard(c, [&] {
+    need_grid_numbering(c);
+    HX_REQUIRE(x && dc && xnew, "null argument");
+    HX_REQUIRE(volfrac > 0 && volfrac <= 1, "volfrac must lie in (0, 1]");
+    HX_REQUIRE(move > 0, "move must be positive");
+    hx::ensure_workspace(c);
+    hx::CgState s{};
+    s.aux[0] = 0.0;
+    s.aux[1] = 1e9;
+    s.status = hx::HX_RUNNING;
+    hx::put_state(c, 3, s);
+    hx::launch_oc(c->stream, x, dc, dv, c->g.elems(), volfrac, move, xnew, c->d_state.p + 3,
+                  c->d_partials.p, 100);
+    const hx::CgState r = hx::get_state(c, 3);
+    if (lambda) *lambda = r.aux[2];
+    if (steps) *steps = r.iter;
     return HX_OK;
   });
 }

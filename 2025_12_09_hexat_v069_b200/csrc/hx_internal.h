@@ -136,6 +136,12 @@ void launch_stress(cudaStream_t s, const double* u, const double* dens, double E
                    double* voigt, double* l1, double* dir);
 void launch_energy(cudaStream_t s, const double* u, const Grid& g, const ElemCoef<double>& K,
                    double* ce);
+// fac = emin + rho^p (e0 - emin); sensitivity: out = -p rho^(p-1) (e0 - emin) * out
+void launch_simp(cudaStream_t s, const double* rho, double p, double e0, double emin, double* out,
+                 int64_t n, bool sensitivity);
+// sigma_PN = (sum vm^P)^(1/P): st->aux[0] = max vm, st->aux[1] = sum (vm/max)^P
+void launch_pnorm(cudaStream_t s, const double* vm, int64_t n, double P, CgState* st,
+                  double* partials);
 void launch_oc(cudaStream_t s, const double* x, const double* dc, const double* dv, int64_t n,
                double volfrac, double move, double* xnew, CgState* st, double* partials,
                int max_steps);

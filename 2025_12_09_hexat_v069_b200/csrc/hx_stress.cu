@@ -157,7 +157,7 @@ __global__ void k_oc_step(const double* __restrict__ x, const double* __restrict
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n;
        e += (int64_t)gridDim.x * blockDim.x) {
     const double xe = x[e];
-    const double be = sqrt(fmax(-dc[e], 0.0) / (lmid * dv[e]));
+    const double be = sqrt(fmax(-dc[e], 0.0) / (lmid * (dv ? dv[e] : 1.0)));
     double xn = xe * be;
     const double lo = fmax(0.0, xe - move), hi = fmin(1.0, xe + move);
     xn = fmin(fmax(xn, lo), hi);
@@ -179,6 +179,43 @@ __global__ void k_oc_step(const double* __restrict__ x, const double* __restrict
   }
 }
 
+// SIMP: fac = emin + max(rho, 0)^p (e0 - emin).  With u (sensitivity mode):
+// out = -p max(rho, 0)^(p-1) (e0 - emin) * ce, ce the unit-modulus element
+// energies u_e^T Ke u_e already in `out`.
+__global__ void k_simp(const double* __restrict__ rho, double p, double e0, double emin,
+                       double* __restrict__ out, int64_t n, int sensitivity) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const double r = fmax(rho[e], 0.0);
+    out[e] = sensitivity ? -p * pow(r, p - 1.0) * (e0 - emin) * out[e]
+                         : emin + pow(r, p) * (e0 - emin);
+  }
+}
+
+// p-norm aggregate of the element von Mises stresses, in two passes for
+// range safety: pass 0 reduces m = max vm into st->aux[0]; pass 1 reduces
+// sum (vm / m)^P into st->aux[1].  sigma_PN = m * aux[1]^(1/P).
+__global__ void k_pnorm(const double* __restrict__ vm, int64_t n, double P, int pass,
+                        CgState* st, double* partials) {
+  const double m = pass ? st->aux[0] : 0.0;
+  double acc = 0.0;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const double v = vm[e];
+    if (pass == 0)
+      acc = fmax(acc, v);
+    else if (m > 0.0)
+      acc += pow(v / m, P);
+  }
+  double r[1] = {acc};
+  if (pass == 0) {
+    if (grid_reduce<1, true>(r, partials, &st->ticket[TK_AUX]) && threadIdx.x == 0)
+      st->aux[0] = r[0];
+  } else {
+    if (grid_reduce<1>(r, partials, &st->ticket[TK_AUX2]) && threadIdx.x == 0) st->aux[1] = r[0];
+  }
+}
+
 unsigned eblocks(int64_t n) {
   return (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv(n, 128), 32LL * sm_count()));
 }
@@ -191,6 +228,22 @@ void launch_stress(cudaStream_t s, const double* u, const double* dens, double E
   k_stress<<<eblocks(g.elems()), 128, 0, s>>>(u, dens, E, nu, g, hx, hy, hz, principal, vm, voigt,
                                               l1, dir);
   HX_CHECK_LAUNCH();
+}
+
+void launch_simp(cudaStream_t s, const double* rho, double p, double e0, double emin, double* out,
+                 int64_t n, bool sensitivity) {
+  k_simp<<<eblocks(n), 128, 0, s>>>(rho, p, e0, emin, out, n, sensitivity ? 1 : 0);
+  HX_CHECK_LAUNCH();
+}
+
+void launch_pnorm(cudaStream_t s, const double* vm, int64_t n, double P, CgState* st,
+                  double* partials) {
+  const unsigned blocks =
+      (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv(n, 256), 8LL * sm_count()));
+  for (int pass = 0; pass < 2; ++pass) {
+    k_pnorm<<<blocks, 256, 0, s>>>(vm, n, P, pass, st, partials);
+    HX_CHECK_LAUNCH();
+  }
 }
 
 void launch_energy(cudaStream_t s, const double* u, const Grid& g, const ElemCoef<double>& K,

@@ -82,6 +82,37 @@ def train(ctx, dims=(128, 64, 64), problems=60, snaps=128, steps=200, batch=8,
     return ctx.net_get_params(), np.array(losses)
 
 
+def finetune(ctx, f_d, fac_d, u_star, steps=40, batch=4, lr=1e-4, snaps=16, every=64,
+             snap_tol=1e-3, seed=0):
+    """Fine-tunes the loaded networks on the current system (device f, factors,
+    and its solution u_star, e.g. the last solve to rtol 1e-6): `snaps`
+    Jacobi-PCG iterates every `every` iterations up to rtol snap_tol, then
+    `steps` Adam steps on batches of (r, e = u_star - x_k) pairs.  The Adam
+    moments restart (hx_net_set_params)."""
+    import torch
+    n = f_d.numel()
+    ctx.net_set_params(ctx.net_get_params())
+    X = torch.zeros((snaps, n), dtype=torch.float64, device=f_d.device)
+    torch.cuda.current_stream().synchronize()
+    taken = ctx.pcg_snapshots(f_d.data_ptr(), fac_d.data_ptr(), every, snaps, snap_tol,
+                              X.data_ptr())
+    ctx.net_prepare(fac_d.data_ptr())
+    rng = np.random.default_rng(seed)
+    R = torch.empty((batch, n), dtype=torch.float64, device=f_d.device)
+    E = torch.empty_like(R)
+    losses = []
+    for _ in range(steps):
+        ks = rng.integers(taken, size=batch)
+        for b, k in enumerate(ks):
+            ctx.residual_device(f_d.data_ptr(), fac_d.data_ptr(), X[k].data_ptr(), R[b].data_ptr())
+            torch.sub(u_star, X[k], out=E[b])
+        torch.cuda.current_stream().synchronize()
+        losses.append(ctx.net_train_batch([R[b].data_ptr() for b in range(batch)],
+                                          [E[b].data_ptr() for b in range(batch)], lr, 0))
+    del X, R, E
+    return np.array(losses)
+
+
 def save_params(path, params):
     os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
     np.save(path, np.asarray(params, np.float32))

@@ -13,6 +13,11 @@ F = (vol/64) S^T A^-1 S is symmetric, so F^T = F):
     dc_x = F(dc);  x <- OC(x, dc_x, dv=1, volfrac, move)
 
 The bisection keeps sum(x_new) <= volfrac*nE on the design variables.
+
+run_oc takes host arrays (each call copies through the C ABI); run_oc_device
+keeps the whole iteration on the GPU (grid meshes) and can solve with the
+mixed-precision and learned forms, fine-tuning the learned preconditioner
+every few iterations on the current design.
 """
 import time
 
@@ -63,4 +68,60 @@ def run_oc(ctx: Context, bc_indicator, f, volfrac, radius, n_iter, p=3.0, e0=1.0
         if callback:
             callback(it, c, rep)
     res.x, res.rho, res.u = x, rho, u
+    return res
+
+
+def run_oc_device(ctx: Context, bc_indicator, f, volfrac, radius, n_iter, p=3.0, e0=1.0,
+                  emin=1e-9, nu=0.3, move=0.2, tol=1e-6, ref_compat=0, filter_tol=1e-5,
+                  filter_max_iter=200, precision=0, preconditioner=0, max_iter=200000,
+                  finetune_every=0, finetune_kw=None, callback=None):
+    """The OC loop of run_oc on device arrays (the mesh set by hx_set_grid):
+    filter, SIMP, warm-started solve (precision / preconditioner as in
+    hx_solve_opts), compliance, sensitivities, filtered sensitivities and the
+    OC update all run on the GPU; only scalars come back.  With the learned
+    preconditioner and finetune_every > 0 the networks are fine-tuned on the
+    current design every finetune_every iterations (learned.finetune)."""
+    import importlib
+
+    import torch
+    (nx, ny, nz), _ = ctx.grid()
+    ne = nx * ny * nz
+    ctx.set_material(1.0, nu)
+    ctx.set_bc(bc_indicator)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    f_d = torch.from_numpy(np.ascontiguousarray(f, dtype=np.float64)).to(dev)
+    x = torch.full((ne,), float(volfrac), dtype=torch.float64, device=dev)
+    xn, rho, fac, dc, dcf = (torch.empty_like(x) for _ in range(5))
+    u = torch.zeros_like(f_d)
+    torch.cuda.current_stream().synchronize()
+    learned = importlib.import_module(__package__ + ".learned") if finetune_every else None
+    res = OCResult()
+    res.finetune_ms = []
+    for it in range(n_iter):
+        ctx.filter_device(x.data_ptr(), rho.data_ptr(), radius, ref_compat, filter_tol,
+                          filter_max_iter)
+        ctx.simp_device(rho.data_ptr(), fac.data_ptr(), p, e0, emin)
+        opts = default_opts(tol=tol, max_iter=max_iter, precision=precision,
+                            preconditioner=preconditioner, warm_start=1 if it else 0)
+        t0 = time.perf_counter()
+        rep = ctx.solve_device(f_d.data_ptr(), fac.data_ptr(), u.data_ptr(), opts=opts,
+                               ok=(HX_OK, HX_NOT_CONVERGED))
+        res.solve_ms.append((time.perf_counter() - t0) * 1e3)
+        c = ctx.compliance_device(f_d.data_ptr(), u.data_ptr())
+        ctx.sensitivity_device(rho.data_ptr(), u.data_ptr(), dc.data_ptr(), p, e0, emin)
+        ctx.filter_device(dc.data_ptr(), dcf.data_ptr(), radius, ref_compat, filter_tol,
+                          filter_max_iter)
+        ctx.oc_update_device(x.data_ptr(), dcf.data_ptr(), xn.data_ptr(), volfrac, move)
+        res.change.append(float((xn - x).abs().max()))  # torch, then synchronised
+        res.compliance.append(c)
+        res.iterations.append(rep.iterations)
+        x, xn = xn, x
+        if callback:
+            callback(it, c, rep)
+        if learned and preconditioner == 1 and (it + 1) % finetune_every == 0 and it + 1 < n_iter:
+            t1 = time.perf_counter()
+            learned.finetune(ctx, f_d, fac, u, **(finetune_kw or {}))
+            res.finetune_ms.append((time.perf_counter() - t1) * 1e3)
+    torch.cuda.current_stream().synchronize()
+    res.x, res.rho, res.u = x.cpu().numpy(), rho.cpu().numpy(), u.cpu().numpy()
     return res

@@ -244,6 +244,14 @@ HX_API hx_status hx_stress(hx_ctx *ctx, int32_t dtype, const void *u,
                            const void *density, double E, double nu,
                            void *principal, void *vonmises, void *voigt,
                            void *l1, void *dir);
+/* p-norm aggregate of the element von Mises stresses (no reference
+ * counterpart; the stress-constrained loop's aggregate):
+ * *pnorm = (sum_e vm_e^P)^(1/P), vm as in hx_stress (0 for void elements),
+ * formed as max(vm) * (sum (vm/max)^P)^(1/P) in FP64 on the device;
+ * *vmax = max vm (may be NULL).  P >= 1 (8 in the stress-aggregated loop). */
+HX_API hx_status hx_stress_pnorm(hx_ctx *ctx, int32_t dtype, const void *u,
+                                 const void *density, double E, double nu,
+                                 double P, double *pnorm, double *vmax);
 /* Drop-in for Stress.compute_stress_field(nodes, elements, U, E, nu,
  * density), src/Core/Stress.jl:57-100. */
 HX_API hx_status hx_compute_stress_field(
@@ -269,6 +277,26 @@ HX_API hx_status hx_oc_update(hx_ctx *ctx, int32_t dtype, const void *x,
                               const void *dc, const void *dv, double volfrac,
                               double move, void *xnew, double *lambda,
                               int32_t *steps);
+
+/* ---- device-resident optimisation loop pieces ---------------------------------------
+ * No reference counterpart (the OC loop is the published method).  FP64
+ * device arrays in grid numbering; need a grid mesh (hx_set_grid).  With
+ * hx_filter_device and hx_solve_device they keep an OC iteration on the
+ * device.  fac = emin + max(rho,0)^p (e0 - emin);  dc = -p max(rho,0)^(p-1)
+ * (e0 - emin) u_e^T Ke u_e;  *c = f.u (FP64);  OC bisection as hx_oc_update
+ * (dv NULL: unit volumes). */
+HX_API hx_status hx_simp_device(hx_ctx *ctx, const double *rho_dev, double p,
+                                double e0, double emin, double *fac_dev);
+HX_API hx_status hx_sensitivity_device(hx_ctx *ctx, const double *rho_dev,
+                                       const double *u_dev, double p, double e0,
+                                       double emin, double *dc_dev);
+HX_API hx_status hx_compliance_device(hx_ctx *ctx, const double *f_dev,
+                                      const double *u_dev, double *c);
+HX_API hx_status hx_oc_update_device(hx_ctx *ctx, const double *x_dev,
+                                     const double *dc_dev, const double *dv_dev,
+                                     double volfrac, double move,
+                                     double *xnew_dev, double *lambda,
+                                     int32_t *steps);
 
 /* ---- learned preconditioner -----------------------------------------------------
  * No reference counterpart.  z = D^-1/2 (I + sum_l R_l^T E_l^T G_l^T G_l E_l R_l) D^-1/2 r

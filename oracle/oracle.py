@@ -140,6 +140,18 @@ def stress(conn0, nodes, u, E, nu, density):
     return tuple(out)
 
 
+def stress_pnorm(conn0, nodes, u, E, nu, density, P=8.0):
+    """p-norm aggregate of the element von Mises stresses (the published
+    aggregation of stress-constrained topology optimisation; no reference
+    counterpart): (sum_e vm_e^P)^(1/P) = m (sum (vm_e / m)^P)^(1/P), m = max vm.
+    Returns (pnorm, m)."""
+    vm = stress(conn0, nodes, u, E, nu, density)[1]
+    m = float(vm.max())
+    if m <= 0.0:
+        return 0.0, m
+    return m * float(np.sum((vm / m) ** P)) ** (1.0 / P), m
+
+
 def element_energy(conn0, ke, u):
     conn0 = _c(conn0, np.int32)
     ce = np.zeros(conn0.shape[0])

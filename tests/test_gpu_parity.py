@@ -218,6 +218,23 @@ def test_stress_matches_oracle(ctx, hx, orc):
     assert np.all(got[0][::7] == 0)
 
 
+def test_stress_pnorm_matches_oracle(ctx, hx, orc):
+    dims = (11, 6, 5)
+    nodes, el, c0 = _setup(ctx, hx, dims)
+    rng = np.random.default_rng(21)
+    u = rng.standard_normal(3 * nodes.shape[0]) * 1e-2
+    dens = rng.uniform(0, 1, c0.shape[0])
+    dens[::5] = 1e-8  # void elements contribute nothing
+    for P in (1.0, 8.0, 32.0):
+        pn, vmax = ctx.stress_pnorm(u, dens, 1.5, 0.3, P)
+        want, wmax = orc.stress_pnorm(c0, nodes, u, 1.5, 0.3, dens, P)
+        assert vmax == pytest.approx(wmax, rel=1e-12)
+        assert pn == pytest.approx(want, rel=1e-12)
+    # the aggregate lies between the max and N^(1/P) times the max
+    pn8, vmax = ctx.stress_pnorm(u, dens, 1.5, 0.3, 8.0)
+    assert vmax <= pn8 <= vmax * c0.shape[0] ** (1 / 8.0)
+
+
 def test_compute_stress_field_reference_shaped(ctx, hx, orc):
     from importlib import import_module
     api = import_module("2025_12_09_hexat_v069_b200.api")
