@@ -329,10 +329,10 @@ def test_batch_step_sums_single_gradients(ctx, hx):
 
 
 def test_shipped_weights_gain_on_unseen_problem(ctx, hx):
-    """The committed networks (trained on 128x64x64 problems) on an unseen
-    seeded problem of another size: FCG converges on the true residual in
-    at least 1.6x fewer iterations than Jacobi-PCG (measured: 709 against
-    1345; the gain grows with the grid, 3.6x at 320x160x160)."""
+    """The committed networks (trained on a mixture of grids up to 128x64x64)
+    on an unseen seeded problem: FCG converges on the true residual in at
+    least 1.6x fewer iterations than Jacobi-PCG (the gain grows with the
+    grid: 5.3x at 320x160x160)."""
     import torch
     from importlib import import_module
     learned = import_module(hx.__name__ + ".learned")
