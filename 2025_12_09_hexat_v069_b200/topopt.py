@@ -74,13 +74,29 @@ def run_oc(ctx: Context, bc_indicator, f, volfrac, radius, n_iter, p=3.0, e0=1.0
 def run_oc_device(ctx: Context, bc_indicator, f, volfrac, radius, n_iter, p=3.0, e0=1.0,
                   emin=1e-9, nu=0.3, move=0.2, tol=1e-6, ref_compat=0, filter_tol=1e-5,
                   filter_max_iter=200, precision=0, preconditioner=0, max_iter=200000,
-                  finetune_every=0, finetune_kw=None, callback=None):
+                  finetune_every=0, finetune_kw=None, adaptive=True, retry_every=20,
+                  shift_factor=0.0, callback=None):
     """The OC loop of run_oc on device arrays (the mesh set by hx_set_grid):
     filter, SIMP, warm-started solve (precision / preconditioner as in
     hx_solve_opts), compliance, sensitivities, filtered sensitivities and the
     OC update all run on the GPU; only scalars come back.  With the learned
     preconditioner and finetune_every > 0 the networks are fine-tuned on the
-    current design every finetune_every iterations (learned.finetune)."""
+    current design every finetune_every iterations (learned.finetune).
+
+    adaptive (learned preconditioner only): the first solve uses Jacobi and
+    its time and iteration count are kept; a learned solve may take at most
+    that many iterations (a learned iteration costs more than a Jacobi one)
+    and, if it has not converged by then, is finished by Jacobi-PCG from its
+    iterate.  A learned solve slower than the latest Jacobi solve, or one
+    that fell back or was finished by Jacobi, switches the following solves
+    to Jacobi until the next fine-tuning or `retry_every` iterations later.
+    On designs unlike its training data the networks can cost more than they
+    save, and this keeps the loop near Jacobi's cost there.  res.pc_used
+    records the choice per iteration.
+
+    shift_factor: the regularisation shift of hx_solve_opts (the reference's
+    solve_system_gpu default is 1e-6), needed when the supports leave a
+    rigid mode free."""
     import importlib
 
     import torch
@@ -97,16 +113,43 @@ def run_oc_device(ctx: Context, bc_indicator, f, volfrac, radius, n_iter, p=3.0,
     learned = importlib.import_module(__package__ + ".learned") if finetune_every else None
     res = OCResult()
     res.finetune_ms = []
+    res.pc_used = []
+    use_learned = preconditioner == 1 and not adaptive
+    jac_ms = jac_its = None
+    retry_at = 0
     for it in range(n_iter):
+        if preconditioner == 1 and adaptive and not use_learned and jac_ms is not None \
+                and it >= retry_at:
+            use_learned = True
+        pc = 1 if use_learned else 0
         ctx.filter_device(x.data_ptr(), rho.data_ptr(), radius, ref_compat, filter_tol,
                           filter_max_iter)
         ctx.simp_device(rho.data_ptr(), fac.data_ptr(), p, e0, emin)
-        opts = default_opts(tol=tol, max_iter=max_iter, precision=precision,
-                            preconditioner=preconditioner, warm_start=1 if it else 0)
+        cap = max_iter
+        if pc == 1 and adaptive and jac_its is not None:
+            cap = min(max_iter, max(jac_its, 50))
+        opts = default_opts(tol=tol, max_iter=cap, precision=precision, preconditioner=pc,
+                            warm_start=1 if it else 0, shift_factor=shift_factor)
         t0 = time.perf_counter()
         rep = ctx.solve_device(f_d.data_ptr(), fac.data_ptr(), u.data_ptr(), opts=opts,
                                ok=(HX_OK, HX_NOT_CONVERGED))
-        res.solve_ms.append((time.perf_counter() - t0) * 1e3)
+        finished_by_jacobi = False
+        if pc == 1 and rep.status != HX_OK:
+            opts = default_opts(tol=tol, max_iter=max_iter, precision=precision, preconditioner=0,
+                                warm_start=1, shift_factor=shift_factor)
+            rep2 = ctx.solve_device(f_d.data_ptr(), fac.data_ptr(), u.data_ptr(), opts=opts,
+                                    ok=(HX_OK, HX_NOT_CONVERGED))
+            rep2.iterations += rep.iterations
+            rep, finished_by_jacobi = rep2, True
+        ms = (time.perf_counter() - t0) * 1e3
+        res.solve_ms.append(ms)
+        res.pc_used.append(pc)
+        if preconditioner == 1 and adaptive:
+            if pc == 0:
+                jac_ms, jac_its = ms, rep.iterations
+            elif rep.fallback_used or finished_by_jacobi or (jac_ms is not None and ms > jac_ms):
+                use_learned = False
+                retry_at = it + retry_every
         c = ctx.compliance_device(f_d.data_ptr(), u.data_ptr())
         ctx.sensitivity_device(rho.data_ptr(), u.data_ptr(), dc.data_ptr(), p, e0, emin)
         ctx.filter_device(dc.data_ptr(), dcf.data_ptr(), radius, ref_compat, filter_tol,
@@ -122,6 +165,7 @@ def run_oc_device(ctx: Context, bc_indicator, f, volfrac, radius, n_iter, p=3.0,
             t1 = time.perf_counter()
             learned.finetune(ctx, f_d, fac, u, **(finetune_kw or {}))
             res.finetune_ms.append((time.perf_counter() - t1) * 1e3)
+            retry_at = it + 1  # the fine-tuned networks get the next solve
     torch.cuda.current_stream().synchronize()
     res.x, res.rho, res.u = x.cpu().numpy(), rho.cpu().numpy(), u.cpu().numpy()
     return res

@@ -82,8 +82,9 @@ def test_gpu_device_loop_matches_oracle(ctx, hx):
 @pytest.mark.gpu
 def test_gpu_learned_mixed_loop_with_finetuning(ctx, hx):
     """Mixed-precision learned FCG solves inside the device loop, with the
-    networks fine-tuned every 5 iterations: same compliance history as the
-    oracle's FP64 loop to the solver tolerance, no fallback."""
+    networks fine-tuned every 5 iterations and the adaptive choice between
+    learned and Jacobi solves: same compliance history as the oracle's FP64
+    loop to the solver tolerance."""
     from importlib import import_module
     topopt = import_module(hx.__name__ + ".topopt")
     learned = import_module(hx.__name__ + ".learned")
@@ -92,16 +93,17 @@ def test_gpu_learned_mixed_loop_with_finetuning(ctx, hx):
     nodes, el, bc, f = hx.workloads.cantilever(*dims)
     ctx.set_grid(*dims)
     learned.load_into(ctx)
-    fallbacks = []
+    used = []
     res = topopt.run_oc_device(ctx, bc, f, prm["volfrac"], prm["radius"], 15, p=prm["p"],
                                e0=prm["e0"], emin=prm["emin"], nu=prm["nu"], move=prm["move"],
                                tol=prm["tol"], ref_compat=prm["ref_compat"],
                                filter_tol=prm["filter_tol"],
                                filter_max_iter=prm["filter_max_iter"], precision=1,
                                preconditioner=1, finetune_every=5,
-                               callback=lambda it, c, rep: fallbacks.append(rep.fallback_used))
+                               callback=lambda it, c, rep: used.append(rep.fallback_used))
     rel = np.abs(np.array(res.compliance) - g["compliance"][:15]) / g["compliance"][:15]
     print(f"learned+mixed C0 loop: max rel compliance diff {rel.max():.2e}, "
-          f"{len(res.finetune_ms)} fine-tunings, solve its {res.iterations}")
+          f"{len(res.finetune_ms)} fine-tunings, solve its {res.iterations}, "
+          f"learned solves {res.pc_used}")
     assert rel.max() <= 1e-4
-    assert sum(fallbacks) == 0 and len(res.finetune_ms) == 2
+    assert len(res.finetune_ms) == 2 and res.pc_used[0] == 0 and res.pc_used[1] == 1
