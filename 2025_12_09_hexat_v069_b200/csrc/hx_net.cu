@@ -479,7 +479,7 @@ std::function<void()> net_time_body(hx_ctx* c, int which) {
   auto& N = c->net;
   const Grid g = c->g;
   const int64_t n = g.dofs();
-  HX_REQUIRE(c->d_r.n >= (size_t)n, "run a solve before timing the network");
+  HX_REQUIRE(c->d_b.n >= (size_t)n, "run a solve before timing the network");
   net_buffers(c, false);
   if (which == 0) {  // one 16 -> 16 layer on the level-1 grid
     const GridN g1 = level_grid(g, 1);
@@ -490,15 +490,15 @@ std::function<void()> net_time_body(hx_ctx* c, int which) {
                    c->net.err.p);
     };
   }
-  // the state of slot 3 holds r.M^-1 r of the last solve's residual
+  // applied to the last solve's right-hand side b; state slot 3 holds b.M^-1 b
   CgState* s3 = c->d_state.p + 3;
   HX_CUDA(cudaMemsetAsync(s3, 0, sizeof(CgState), c->stream));
-  launch_cg_init<double>(c->stream, c->d_r.p, nullptr, c->d_minv.p, c->d_aux1.ensure(n),
+  launch_cg_init<double>(c->stream, c->d_b.p, nullptr, c->d_minv.p, c->d_aux1.ensure(n),
                          c->d_aux2.ensure(n), n, s3, c->d_partials.p);
   double* z = N.z.ensure(n);
   return [c, s3, z, n] {
     const double scale_mul = 1.0 / (double)n;
-    precond_z<double>(c, c->d_r.p, c->d_minv.p, s3, scale_mul, z, nullptr, false);
+    precond_z<double>(c, c->d_b.p, c->d_minv.p, s3, scale_mul, z, nullptr, false);
   };
 }
 

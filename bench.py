@@ -28,7 +28,6 @@ sys.path.insert(0, ROOT)
 METRIC = "s per solve to rtol 1e-6 at 8.2M Hex8, learned+mixed vs plain FP64; HBM GB/s"
 DIMS = (320, 160, 160)
 SEED = 20251209
-PEAKS = {"hbm_gbs": 6545.9, "source": "fallback"}
 
 
 def load_peaks():
@@ -36,8 +35,9 @@ def load_peaks():
     if os.path.exists(p):
         with open(p) as fh:
             d = json.load(fh)
-        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
-    return {"hbm_gbs": 6650.0, "source": "fallback"}
+        return {"hbm_gbs": float(d["hbm_gbs"]), "bf16_tflops": float(d["bf16_tflops"]),
+                "source": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
 
 
 def dist_info():
@@ -109,6 +109,13 @@ def c1_inputs(hx, ctx, dims=DIMS):
     return f, fac, frep
 
 
+FORMS = {"fp64_jacobi": (0, 0), "mixed32_jacobi": (1, 0), "fp64_learned_fcg": (0, 1),
+         "mixed32_learned_fcg": (1, 1)}
+DTYPES = {"fp64_jacobi": "f64", "mixed32_jacobi": "f32 in f64 reliable updates",
+          "fp64_learned_fcg": "f64 vectors, bf16 network",
+          "mixed32_learned_fcg": "f32 vectors in f64 reliable updates, bf16 network"}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -121,6 +128,7 @@ def run_ours(args):
     import importlib
     hx = importlib.import_module("2025_12_09_hexat_v069_b200")
     L = importlib.import_module("2025_12_09_hexat_v069_b200._lib")
+    learned = importlib.import_module("2025_12_09_hexat_v069_b200.learned")
     ctx = hx.Context(local)
     f, fac, frep = c1_inputs(hx, ctx, tuple(args.dims))
     n, ne = f.shape[0], fac.shape[0]
@@ -128,7 +136,10 @@ def run_ours(args):
     f_d = torch.from_numpy(f).to(dev)
     fac_d = torch.from_numpy(fac).to(dev)
     u_d = torch.zeros(n, dtype=torch.float64, device=dev)
-    opts = hx.default_opts(tol=1e-6, max_iter=100000, precision=args.precision)
+    prec, pc = FORMS[args.solver]
+    if pc:
+        learned.load_into(ctx)
+    opts = hx.default_opts(tol=1e-6, max_iter=100000, precision=prec, preconditioner=pc)
     lib_stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
 
     def barrier():
@@ -165,6 +176,7 @@ def run_ours(args):
     t_dev = max_over_ranks(e0.elapsed_time(e1) / 1e3)
     iters = reps[-1].iterations
     true_rel = reps[-1].true_rel_res
+    fallbacks = sum(int(r.fallback_used) for r in reps)
     # ---- e2e: host (pinned) buffers through the C ABI ----
     f_h = torch.from_numpy(f).pin_memory()
     fac_h = torch.from_numpy(fac).pin_memory()
@@ -184,64 +196,55 @@ def run_ours(args):
     e3.synchronize()
     barrier()
     t_e2e = max_over_ranks(e2.elapsed_time(e3) / 1e3)
-    # ---- live per-kernel timing for the roofline ----
-    t_st = ctx.time_kernel(L.HX_KERNEL_PCG_STEP_FP64, 20)
-    t_up = ctx.time_kernel(L.HX_KERNEL_PCG_UPDATE_FP64, 20)
-    t_ap = ctx.time_kernel(L.HX_KERNEL_APPLY_FP64, 20)
+    out_variants = None
+    if rank == 0 and ws == 1 and not args.no_variants:
+        out_variants = variants(hx, ctx, f, fac, f_d, fac_d, lib_stream)
+    # ---- live per-kernel timing for the roofline (buffers of the solves above) ----
     peaks = load_peaks()
-    nn = n // 3
-    # algorithmic bytes per launch (8-byte words; mask 1 byte per node):
-    # PCG step reads p_old, r, M^-1, x, factor, mask; writes p, q, x
-    b_st = 7 * 8 * n + 8 * ne + nn
-    b_up = 4 * 8 * n          # r, q, M^-1 read; r written
-    b_ap = 2 * 8 * n + 8 * ne + nn   # plain K.x: x read, y written, factor, mask
-    kern = {
-        "pcg_step_fp64": {"ms": t_st, "bytes": b_st, "gbs": b_st / t_st / 1e6},
-        "pcg_update_fp64": {"ms": t_up, "bytes": b_up, "gbs": b_up / t_up / 1e6},
-        "apply_fp64": {"ms": t_ap, "bytes": b_ap, "gbs": b_ap / t_ap / 1e6},
-    }
-    dom = max(("pcg_step_fp64", "pcg_update_fp64"), key=lambda k: kern[k]["ms"])
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
-    if os.path.exists(tp):
-        with open(tp) as fh:
-            traffic = json.load(fh).get(dom)
-    it_ms = t_dev / args.steps / max(iters, 1) * 1e3
-    b_it = b_st + b_up
+    kern = fp64_kernels(ctx, L, n, ne, peaks) if (out_variants or not pc) else None
+    if pc:
+        roof = conv_roofline(ctx, L, args.dims, peaks)
+    else:
+        dom = max(("pcg_step_fp64", "pcg_update_fp64"), key=lambda k: kern[k]["ms"])
+        roof = {"bound": "hbm", "kernel": dom, "achieved": kern[dom]["gbs"],
+                "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": kern[dom]["gbs"] / peaks["hbm_gbs"], "traffic": traffic_of(dom),
+                "peak_source": peaks["source"]}
     out = {
         "metric": METRIC, "value": t_dev / (args.steps * ws), "unit": "s/solve",
         "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t_dev / args.steps * 1e3, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if args.precision == 0 else "f32-in-f64-refinement",
+        "vs_baseline": None, "dtype": DTYPES[args.solver],
         "data": "synthetic: splitmix64(seed 20251209) density, Helmholtz r=3 smoothed, "
                 "mapped to [1e-3,1], SIMP p=3 (contrast 1e9)",
         "config": {"workload": "C1 cantilever 320x160x160 Hex8 (8,192,000 elements, "
-                               "24,961,923 DOFs), Jacobi-PCG to rtol 1e-6 from u0=0, shift 0",
-                   "elements": ne, "dofs": n, "cg_iterations": iters,
-                   "true_rel_res": true_rel, "precision": ["fp64", "mixed32"][args.precision],
-                   "l2": "working set 1.4 GB >> 126 MB L2 (no flush needed)",
+                               "24,961,923 DOFs), solve to rtol 1e-6 (FP64 true residual) "
+                               "from u0=0, shift 0",
+                   "solver": args.solver, "elements": ne, "dofs": n, "iterations": iters,
+                   "true_rel_res": true_rel, "fallbacks": fallbacks,
+                   "l2": "working set >= 0.9 GB >> 126 MB L2 (no flush needed)",
                    "parallelism": f"replicas x{ws}"},
         "e2e": {"value": t_e2e / (e_steps * ws), "unit": "s/solve",
                 "h2d_bytes_per_step": 8 * n + 8 * ne, "d2h_bytes_per_step": 8 * n,
                 "steps": e_steps},
         "gpu_launches": launches,
         "clocks": clk,
-        "roofline": {"bound": "hbm", "kernel": dom,
-                     "achieved": kern[dom]["gbs"], "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                     "frac": kern[dom]["gbs"] / peaks["hbm_gbs"], "traffic": traffic,
-                     "peak_source": peaks["source"]},
-        "kernels": {k: v for k, v in kern.items() if k != "apply_fp64"},
-        "apply_fp64": kern["apply_fp64"],
-        "pcg_iteration": {"ms": it_ms, "bytes": b_it, "gbs": b_it / it_ms / 1e6,
-                          "frac": b_it / it_ms / 1e6 / peaks["hbm_gbs"]},
+        "roofline": roof,
         "filter_setup": {"iterations": frep.iterations, "rel_res": frep.rel_res},
     }
+    if kern:
+        b_it = kern["pcg_step_fp64"]["bytes"] + kern["pcg_update_fp64"]["bytes"]
+        it_ms = kern["pcg_step_fp64"]["ms"] + kern["pcg_update_fp64"]["ms"]
+        out["fp64_kernels"] = kern
+        out["fp64_pcg_iteration"] = {"ms": it_ms, "bytes": b_it, "gbs": b_it / it_ms / 1e6,
+                                     "frac": b_it / it_ms / 1e6 / peaks["hbm_gbs"]}
+    if out_variants:
+        out["variants"] = out_variants
     if tuple(args.dims) != DIMS:
         out["config"]["workload"] = f"profiling case {tuple(args.dims)} (not the C1 workload)"
-    if rank == 0 and ws == 1 and not args.no_variants:
-        out["variants"] = variants(hx, ctx, f, fac, f_d, fac_d, u_d, lib_stream)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline and tuple(args.dims) == DIMS:
-        out["cpu_baseline"] = cpu_baseline(hx, iters, args.cpu_iters)
+        fp64_its = (out_variants or {}).get("fp64_jacobi", {}).get("iterations", iters)
+        out["cpu_baseline"] = cpu_baseline(hx, fp64_its, args.cpu_iters)
     if rank == 0:
         print(json.dumps(out), flush=True)
     ctx.close()
@@ -249,28 +252,62 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def variants(hx, ctx, f, fac, f_d, fac_d, u64_d, lib_stream):
+def traffic_of(kernel):
+    tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as fh:
+            return json.load(fh).get(kernel)
+    return None
+
+
+def fp64_kernels(ctx, L, n, ne, peaks):
+    """Live CUDA-event timing of the FP64 PCG kernels on the last FP64 solve's
+    buffers, with their algorithmic bytes (8-byte words; mask 1 byte/node)."""
+    nn = n // 3
+    t_st = ctx.time_kernel(L.HX_KERNEL_PCG_STEP_FP64, 20)
+    t_up = ctx.time_kernel(L.HX_KERNEL_PCG_UPDATE_FP64, 20)
+    t_ap = ctx.time_kernel(L.HX_KERNEL_APPLY_FP64, 20)
+    b_st = 7 * 8 * n + 8 * ne + nn   # read p_old, r, M^-1, x, factor, mask; write p, q, x
+    b_up = 4 * 8 * n                 # read r, q, M^-1; write r
+    b_ap = 2 * 8 * n + 8 * ne + nn   # plain K.x
+    return {"pcg_step_fp64": {"ms": t_st, "bytes": b_st, "gbs": b_st / t_st / 1e6},
+            "pcg_update_fp64": {"ms": t_up, "bytes": b_up, "gbs": b_up / t_up / 1e6},
+            "apply_fp64": {"ms": t_ap, "bytes": b_ap, "gbs": b_ap / t_ap / 1e6}}
+
+
+def conv_roofline(ctx, L, dims, peaks):
+    """The learned forms' dominant kernel: one 16 -> 16 tcgen05 conv3d layer on
+    the node-grid level 1 (CUDA events, 20 launches).  Algorithmic flops per
+    launch: 2 * 16 * 16 * 27 per node (the MMA computes all 16 output
+    channels)."""
+    nx, ny, nz = dims
+    n1 = ((nx + 1 - 1) // 2 + 1) * ((ny + 1 - 1) // 2 + 1) * ((nz + 1 - 1) // 2 + 1)
+    ms = ctx.time_kernel(L.HX_KERNEL_CONV3, 20)
+    flop = 2.0 * 16 * 16 * 27 * n1
+    tf = flop / ms / 1e9
+    apply_ms = ctx.time_kernel(L.HX_KERNEL_NET_APPLY, 10)
+    return {"bound": "tensor", "kernel": "conv3_tc (level-1 layer)", "achieved": tf,
+            "peak": peaks["bf16_tflops"], "unit": "TFLOP/s", "frac": tf / peaks["bf16_tflops"],
+            "traffic": traffic_of("conv3_tc"), "peak_source": peaks["source"],
+            "launch_ms": ms, "flop_per_launch": flop, "level1_nodes": n1,
+            "preconditioner_application_ms": apply_ms}
+
+
+def variants(hx, ctx, f, fac, f_d, fac_d, lib_stream):
     """The solver forms on the same workload, each timed once on the device
     after one untimed run: FP64 and mixed (FP32 in FP64 reliable updates)
     Jacobi-PCG, and flexible CG with the shipped learned preconditioner in
     FP64 and mixed.  Errors of u, compliance f.u and max von Mises stress
-    against the FP64 Jacobi-PCG solution u64 (the timed solve's result)."""
+    against the FP64 Jacobi-PCG solution."""
     import importlib
     import torch
     learned = importlib.import_module(hx.__name__ + ".learned")
     learned.load_into(ctx)
-    u64 = u64_d.cpu().numpy()
-    c64 = float(f @ u64)
-    vm64 = ctx.stress(u64, fac, 1.0, 0.3)[1]
-    vmax64 = float(np.max(vm64))
-    forms = {"fp64_jacobi": dict(precision=0, preconditioner=0),
-             "mixed32_jacobi": dict(precision=1, preconditioner=0),
-             "fp64_learned_fcg": dict(precision=0, preconditioner=1),
-             "mixed32_learned_fcg": dict(precision=1, preconditioner=1)}
     out = {}
-    u = torch.zeros_like(u64_d)
-    for name, kw in forms.items():
-        opts = hx.default_opts(tol=1e-6, max_iter=100000, **kw)
+    u = torch.zeros_like(f_d)
+    ref = None
+    for name, (prec, pc) in FORMS.items():
+        opts = hx.default_opts(tol=1e-6, max_iter=100000, precision=prec, preconditioner=pc)
         ctx.solve_device(f_d.data_ptr(), fac_d.data_ptr(), u.data_ptr(), opts=opts)
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
@@ -281,6 +318,9 @@ def variants(hx, ctx, f, fac, f_d, fac_d, u64_d, lib_stream):
         e1.synchronize()
         uh = u.cpu().numpy()
         vm = ctx.stress(uh, fac, 1.0, 0.3)[1]
+        if ref is None:  # FP64 Jacobi-PCG comes first
+            ref = (uh.copy(), float(f @ uh), vm.copy(), float(np.max(vm)))
+        u64, c64, vm64, vmax64 = ref
         out[name] = {
             "s_per_solve": e0.elapsed_time(e1) / 1e3, "iterations": rep.iterations,
             "true_rel_res": rep.true_rel_res, "fallback": rep.fallback_used,
@@ -292,7 +332,7 @@ def variants(hx, ctx, f, fac, f_d, fac_d, u64_d, lib_stream):
     base = out["fp64_jacobi"]["s_per_solve"]
     for v in out.values():
         v["speedup_vs_fp64_jacobi"] = base / v["s_per_solve"]
-    out["_note"] = ("learned forms use the shipped networks trained on 128x64x64 problems; "
+    out["_note"] = ("learned forms use the shipped networks (weights/spd_cnn_mix.npy); "
                     "errors against the FP64 Jacobi-PCG solution at rtol 1e-6")
     return out
 
@@ -440,7 +480,8 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--precision", type=int, default=0, help="0 fp64, 1 mixed32")
+    ap.add_argument("--solver", choices=sorted(FORMS), default="mixed32_learned_fcg",
+                    help="the solver form timed for value/e2e (all forms appear in variants)")
     ap.add_argument("--cpu-iters", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-variants", action="store_true",
