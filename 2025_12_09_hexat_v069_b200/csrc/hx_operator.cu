@@ -239,9 +239,35 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
     for (int q = 0; q < 4; ++q) Ytp[c][q] = T(0);
   double dsum = 0.0;
 
+  // The element factor and the node mask are plain loads.  In FP32 both are
+  // fetched one plane ahead so that their latency overlaps a plane of work;
+  // in FP64 the extra live registers would spill (128-register bound), so
+  // they are loaded where they are used.
+  constexpr bool PREFETCH = sizeof(T) == 4;
+  auto load_fac = [&](int ke) -> T {
+    return (col_ok && ke >= 0 && ke < g.nze) ? A.fac[(int64_t)ke * eplane + (int64_t)jn * g.nxe + in]
+                                             : T(0);
+  };
+  auto load_mask = [&](int kn) -> unsigned {
+    if (!A.nmask || !out_ok || kn < k0 || kn >= k1) return 7u;
+    return A.nmask[(int64_t)kn * nplane + (int64_t)jn * g.nxn + in];
+  };
+  T f_next = PREFETCH ? load_fac(k0 - 1) : T(0);
+  unsigned m_next = PREFETCH ? load_mask(k0) : 7u;
+
   for (int ke = k0 - 1; ke < k1; ++ke) {
-    T f = T(0);
-    if (col_ok && ke >= 0 && ke < g.nze) f = A.fac[(int64_t)ke * eplane + (int64_t)jn * g.nxe + in];
+    T f;
+    unsigned m_pre = 7u;
+    if (PREFETCH) {
+      f = f_next;
+      f_next = load_fac(ke + 1);
+      if (ke >= k0) {
+        m_pre = m_next;
+        m_next = load_mask(ke + 1);
+      }
+    } else {
+      f = load_fac(ke);
+    }
     cp_async_wait_all();
     __syncthreads();  // A: planes ke, ke+1 ready; ke+2 landed; red consumed
     if (ke + 2 <= k1) transform(ke + 2);
@@ -286,7 +312,7 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
     __syncthreads();  // B: red of this layer visible
     if (ke >= k0 && out_ok) {
       const int64_t node = (int64_t)ke * nplane + (int64_t)jn * g.nxn + in;
-      const unsigned m = A.nmask ? A.nmask[node] : 7u;
+      const unsigned m = PREFETCH ? m_pre : (A.nmask ? A.nmask[node] : 7u);
       const T* own = &sm.p[ring4(ke)][ly * RW + lx];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
