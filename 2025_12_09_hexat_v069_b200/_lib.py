@@ -279,6 +279,7 @@ class Context:
 
     # ---- learned preconditioner ----
     NET_PARAMS = 3 * 4 * 27 * 256
+    NET_FIRST_LEVEL = 2  # HX_NET_FIRST_LEVEL
 
     def net_init(self, seed=1):
         self.check(self.lib.hx_net_init(self.h, int(seed)), "hx_net_init")

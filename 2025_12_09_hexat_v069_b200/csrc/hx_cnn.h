@@ -13,7 +13,9 @@ struct GridN {  // node grid of the network (nodes per axis)
 constexpr int NET_LAYERS = 4;
 constexpr int NET_LAYER_PARAMS = 27 * 256;  // weights [27 taps][16 co][16 ci], no bias
 constexpr int NET_NET_PARAMS = NET_LAYERS * NET_LAYER_PARAMS;  // one network
-constexpr int NET_NETS = 3;        // networks on node-grid levels 1 .. NET_NETS
+constexpr int NET_NETS = 3;        // networks on node-grid levels NET_L0 .. NET_TOP
+constexpr int NET_L0 = 2;          // level of the first (finest) network
+constexpr int NET_TOP = NET_L0 + NET_NETS - 1;
 constexpr int NET_PARAMS = NET_NETS * NET_NET_PARAMS;
 constexpr int NET_IN = 6;  // live input channels: D^-1/2 r / s and the same times the density
 

@@ -210,7 +210,7 @@ struct hx_ctx {
       hx::DevBuf<float> x, acc, gx, feat;  // [node][3] fields, [node] feature
       hx::DevBuf<__nv_bfloat16> x0, y, act[7];  // network input, output, training activations
       hx::DevBuf<__nv_bfloat16> pp[2];          // application ping-pong (levels >= 2)
-    } lv[4];
+    } lv[8];
     // side streams and events: the coarser levels' networks run beside level 1
     cudaStream_t side[2] = {nullptr, nullptr};
     cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};

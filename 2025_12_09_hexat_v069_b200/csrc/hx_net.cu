@@ -1,9 +1,9 @@
 // hx_net.cu -- the learned preconditioner on the host side: parameters,
 // training (forward, backward, Adam, all on the GPU), PCG snapshots for
-// training data, and the flexible-CG solve that applies it.
+// training data, and the flexible-CG solves that apply it.
 //
 // Preconditioner (symmetric positive definite for every choice of weights):
-//     z = D^-1/2 (I + sum_{l=1..3} R_l^T E_l^T G_l^T G_l E_l R_l) D^-1/2 r.
+//     z = D^-1/2 (I + sum_{l=NET_L0..NET_TOP} R_l^T E_l^T G_l^T G_l E_l R_l) D^-1/2 r.
 // D^-1/2 r is taken as a nodal field (3 components per node of the mesh's
 // node grid, level 0).  R_l restricts it to node-grid level l (each level
 // halves the grid: coarse node i <-> fine node 2i, full weighting 1/2, 1,
@@ -11,15 +11,16 @@
 // a field to 6 channels (x, feat_l * x), feat_l being the density feature
 // restricted to level l, and G_l is a network of 4 conv3d layers (3x3x3, no
 // bias, no activation, 6 -> 16 -> 16 -> 16 -> 16 channels) with G_l^T its
-// transposed convolutions.  Each term is positive semi-definite, zero
-// weights give Jacobi, and the networks act only on coarse levels: a
-// level-1 network costs 1/8 of one on the mesh's grid and sees twice as far,
-// which is where Jacobi-PCG is slow (smooth error).  Only the BF16 roundings
-// make the operator slightly nonlinear, which flexible CG (Notay's FCG, one
-// stored direction) absorbs.  The input is scaled by the RMS s of D^-1/2 r
-// to keep BF16 in range (z does not depend on s otherwise).  A nonlinear
-// network (ReLU, biases) on the mesh's grid was tried first: it breaks
-// symmetry and linearity, and FCG(1) with it stagnated.
+// transposed convolutions.  Each term is positive semi-definite, and zero
+// weights give Jacobi.  The networks act only on coarse levels (2, 3, 4): a
+// level-l network costs 8^-l of one on the mesh's grid and sees 2^l times as
+// far, which is where Jacobi-PCG is slow (smooth error); level 1 carries
+// only the restricted field.  Only the BF16 roundings make the operator
+// slightly nonlinear, which flexible CG (Notay's FCG, one stored direction)
+// absorbs.  The input is scaled by the RMS s of D^-1/2 r to keep BF16 in
+// range (z does not depend on s otherwise).  A nonlinear network (ReLU,
+// biases) on the mesh's grid was tried first: it breaks symmetry and
+// linearity, and FCG(1) with it stagnated.
 //
 // Training minimises, over residual/error pairs (r = b - A x_k, e = u* - x_k)
 // taken from Jacobi-PCG iterates, the energy-norm error of one
@@ -43,6 +44,7 @@ namespace {
 constexpr int LP = NET_LAYER_PARAMS;
 constexpr int NP = NET_NET_PARAMS;
 static_assert(NET_NETS >= 1 && NET_NETS <= 3, "one side stream per level beyond the first");
+static_assert(NET_L0 >= 1 && NET_TOP < 8, "level range of the networks");
 
 GridN level_grid(const Grid& g, int l) {
   GridN a{g.nxn, g.nyn, g.nzn};
@@ -108,32 +110,33 @@ void net_upload(hx_ctx* c, const std::vector<float>& w) {
   N.ready = true;
 }
 
-// Buffers of every level for the current mesh.  Application needs the
-// fields, the network input/output per level and two ping-pong activation
-// buffers (sized for level 1, the largest network grid); training keeps
-// every activation of every level.
+// Buffers of every level for the current mesh: fields on levels 1 ..
+// NET_TOP, network input/output on the network levels, two ping-pong
+// activation buffers for the finest network (level NET_L0, the largest) and
+// two per coarser network (their side streams); training keeps every
+// activation of every network.
 void net_buffers(hx_ctx* c, bool train) {
   auto& N = c->net;
-  const GridN g1 = level_grid(c->g, 1);
+  const GridN g1 = level_grid(c->g, NET_L0);
   const size_t a1 = (size_t)nodes_of(g1) * 16;
   N.tmp[0].ensure(a1);
   N.tmp[1].ensure(a1);
   N.lv[0].feat.ensure((size_t)nodes_of(level_grid(c->g, 0)));  // only the feature on level 0
-  for (int l = 1; l <= NET_NETS; ++l) {
+  for (int l = 1; l <= NET_TOP; ++l) {
     const size_t nl = (size_t)nodes_of(level_grid(c->g, l));
     auto& L = N.lv[l];
     L.x.ensure(nl * 3);
     L.acc.ensure(nl * 3);
     L.feat.ensure(nl);
+    if (train) L.gx.ensure(nl * 3);
+    if (l < NET_L0) continue;
     L.x0.ensure(nl * 16);
     L.y.ensure(nl * 8);
-    if (train) {
-      L.gx.ensure(nl * 3);
+    if (train)
       for (auto& a : L.act) a.ensure(nl * 16);
-    }
+    if (l > NET_L0)
+      for (auto& b : L.pp) b.ensure(nl * 16);
   }
-  for (int l = 2; l <= NET_NETS; ++l)
-    for (auto& b : N.lv[l].pp) b.ensure((size_t)nodes_of(level_grid(c->g, l)) * 16);
   if (!N.ev_fork) {
     HX_CUDA(cudaEventCreateWithFlags(&N.ev_fork, cudaEventDisableTiming));
     for (int i = 0; i < 2; ++i) {
@@ -210,47 +213,54 @@ void stack_backward_train(hx_ctx* c, int k, const GridN& g, const __nv_bfloat16*
 // z = M^-1 r + s D^-1/2 sum_l R_l^T E_l^T G_l^T G_l E_l R_l (D^-1/2 r / s).
 // The mesh-grid passes are fused: the level-1 field is restricted straight
 // from r (k_restrict_dof) and the level-1 correction is prolongated inside
-// the output kernel, so no field is stored on the mesh's node grid.  The
-// levels run coarsest first: acc_l = E_l^T y_l + R^T acc_{l+1}.  `train`
+// the output kernel, so no field is stored on the mesh's node grid.  `train`
 // keeps the activations; q_old: FCG beta reduction (see k_net_output).
 // T: precision of r, minv, z, q_old (the solver's vectors).
 template <typename T>
 void precond_z(hx_ctx* c, const T* r, const T* minv, CgState* st, double scale_mul, T* z,
                const T* q_old, bool train) {
   auto& N = c->net;
-  GridN gl[NET_NETS + 1];
-  for (int l = 0; l <= NET_NETS; ++l) gl[l] = level_grid(c->g, l);
+  GridN gl[NET_TOP + 1];
+  for (int l = 0; l <= NET_TOP; ++l) gl[l] = level_grid(c->g, l);
   launch_restrict_dof<T>(c->stream, r, minv, st, nullptr, 0, scale_mul, N.lv[1].x.p, gl[0], gl[1]);
-  for (int l = 2; l <= NET_NETS; ++l)
+  for (int l = 2; l <= NET_TOP; ++l)
     launch_restrict(c->stream, 3, N.lv[l - 1].x.p, N.lv[l].x.p, gl[l - 1], gl[l], false);
   if (train) {
-    for (int l = NET_NETS; l >= 1; --l) {
+    for (int l = NET_TOP; l >= NET_L0; --l) {
       auto& L = N.lv[l];
       launch_lift(c->stream, L.x.p, L.feat.p, L.x0.p, nodes_of(gl[l]));
-      stack_forward_train(c, l - 1, gl[l], L.x0.p, L.act, L.y.p);
+      stack_forward_train(c, l - NET_L0, gl[l], L.x0.p, L.act, L.y.p);
     }
   } else {
-    // the networks of levels 2.. on side streams, level 1 on the main one
+    // the coarser networks on side streams, the finest on the main one
     // (fork/join by events; inside a stream capture these become parallel
     // branches of the graph)
     HX_CUDA(cudaEventRecord(N.ev_fork, c->stream));
-    for (int l = 2; l <= NET_NETS; ++l) {
-      cudaStream_t ss = N.side[l - 2];
+    for (int l = NET_L0 + 1; l <= NET_TOP; ++l) {
+      const int side = l - NET_L0 - 1;
+      cudaStream_t ss = N.side[side];
       auto& L = N.lv[l];
       HX_CUDA(cudaStreamWaitEvent(ss, N.ev_fork, 0));
       launch_lift(ss, L.x.p, L.feat.p, L.x0.p, nodes_of(gl[l]));
-      stack_apply(c, ss, l - 1, gl[l], L.x0.p, L.y.p, L.pp[0].p, L.pp[1].p);
-      HX_CUDA(cudaEventRecord(N.ev_join[l - 2], ss));
+      stack_apply(c, ss, l - NET_L0, gl[l], L.x0.p, L.y.p, L.pp[0].p, L.pp[1].p);
+      HX_CUDA(cudaEventRecord(N.ev_join[side], ss));
     }
-    auto& L1 = N.lv[1];
-    launch_lift(c->stream, L1.x.p, L1.feat.p, L1.x0.p, nodes_of(gl[1]));
-    stack_apply(c, c->stream, 0, gl[1], L1.x0.p, L1.y.p, N.tmp[0].p, N.tmp[1].p);
-    for (int l = 2; l <= NET_NETS; ++l) HX_CUDA(cudaStreamWaitEvent(c->stream, N.ev_join[l - 2], 0));
+    auto& L1 = N.lv[NET_L0];
+    launch_lift(c->stream, L1.x.p, L1.feat.p, L1.x0.p, nodes_of(gl[NET_L0]));
+    stack_apply(c, c->stream, 0, gl[NET_L0], L1.x0.p, L1.y.p, N.tmp[0].p, N.tmp[1].p);
+    for (int l = NET_L0 + 1; l <= NET_TOP; ++l)
+      HX_CUDA(cudaStreamWaitEvent(c->stream, N.ev_join[l - NET_L0 - 1], 0));
   }
-  for (int l = NET_NETS; l >= 1; --l) {
+  // acc_l = E_l^T y_l (network levels) + R^T acc_{l+1}, coarsest first
+  for (int l = NET_TOP; l >= 1; --l) {
     auto& L = N.lv[l];
-    launch_unlift(c->stream, L.y.p, L.feat.p, L.acc.p, false, nodes_of(gl[l]));
-    if (l < NET_NETS) launch_prolong(c->stream, N.lv[l + 1].acc.p, L.acc.p, gl[l], gl[l + 1], true);
+    if (l >= NET_L0) {
+      launch_unlift(c->stream, L.y.p, L.feat.p, L.acc.p, false, nodes_of(gl[l]));
+      if (l < NET_TOP)
+        launch_prolong(c->stream, N.lv[l + 1].acc.p, L.acc.p, gl[l], gl[l + 1], true);
+    } else {
+      launch_prolong(c->stream, N.lv[l + 1].acc.p, L.acc.p, gl[l], gl[l + 1], false);
+    }
   }
   launch_net_output<T>(c->stream, r, minv, N.lv[1].acc.p, gl[0], gl[1], st, scale_mul, z, q_old,
                        c->d_partials.p);
@@ -264,7 +274,7 @@ void net_operator_inputs(hx_ctx* c, const double* fac) {
   HX_REQUIRE(c->d_minv.n >= (size_t)n, "no Jacobi data: run a solve on this grid first");
   net_buffers(c, false);
   launch_rho_feature(c->stream, fac, N.lv[0].feat.p, c->g);
-  for (int l = 1; l <= NET_NETS; ++l)
+  for (int l = 1; l <= NET_TOP; ++l)
     launch_restrict(c->stream, 1, N.lv[l - 1].feat.p, N.lv[l].feat.p, level_grid(c->g, l - 1),
                     level_grid(c->g, l), true);
   // private copy: training steps apply the operator long after the caller's call
@@ -411,13 +421,13 @@ double net_loss_grad(hx_ctx* c, const double* r, const double* e, int loss_kind,
   // output gradient is its lifting E_l
   launch_restrict_dof<double>(c->stream, gvec, c->d_minv.p, s3, s2, mode, scale_mul, N.lv[1].gx.p,
                       level_grid(g, 0), level_grid(g, 1));
-  for (int l = 2; l <= NET_NETS; ++l)
+  for (int l = 2; l <= NET_TOP; ++l)
     launch_restrict(c->stream, 3, N.lv[l - 1].gx.p, N.lv[l].gx.p, level_grid(g, l - 1),
                     level_grid(g, l), false);
-  for (int l = 1; l <= NET_NETS; ++l) {
+  for (int l = NET_L0; l <= NET_TOP; ++l) {
     const GridN gl = level_grid(g, l);
     launch_lift(c->stream, N.lv[l].gx.p, N.lv[l].feat.p, N.da.p, nodes_of(gl));
-    stack_backward_train(c, l - 1, gl, N.lv[l].x0.p, N.lv[l].act, !first);
+    stack_backward_train(c, l - NET_L0, gl, N.lv[l].x0.p, N.lv[l].act, !first);
   }
   double loss = 0;
   if (host_ratio) {
@@ -481,8 +491,8 @@ std::function<void()> net_time_body(hx_ctx* c, int which) {
   const int64_t n = g.dofs();
   HX_REQUIRE(c->d_b.n >= (size_t)n, "run a solve before timing the network");
   net_buffers(c, false);
-  if (which == 0) {  // one 16 -> 16 layer on the level-1 grid
-    const GridN g1 = level_grid(g, 1);
+  if (which == 0) {  // one 16 -> 16 layer on the finest network's grid
+    const GridN g1 = level_grid(g, NET_L0);
     HX_CUDA(cudaMemsetAsync(N.tmp[0].p, 0, (size_t)nodes_of(g1) * 16 * sizeof(__nv_bfloat16),
                             c->stream));
     return [c, g1] {

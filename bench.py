@@ -277,19 +277,21 @@ def fp64_kernels(ctx, L, n, ne, peaks):
 
 def conv_roofline(ctx, L, dims, peaks):
     """The learned forms' dominant kernel: one 16 -> 16 tcgen05 conv3d layer on
-    the node-grid level 1 (CUDA events, 20 launches).  Algorithmic flops per
+    the finest network's node-grid level (CUDA events, 20 launches).  Algorithmic flops per
     launch: 2 * 16 * 16 * 27 per node (the MMA computes all 16 output
     channels)."""
-    nx, ny, nz = dims
-    n1 = ((nx + 1 - 1) // 2 + 1) * ((ny + 1 - 1) // 2 + 1) * ((nz + 1 - 1) // 2 + 1)
+    g = [d + 1 for d in dims]  # node grid, then halved per level
+    for _ in range(L.Context.NET_FIRST_LEVEL):
+        g = [(a - 1) // 2 + 1 for a in g]
+    n1 = g[0] * g[1] * g[2]
     ms = ctx.time_kernel(L.HX_KERNEL_CONV3, 20)
     flop = 2.0 * 16 * 16 * 27 * n1
     tf = flop / ms / 1e9
     apply_ms = ctx.time_kernel(L.HX_KERNEL_NET_APPLY, 10)
-    return {"bound": "tensor", "kernel": "conv3_tc (level-1 layer)", "achieved": tf,
+    return {"bound": "tensor", "kernel": "conv3_tc (finest network layer)", "achieved": tf,
             "peak": peaks["bf16_tflops"], "unit": "TFLOP/s", "frac": tf / peaks["bf16_tflops"],
             "traffic": traffic_of("conv3_tc"), "peak_source": peaks["source"],
-            "launch_ms": ms, "flop_per_launch": flop, "level1_nodes": n1,
+            "launch_ms": ms, "flop_per_launch": flop, "level_nodes": n1,
             "preconditioner_application_ms": apply_ms}
 
 

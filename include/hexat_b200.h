@@ -300,19 +300,20 @@ HX_API hx_status hx_oc_update_device(hx_ctx *ctx, const double *x_dev,
 
 /* ---- learned preconditioner -----------------------------------------------------
  * No reference counterpart.  z = D^-1/2 (I + sum_l R_l^T E_l^T G_l^T G_l E_l R_l) D^-1/2 r
- * for l = 1, 2, 3: R_l restricts a nodal field to node-grid level l (each
- * level halves the grid, full weighting) and R_l^T is its exact transpose;
- * E_l lifts a field to 6 channels (x, density * x); G_l is a 3D CNN of 4
- * conv3d layers (3x3x3, no bias, 6 -> 16 -> 16 -> 16 -> 16 channels, BF16
- * weights and activations, FP32 accumulation on the tensor cores) and G_l^T
- * its transposed convolutions.  Symmetric positive definite for every choice
- * of weights; zero weights give Jacobi.  hx_solve with preconditioner
- * HX_PC_LEARNED applies it in flexible CG (Notay, one stored direction) and
- * falls back to Jacobi-PCG from the current iterate on breakdown or
- * stagnation (report->fallback_used).
- * Parameters: HX_NET_PARAMS floats, the 3 networks one after the other, each
- * 4 layers of [27 taps][16 out][16 in] weights; input channels >= 6 of each
- * first layer are forced to zero. */
+ * for l = HX_NET_FIRST_LEVEL .. HX_NET_FIRST_LEVEL + 2: R_l restricts a nodal
+ * field to node-grid level l (each level halves the grid, full weighting)
+ * and R_l^T is its exact transpose; E_l lifts a field to 6 channels
+ * (x, density * x); G_l is a 3D CNN of 4 conv3d layers (3x3x3, no bias,
+ * 6 -> 16 -> 16 -> 16 -> 16 channels, BF16 weights and activations, FP32
+ * accumulation on the tensor cores) and G_l^T its transposed convolutions.
+ * Symmetric positive definite for every choice of weights; zero weights give
+ * Jacobi.  hx_solve with preconditioner HX_PC_LEARNED applies it in flexible
+ * CG (Notay, one stored direction) and falls back to Jacobi-PCG from the
+ * current iterate on breakdown or stagnation (report->fallback_used).
+ * Parameters: HX_NET_PARAMS floats, the 3 networks one after the other
+ * (finest level first), each 4 layers of [27 taps][16 out][16 in] weights;
+ * input channels >= 6 of each first layer are forced to zero. */
+#define HX_NET_FIRST_LEVEL 2
 #define HX_NET_PARAMS (3 * 4 * 27 * 256)
 HX_API hx_status hx_net_init(hx_ctx *ctx, uint64_t seed);
 HX_API hx_status hx_net_set_params(hx_ctx *ctx, const float *params);

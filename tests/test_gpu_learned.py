@@ -1,5 +1,5 @@
 """The learned preconditioner
-P = D^-1/2 (I + sum_l R_l^T E_l^T G_l^T G_l E_l R_l) D^-1/2  (levels 1-3):
+P = D^-1/2 (I + sum_l R_l^T E_l^T G_l^T G_l E_l R_l) D^-1/2  (levels L0..L0+2):
 the BF16 tensor-core convolutions of G and G^T and the weight gradient, and
 the whole application of P, checked against a CPU reference built on torch
 (FP32 arithmetic with the kernels' BF16 roundings of weights, activations
@@ -13,7 +13,8 @@ pytestmark = pytest.mark.gpu
 
 LP = 27 * 256
 NP = 4 * LP       # one network
-NETS = 3          # networks on node-grid levels 1..3
+NETS = 3          # networks on node-grid levels L0 .. L0 + 2
+L0 = 2            # HX_NET_FIRST_LEVEL
 NET_IN = 6
 
 
@@ -157,17 +158,21 @@ def _torch_precond(params, dims, fac, minv, r):
     cnt = sum(cp[a:a + nz1, b:b + ny1, c:c + nx1] for a in (0, 1) for b in (0, 1) for c in (0, 1))
     feat = [torch.from_numpy((ssum / cnt).astype(np.float32))[None, None]]
     xs = [x]
-    for l in range(1, NETS + 1):
+    top = L0 + NETS - 1
+    for l in range(1, top + 1):
         feat.append(_restrict(feat[-1], True))
         xs.append(_restrict(xs[-1]))
     acc = None
-    for l in range(NETS, 0, -1):
-        X0 = torch.zeros((1, 16) + xs[l].shape[2:])
-        X0[:, :3] = _bf(xs[l])
-        X0[:, 3:6] = _bf(xs[l] * feat[l])
-        _, b = _gtg(_weights(params, l - 1), X0)
-        t = b[0][:, :3] + feat[l] * b[0][:, 3:6]
-        acc = t if acc is None else t + _prolong(acc, xs[l].shape[2:])
+    for l in range(top, 0, -1):
+        if l >= L0:
+            X0 = torch.zeros((1, 16) + xs[l].shape[2:])
+            X0[:, :3] = _bf(xs[l])
+            X0[:, 3:6] = _bf(xs[l] * feat[l])
+            _, b = _gtg(_weights(params, l - L0), X0)
+            t = b[0][:, :3] + feat[l] * b[0][:, 3:6]
+            acc = t if acc is None else t + _prolong(acc, xs[l].shape[2:])
+        else:
+            acc = _prolong(acc, xs[l].shape[2:])
     acc = _prolong(acc, xs[0].shape[2:])
     corr = acc[0].permute(1, 2, 3, 0).reshape(-1).double().numpy()
     return minv * r + s * dinvs * corr, minv * r
@@ -175,7 +180,7 @@ def _torch_precond(params, dims, fac, minv, r):
 
 def test_full_preconditioner_matches_torch(ctx, hx):
     import torch
-    dims = (22, 9, 7)  # odd and even node counts on the levels
+    dims = (30, 13, 11)  # odd and even node counts on the levels
     f_d, fac_d = _problem(ctx, hx, dims, seed=6)
     ctx.solve_device(f_d.data_ptr(), fac_d.data_ptr(), torch.zeros_like(f_d).data_ptr(),
                      opts=hx.default_opts(tol=1e-2))
@@ -238,8 +243,12 @@ def test_preconditioner_is_symmetric_positive_definite(ctx, hx):
 
 
 def test_training_reduces_loss_and_iterations(ctx, hx):
+    """Training from a fresh initialisation on one problem's Jacobi-PCG
+    snapshots (mini-batches of 4): the loss falls and flexible CG with the
+    trained networks converges on the true residual in at least 1.5x fewer
+    iterations than Jacobi-PCG."""
     import torch
-    dims = (40, 12, 12)
+    dims = (64, 24, 24)  # coarse network levels of some extent (17x7x7 .. 5x2x2)
     f_d, fac_d = _problem(ctx, hx, dims, seed=3)
     n = f_d.numel()
     # reference solution and Jacobi-PCG snapshots
@@ -250,22 +259,28 @@ def test_training_reduces_loss_and_iterations(ctx, hx):
                                   torch.zeros_like(f_d).data_ptr(),
                                   opts=hx.default_opts(tol=1e-6)).iterations
     snaps = torch.zeros((64, n), dtype=torch.float64, device=f_d.device)
-    taken = ctx.pcg_snapshots(f_d.data_ptr(), fac_d.data_ptr(), 4, 64, 1e-8, snaps.data_ptr())
+    taken = ctx.pcg_snapshots(f_d.data_ptr(), fac_d.data_ptr(), 8, 64, 1e-8, snaps.data_ptr())
     assert taken >= 8
     ctx.net_init(seed=5)
     ctx.net_prepare(fac_d.data_ptr())
-    r = torch.empty_like(f_d)
+    B = 4
+    R = torch.empty((B, n), dtype=torch.float64, device=f_d.device)
+    E = torch.empty_like(R)
     losses = []
     rng = np.random.default_rng(0)
-    for step in range(1500):
-        k = int(rng.integers(taken))
-        ctx.residual_device(f_d.data_ptr(), fac_d.data_ptr(), snaps[k].data_ptr(), r.data_ptr())
-        e = (u_star - snaps[k]).contiguous()
-        losses.append(ctx.net_train_step(r.data_ptr(), e.data_ptr(), 1e-3))
-    first = np.mean(losses[:100])
-    last = np.mean(losses[-100:])
+    for step in range(500):
+        for b, k in enumerate(rng.integers(taken, size=B)):
+            ctx.residual_device(f_d.data_ptr(), fac_d.data_ptr(), snaps[k].data_ptr(),
+                                R[b].data_ptr())
+            torch.sub(u_star, snaps[k], out=E[b])
+        torch.cuda.current_stream().synchronize()
+        losses.append(ctx.net_train_batch([R[b].data_ptr() for b in range(B)],
+                                          [E[b].data_ptr() for b in range(B)],
+                                          3e-4 if step < 250 else 1e-4))
+    first = np.mean(losses[:50])
+    last = np.mean(losses[-50:])
     assert np.isfinite(losses).all() and last < first
-    # flexible CG with the trained network: converges on the true residual
+    # flexible CG with the trained networks: converges on the true residual
     u = torch.zeros_like(f_d)
     rl = ctx.solve_device(f_d.data_ptr(), fac_d.data_ptr(), u.data_ptr(),
                           opts=hx.default_opts(tol=1e-6, preconditioner=1, max_iter=20000,
