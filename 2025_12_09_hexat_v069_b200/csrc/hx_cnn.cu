@@ -262,38 +262,48 @@ __device__ __forceinline__ double field_coef(const CgState* sst, const CgState* 
 // T: the precision of the solver's vectors; the field is FP32 (it feeds the
 // BF16 network), so it is formed in FP32 whatever T is.
 template <typename T>
-__global__ void k_restrict_dof(const T* __restrict__ v, const T* __restrict__ minv,
-                               const CgState* sst, const CgState* lst, int mode, double scale_mul,
-                               float* __restrict__ out, GridN gf, GridN gc) {
-  const double kc = field_coef(sst, lst, mode, scale_mul);
+__global__ void __launch_bounds__(256)
+    k_restrict_dof(const T* __restrict__ v, const T* __restrict__ minv, const CgState* sst,
+                   const CgState* lst, int mode, double scale_mul, float* __restrict__ out,
+                   GridN gf, GridN gc) {
+  // one coarse node per thread; the 27 fine neighbours are read at clamped
+  // indices with weight 0 outside the grid, so every load is unconditional
+  // and they can all be in flight together
   const int64_t nc = (int64_t)gc.nx * gc.ny * gc.nz;
-  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nc;
-       n += (int64_t)gridDim.x * blockDim.x) {
-    const unsigned un = (unsigned)n, t = un / (unsigned)gc.nx;
-    const int i = (int)(un - t * (unsigned)gc.nx);
-    const int j = (int)(t % (unsigned)gc.ny), k = (int)(t / (unsigned)gc.ny);
-    float a0 = 0.f, a1 = 0.f, a2 = 0.f;
-    for (int dz = -1; dz <= 1; ++dz) {
-      const int fz = 2 * k + dz;
-      if (fz < 0 || fz >= gf.nz) continue;
-      for (int dy = -1; dy <= 1; ++dy) {
-        const int fy = 2 * j + dy;
-        if (fy < 0 || fy >= gf.ny) continue;
-        for (int dx = -1; dx <= 1; ++dx) {
-          const int fx = 2 * i + dx;
-          if (fx < 0 || fx >= gf.nx) continue;
-          const float w = fw(dz) * fw(dy) * fw(dx);
-          const int64_t f = 3 * (((int64_t)fz * gf.ny + fy) * gf.nx + fx);
-          a0 += w * sqrtf((float)minv[f + 0]) * (float)v[f + 0];
-          a1 += w * sqrtf((float)minv[f + 1]) * (float)v[f + 1];
-          a2 += w * sqrtf((float)minv[f + 2]) * (float)v[f + 2];
-        }
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= nc) return;
+  const float kc = (float)field_coef(sst, lst, mode, scale_mul);
+  const unsigned un = (unsigned)n, t = un / (unsigned)gc.nx;
+  const int i = (int)(un - t * (unsigned)gc.nx);
+  const int j = (int)(t % (unsigned)gc.ny), k = (int)(t / (unsigned)gc.ny);
+  float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+#pragma unroll
+  for (int dz = -1; dz <= 1; ++dz) {
+    const int fz0 = 2 * k + dz;
+    const bool okz = fz0 >= 0 && fz0 < gf.nz;
+    const int fz = min(max(fz0, 0), gf.nz - 1);
+#pragma unroll
+    for (int dy = -1; dy <= 1; ++dy) {
+      const int fy0 = 2 * j + dy;
+      const bool oky = okz && fy0 >= 0 && fy0 < gf.ny;
+      const int fy = min(max(fy0, 0), gf.ny - 1);
+      const int64_t fr = ((int64_t)fz * gf.ny + fy) * gf.nx;
+#pragma unroll
+      for (int dx = -1; dx <= 1; ++dx) {
+        const int fx0 = 2 * i + dx;
+        const bool ok = oky && fx0 >= 0 && fx0 < gf.nx;
+        const int fx = min(max(fx0, 0), gf.nx - 1);
+        const float w = ok ? fw(dz) * fw(dy) * fw(dx) : 0.f;
+        const int64_t f = 3 * (fr + fx);
+        a0 += w * sqrtf((float)minv[f + 0]) * (float)v[f + 0];
+        a1 += w * sqrtf((float)minv[f + 1]) * (float)v[f + 1];
+        a2 += w * sqrtf((float)minv[f + 2]) * (float)v[f + 2];
       }
     }
-    out[3 * n + 0] = (float)kc * a0;
-    out[3 * n + 1] = (float)kc * a1;
-    out[3 * n + 2] = (float)kc * a2;
   }
+  out[3 * n + 0] = kc * a0;
+  out[3 * n + 1] = kc * a1;
+  out[3 * n + 2] = kc * a2;
 }
 
 // Prolongation, the exact transpose of k_restrict (without normalisation):
@@ -380,17 +390,25 @@ __global__ void k_unlift(const __nv_bfloat16* __restrict__ Y, const float* __res
 // D^-1/2 = sqrt(minv) (masked DOFs have minv = 0).  With q_old: reduces
 // z.q_old and sets the flexible-CG coefficient st->beta = -(z.q_old) /
 // (p_old.q_old) (0 without a previous step).  T: vector precision.
+constexpr int OUT_NPT = 4;  // fine nodes per thread of k_net_output
+
 template <typename T>
-__global__ void k_net_output(const T* __restrict__ r, const T* __restrict__ minv,
-                             const float* __restrict__ t, GridN gf, GridN gc, CgState* st,
-                             double scale_mul, T* __restrict__ z, const T* __restrict__ q_old,
-                             double* partials) {
+__global__ void __launch_bounds__(256)
+    k_net_output(const T* __restrict__ r, const T* __restrict__ minv, const float* __restrict__ t,
+                 GridN gf, GridN gc, CgState* st, double scale_mul, T* __restrict__ z,
+                 const T* __restrict__ q_old, double* partials) {
+  // OUT_NPT fine nodes per thread, each a block-wide coalesced chunk, with
+  // no dependence between them (one block partial of z.q_old per 1024
+  // nodes); the 8 coarse neighbours are read at valid indices with weight
+  // 0 where they do not exist, so every load is unconditional
   if (st->status != HX_RUNNING) return;
   const double s = sqrt(st->rz * scale_mul);
   const int64_t nf = (int64_t)gf.nx * gf.ny * gf.nz;
   double zq = 0.0;
-  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nf;
-       n += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+  for (int u = 0; u < OUT_NPT; ++u) {
+    const int64_t n = ((int64_t)blockIdx.x * OUT_NPT + u) * blockDim.x + threadIdx.x;
+    if (n >= nf) continue;
     const unsigned un = (unsigned)n, tt = un / (unsigned)gf.nx;
     const int fx = (int)(un - tt * (unsigned)gf.nx);
     const int fy = (int)(tt % (unsigned)gf.ny), fz = (int)(tt / (unsigned)gf.ny);
@@ -403,22 +421,24 @@ __global__ void k_net_output(const T* __restrict__ r, const T* __restrict__ minv
 #pragma unroll
     for (int az = 0; az < 2; ++az)
 #pragma unroll
-      for (int ay = 0; ay < 2; ++ay)
+      for (int ay = 0; ay < 2; ++ay) {
+        const int64_t cr = ((int64_t)iz[az] * gc.ny + iy[ay]) * gc.nx;
+        const float wyz = wz[az] * wy[ay];
 #pragma unroll
         for (int ax = 0; ax < 2; ++ax) {
-          const float w = wz[az] * wy[ay] * wx[ax];
-          if (w == 0.f) continue;
-          const int64_t c = 3 * (((int64_t)iz[az] * gc.ny + iy[ay]) * gc.nx + ix[ax]);
-          a[0] += w * t[c + 0];
-          a[1] += w * t[c + 1];
-          a[2] += w * t[c + 2];
+          const float w = wyz * wx[ax];
+          const int64_t c3 = 3 * (cr + ix[ax]);
+          a[0] += w * t[c3 + 0];
+          a[1] += w * t[c3 + 1];
+          a[2] += w * t[c3 + 2];
         }
+      }
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const int64_t i = 3 * n + c;
+      const T m = minv[i];
       // the correction is BF16-accurate: its scale sqrt(minv) in FP32
-      const double m = (double)minv[i];
-      const T zi = (T)(m * (double)r[i] + s * (double)(sqrtf((float)minv[i]) * a[c]));
+      const T zi = m * r[i] + (T)(s * (double)(sqrtf((float)m) * a[c]));
       z[i] = zi;
       if (q_old) zq += (double)zi * (double)q_old[i];
     }
@@ -497,8 +517,8 @@ void launch_restrict_dof(cudaStream_t s, const T* v, const T* minv, const CgStat
                          const CgState* lst, int mode, double scale_mul, float* out,
                          const GridN& gf, const GridN& gc) {
   const int64_t nc = (int64_t)gc.nx * gc.ny * gc.nz;
-  k_restrict_dof<T><<<vec_blocks(nc), 256, 0, s>>>(v, minv, sst, lst, mode, scale_mul, out, gf,
-                                                   gc);
+  k_restrict_dof<T><<<(unsigned)cdiv(nc, 256), 256, 0, s>>>(v, minv, sst, lst, mode, scale_mul,
+                                                            out, gf, gc);
   HX_CHECK_LAUNCH();
 }
 template void launch_restrict_dof<double>(cudaStream_t, const double*, const double*,
@@ -542,10 +562,15 @@ template <typename T>
 void launch_net_output(cudaStream_t s, const T* r, const T* minv, const float* t, const GridN& gf,
                        const GridN& gc, CgState* st, double scale_mul, T* z, const T* q_old,
                        double* partials) {
-  const int64_t nf = (int64_t)gf.nx * gf.ny * gf.nz;
-  k_net_output<T><<<vec_blocks(nf), 256, 0, s>>>(r, minv, t, gf, gc, st, scale_mul, z, q_old,
-                                                 partials);
+  // one block partial per 256 * OUT_NPT nodes: `partials` must hold
+  // net_output_blocks(gf)
+  k_net_output<T><<<(unsigned)net_output_blocks(gf), 256, 0, s>>>(r, minv, t, gf, gc, st,
+                                                                  scale_mul, z, q_old, partials);
   HX_CHECK_LAUNCH();
+}
+
+size_t net_output_blocks(const GridN& gf) {
+  return (size_t)cdiv((int64_t)gf.nx * gf.ny * gf.nz, 256 * OUT_NPT);
 }
 template void launch_net_output<double>(cudaStream_t, const double*, const double*, const float*,
                                         const GridN&, const GridN&, CgState*, double, double*,

@@ -45,6 +45,8 @@ void launch_prolong(cudaStream_t s, const float* coarse, float* fine, const Grid
 void launch_lift(cudaStream_t s, const float* x, const float* feat, __nv_bfloat16* X, int64_t nn);
 void launch_unlift(cudaStream_t s, const __nv_bfloat16* Y, const float* feat, float* acc,
                    bool accumulate, int64_t nn);
+// partials k_net_output needs (one per block)
+size_t net_output_blocks(const GridN& gf);
 // z = M^-1 r + s D^-1/2 R^T t  (t: level-1 correction), with the FCG beta from q_old
 template <typename T>
 void launch_net_output(cudaStream_t s, const T* r, const T* minv, const float* t, const GridN& gf,

@@ -160,15 +160,33 @@ __device__ bool grid_reduce(double (&v)[NV], double* partials, unsigned int* tic
   __syncthreads();
   if (!last) return false;
   __threadfence();
-  double s[NV];
+  // four independent running sums per thread (loads in flight together),
+  // combined in a fixed order: deterministic for a given grid
+  double s4[4][NV];
 #pragma unroll
-  for (int k = 0; k < NV; ++k) s[k] = MAX ? -INFINITY : 0.0;
-  for (unsigned b = tid; b < nblk; b += nthr)
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int k = 0; k < NV; ++k) s4[a][k] = MAX ? -INFINITY : 0.0;
+  unsigned b = tid;
+  for (; b + 3 * nthr < nblk; b += 4 * nthr)
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int k = 0; k < NV; ++k) {
+        const double pv = __ldcg(&partials[(size_t)(b + a * nthr) * NV + k]);
+        s4[a][k] = MAX ? fmax(s4[a][k], pv) : s4[a][k] + pv;
+      }
+  for (; b < nblk; b += nthr)
 #pragma unroll
     for (int k = 0; k < NV; ++k) {
-      double pv = __ldcg(&partials[(size_t)b * NV + k]);
-      s[k] = MAX ? fmax(s[k], pv) : s[k] + pv;
+      const double pv = __ldcg(&partials[(size_t)b * NV + k]);
+      s4[0][k] = MAX ? fmax(s4[0][k], pv) : s4[0][k] + pv;
     }
+  double s[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k)
+    s[k] = MAX ? fmax(fmax(s4[0][k], s4[1][k]), fmax(s4[2][k], s4[3][k]))
+               : (s4[0][k] + s4[1][k]) + (s4[2][k] + s4[3][k]);
   __syncthreads();
   block_reduce<NV, MAX>(s, red);
   if (tid == 0) {

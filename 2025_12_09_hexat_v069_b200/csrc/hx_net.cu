@@ -122,6 +122,9 @@ void net_buffers(hx_ctx* c, bool train) {
   N.tmp[0].ensure(a1);
   N.tmp[1].ensure(a1);
   N.lv[0].feat.ensure((size_t)nodes_of(level_grid(c->g, 0)));  // only the feature on level 0
+  ensure_workspace(c);
+  const size_t need = net_output_blocks(level_grid(c->g, 0));
+  if (c->d_partials.n < need) c->d_partials.ensure(need);
   for (int l = 1; l <= NET_TOP; ++l) {
     const size_t nl = (size_t)nodes_of(level_grid(c->g, l));
     auto& L = N.lv[l];
