@@ -47,6 +47,26 @@ def dist_info():
     return ws, rank, local
 
 
+def barrier(ws):
+    """All ranks meet (no-op for one process)."""
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, ws, device):
+    """The largest of the ranks' values of x: the whole job's time is its
+    slowest replica's.  device: where the process group's tensors live
+    ("cuda" with NCCL, "cpu" with gloo)."""
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 class Clocks:
     """nvidia-smi sampler for the timed region."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -142,22 +162,11 @@ def run_ours(args):
     opts = hx.default_opts(tol=1e-6, max_iter=100000, precision=prec, preconditioner=pc)
     lib_stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
 
-    def barrier():
-        if ws > 1:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if ws == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     for _ in range(args.warmup):
         rep = ctx.solve_device(f_d.data_ptr(), fac_d.data_ptr(), u_d.data_ptr(), opts=opts)
     # ---- timed region: device-resident inputs ----
     clocks = Clocks(local)
-    barrier()
+    barrier(ws)
     torch.cuda.synchronize()
     clocks.start()
     e0 = torch.cuda.Event(enable_timing=True)
@@ -172,8 +181,8 @@ def run_ours(args):
     e1.synchronize()
     torch.cuda.synchronize()
     clk = clocks.stop()
-    barrier()
-    t_dev = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    barrier(ws)
+    t_dev = max_over_ranks(e0.elapsed_time(e1) / 1e3, ws, dev)
     iters = reps[-1].iterations
     true_rel = reps[-1].true_rel_res
     fallbacks = sum(int(r.fallback_used) for r in reps)
@@ -183,7 +192,7 @@ def run_ours(args):
     u_h = torch.zeros(n, dtype=torch.float64).pin_memory()
     f_np, fac_np, u_np = f_h.numpy(), fac_h.numpy(), u_h.numpy()
     e_steps = max(1, min(args.steps, 3))
-    barrier()
+    barrier(ws)
     torch.cuda.synchronize()
     e2 = torch.cuda.Event(enable_timing=True)
     e3 = torch.cuda.Event(enable_timing=True)
@@ -194,8 +203,8 @@ def run_ours(args):
         ctx.check(st, "hx_solve")
     e3.record(lib_stream)
     e3.synchronize()
-    barrier()
-    t_e2e = max_over_ranks(e2.elapsed_time(e3) / 1e3)
+    barrier(ws)
+    t_e2e = max_over_ranks(e2.elapsed_time(e3) / 1e3, ws, dev)
     out_variants = None
     if rank == 0 and ws == 1 and not args.no_variants:
         out_variants = variants(hx, ctx, f, fac, f_d, fac_d, lib_stream)
