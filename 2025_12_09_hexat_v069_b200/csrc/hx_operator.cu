@@ -242,7 +242,7 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
   // The element factor and the node mask are plain loads.  In FP32 both are
   // fetched one plane ahead so that their latency overlaps a plane of work;
   // in FP64 the extra live registers would spill (128-register bound), so
-  // they are loaded where they are used.
+  // they are loaded where they are used (so is the face carry below).
   constexpr bool PREFETCH = sizeof(T) == 4;
   auto load_fac = [&](int ke) -> T {
     return (col_ok && ke >= 0 && ke < g.nze) ? A.fac[(int64_t)ke * eplane + (int64_t)jn * g.nxe + in]
@@ -254,6 +254,13 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
   };
   T f_next = PREFETCH ? load_fac(k0 - 1) : T(0);
   unsigned m_next = PREFETCH ? load_mask(k0) : 7u;
+  // FP32 also carries each plane's face transform from the layer it tops to
+  // the layer it bottoms (the plane is not modified in between)
+  T Pcarry[3][4];
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) Pcarry[c][q] = T(0);
 
   for (int ke = k0 - 1; ke < k1; ++ke) {
     T f;
@@ -277,12 +284,18 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       T v[4], Pb[4], Pt[4];
-      face(ke, c, v);
-      face_fwd(v, Pb);
+      if (PREFETCH && ke > k0 - 1) {  // this plane's face transform, from the layer below
+#pragma unroll
+        for (int q = 0; q < 4; ++q) Pb[q] = Pcarry[c][q];
+      } else {
+        face(ke, c, v);
+        face_fwd(v, Pb);
+      }
       face(ke + 1, c, v);
       face_fwd(v, Pt);
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
+        if (PREFETCH) Pcarry[c][q] = Pt[q];
         U[c][q] = Pb[q] + Pt[q];
         U[c][q + 4] = Pt[q] - Pb[q];
       }
