@@ -87,6 +87,7 @@ PROTOTYPES = {
     "hx_net_forward_backward": (_i32, [_vp, _i32, _i32, _i32, _vp, _vp, _vp, _vp]),
     "hx_net_prepare": (_i32, [_vp, _vp]),
     "hx_net_apply": (_i32, [_vp, _vp, _vp]),
+    "hx_selftest_wait_timeout": (_i32, [_vp, C.POINTER(_i32)]),
     "hx_simp_device": (_i32, [_vp, _vp, _dbl, _dbl, _dbl, _vp]),
     "hx_sensitivity_device": (_i32, [_vp, _vp, _vp, _dbl, _dbl, _dbl, _vp]),
     "hx_compliance_device": (_i32, [_vp, _vp, _vp, C.POINTER(_dbl)]),
@@ -305,6 +306,14 @@ class Context:
 
     def net_prepare(self, fac_ptr):
         self.check(self.lib.hx_net_prepare(self.h, C.c_void_p(fac_ptr)), "hx_net_prepare")
+
+    def selftest_wait_timeout(self):
+        """True when a convolution CTA's bounded wait ran out and was reported
+        (see hx_selftest_wait_timeout)."""
+        d = C.c_int32()
+        self.check(self.lib.hx_selftest_wait_timeout(self.h, C.byref(d)),
+                   "hx_selftest_wait_timeout")
+        return bool(d.value)
 
     def net_apply(self, r_ptr, z_ptr):
         self.check(self.lib.hx_net_apply(self.h, C.c_void_p(r_ptr), C.c_void_p(z_ptr)),

@@ -908,6 +908,14 @@ HX_API hx_status hx_net_prepare(hx_ctx* c, const double* fac) {
   });
 }
 
+HX_API hx_status hx_selftest_wait_timeout(hx_ctx* c, int32_t* detected) {
+  return guard(c, [&] {
+    HX_REQUIRE(detected != nullptr, "null argument");
+    *detected = hx::conv_wait_selftest(c) ? 1 : 0;
+    return HX_OK;
+  });
+}
+
 HX_API hx_status hx_net_apply(hx_ctx* c, const double* r, double* z) {
   return guard(c, [&] {
     need_mesh(c);

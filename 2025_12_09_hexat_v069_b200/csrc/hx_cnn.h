@@ -24,6 +24,9 @@ size_t conv_num_tiles(const GridN& g);
 // on the tcgen05 tensor cores; *err is set when a CTA's bounded wait ran out
 void launch_conv3(cudaStream_t s, int cout, const __nv_bfloat16* X, __nv_bfloat16* Y,
                   const __nv_bfloat16* W, const GridN& g, int* err);
+// failure-detection self test: one CTA whose wait must run out (8 x 16 x 4 nodes)
+void launch_conv3_selftest(cudaStream_t s, const __nv_bfloat16* X, __nv_bfloat16* Y,
+                           const __nv_bfloat16* W, int* err);
 // grad (+)= dW of one layer from the per-CTA partials
 void launch_conv3_wgrad(cudaStream_t s, const __nv_bfloat16* X, const __nv_bfloat16* D,
                         float* part, float* grad, bool accumulate, const GridN& g);

@@ -160,7 +160,9 @@ template <int COUT>
 __global__ void __launch_bounds__(NTHREADS) k_conv3_tc(const __grid_constant__ CUtensorMap xmap,
                                                        const __nv_bfloat16* __restrict__ W,
                                                        __nv_bfloat16* __restrict__ Y, GridN g,
-                                                       int* __restrict__ err) {
+                                                       int* __restrict__ err, int selftest) {
+  // selftest != 0 (hx_selftest_wait_timeout only): no load is issued, so the
+  // load barrier never completes and the bounded wait must run out
   extern __shared__ __align__(1024) unsigned char smem[];
   unsigned char* xs = smem;                        // [plane][1080 nodes][16 B]
   unsigned char* ws = smem + X_BYTES;              // [tap][plane][16 co][16 B]
@@ -185,15 +187,17 @@ __global__ void __launch_bounds__(NTHREADS) k_conv3_tc(const __grid_constant__ C
     *fail = 0;
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // barriers visible to TMA
     // the input tile (two 8-channel planes) and the layer's weights on one barrier
-    mbar_expect_tx(load_bar, TMA_BYTES + W_BYTES);
-    for (int h = 0; h < 2; ++h)
-      tma_load_4d(xb + (uint32_t)(h * PLANE_BYTES), &xmap, load_bar, h * 8, x0 - 1, y0 - 1,
-                  z0 - 1);
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
-            "r"(wsb),
-        "l"(W), "r"(W_BYTES), "r"(load_bar)
-        : "memory");
+    if (!selftest) {
+      mbar_expect_tx(load_bar, TMA_BYTES + W_BYTES);
+      for (int h = 0; h < 2; ++h)
+        tma_load_4d(xb + (uint32_t)(h * PLANE_BYTES), &xmap, load_bar, h * 8, x0 - 1, y0 - 1,
+                    z0 - 1);
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+          "[%3];" ::"r"(wsb),
+          "l"(W), "r"(W_BYTES), "r"(load_bar)
+          : "memory");
+    }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -204,7 +208,7 @@ __global__ void __launch_bounds__(NTHREADS) k_conv3_tc(const __grid_constant__ C
     if (!mbar_wait(load_bar, 0)) {
       *fail = 1;
       atomicExch(err, 1);
-      mbar_wait(load_bar, 0);  // give the loads in flight another bounded chance
+      if (!selftest) mbar_wait(load_bar, 0);  // give the loads in flight another bounded chance
     } else {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       // descriptors: a fixed part plus the start address (16-byte units, low
@@ -301,8 +305,8 @@ CUtensorMap activation_map(const __nv_bfloat16* X, const GridN& g) {
 
 }  // namespace
 
-void launch_conv3(cudaStream_t s, int cout, const __nv_bfloat16* X, __nv_bfloat16* Y,
-                  const __nv_bfloat16* W, const GridN& g, int* err) {
+static void conv3_launch(cudaStream_t s, int cout, const __nv_bfloat16* X, __nv_bfloat16* Y,
+                         const __nv_bfloat16* W, const GridN& g, int* err, int selftest) {
   HX_REQUIRE(cout == 16 || cout == 8, "unsupported conv configuration");
   HX_REQUIRE(err != nullptr, "conv error flag missing");
   static bool cfg[2] = {false, false};
@@ -315,10 +319,22 @@ void launch_conv3(cudaStream_t s, int cout, const __nv_bfloat16* X, __nv_bfloat1
   const CUtensorMap map = activation_map(X, g);
   const dim3 grid((unsigned)cdiv(g.nx, TX), (unsigned)cdiv(g.ny, TY), (unsigned)cdiv(g.nz, TZ));
   if (cout == 16)
-    k_conv3_tc<16><<<grid, NTHREADS, SMEM_BYTES, s>>>(map, W, Y, g, err);
+    k_conv3_tc<16><<<grid, NTHREADS, SMEM_BYTES, s>>>(map, W, Y, g, err, selftest);
   else
-    k_conv3_tc<8><<<grid, NTHREADS, SMEM_BYTES, s>>>(map, W, Y, g, err);
+    k_conv3_tc<8><<<grid, NTHREADS, SMEM_BYTES, s>>>(map, W, Y, g, err, selftest);
   HX_CHECK_LAUNCH();
+}
+
+void launch_conv3(cudaStream_t s, int cout, const __nv_bfloat16* X, __nv_bfloat16* Y,
+                  const __nv_bfloat16* W, const GridN& g, int* err) {
+  conv3_launch(s, cout, X, Y, W, g, err, 0);
+}
+
+// One CTA whose load barrier is never armed: its bounded wait runs out, it
+// records the error in *err and returns (no load or MMA in flight).
+void launch_conv3_selftest(cudaStream_t s, const __nv_bfloat16* X, __nv_bfloat16* Y,
+                           const __nv_bfloat16* W, int* err) {
+  conv3_launch(s, 16, X, Y, W, GridN{TX, TY, TZ}, err, 1);
 }
 
 }  // namespace hx

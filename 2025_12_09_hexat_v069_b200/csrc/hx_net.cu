@@ -465,6 +465,34 @@ double net_train_step(hx_ctx* c, const double* const* r, const double* const* e,
 
 void net_prepare(hx_ctx* c, const double* fac) { net_operator_inputs(c, fac); }
 
+// Failure detection of the tensor-core convolution, without a fault: one CTA
+// waits on a barrier nothing arrives on; its bounded wait must run out, set
+// the error flag and return.  Then an ordinary convolution on the same
+// context must succeed.  Returns whether the timeout was detected.
+bool conv_wait_selftest(hx_ctx* c) {
+  auto& N = c->net;
+  net_alloc_params(c);
+  const GridN g{8, 16, 4};
+  const size_t a = (size_t)g.nx * g.ny * g.nz * 16;
+  DevBuf<__nv_bfloat16> x, y;
+  x.ensure(a);
+  y.ensure(a);
+  HX_CUDA(cudaMemsetAsync(x.p, 0, a * sizeof(__nv_bfloat16), c->stream));
+  HX_CUDA(cudaMemsetAsync(N.wf.p, 0, NET_PARAMS * sizeof(__nv_bfloat16), c->stream));
+  HX_CUDA(cudaMemsetAsync(N.err.p, 0, sizeof(int), c->stream));
+  launch_conv3_selftest(c->stream, x.p, y.p, N.wf.p, N.err.p);
+  int e = 0;
+  HX_CUDA(cudaMemcpyAsync(&e, N.err.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  HX_CUDA(cudaStreamSynchronize(c->stream));
+  HX_CUDA(cudaMemsetAsync(N.err.p, 0, sizeof(int), c->stream));
+  // the context stays usable: an ordinary layer runs and reports no error
+  launch_conv3(c->stream, 16, x.p, y.p, N.wf.p, g, N.err.p);
+  check_conv_error(c);
+  if (N.ready) net_pack(c);  // restore the packed weights the test cleared
+  HX_CUDA(cudaStreamSynchronize(c->stream));
+  return e != 0;
+}
+
 // z = P r with the prepared operator (FP64 device vectors, grid numbering).
 void net_apply_vec(hx_ctx* c, const double* r, double* z) {
   require_prepared(c);

@@ -34,6 +34,7 @@ void net_forward_backward(hx_ctx* c, int nx, int ny, int nz, const float* x0, co
 double net_train_step(hx_ctx* c, const double* const* r, const double* const* e, int count,
                       double lr, int loss_kind);
 void net_prepare(hx_ctx* c, const double* fac);
+bool conv_wait_selftest(hx_ctx* c);
 void net_apply_vec(hx_ctx* c, const double* r, double* z);
 // Timing bodies on the prepared network: 0 = one 16 -> 16 conv layer on the
 // node grid, 1 = one preconditioner application (lift, 8 layers, output).

@@ -329,6 +329,14 @@ HX_API hx_status hx_net_forward_backward(hx_ctx *ctx, int32_t nx, int32_t ny,
 /* Operator inputs of the network (Jacobi scaling, density feature) for the
  * FP64 device factors `fac` on the current mesh and BCs. */
 HX_API hx_status hx_net_prepare(hx_ctx *ctx, const double *fac_dev);
+/* Failure detection of the tensor-core convolution (no reference
+ * counterpart): launches one convolution CTA whose load barrier is never
+ * armed, so its bounded wait (about a second at most) runs out; the kernel
+ * records the timeout and returns without a fault.  *detected = 1 when the
+ * host saw it; the call then runs an ordinary convolution on the same
+ * context and returns HX_OK only if that succeeds.  Clears the packed
+ * weights' staging and re-packs them from the loaded parameters. */
+HX_API hx_status hx_selftest_wait_timeout(hx_ctx *ctx, int32_t *detected);
 /* z = P r, the learned preconditioner of the prepared operator (FP64 device
  * vectors, grid numbering); z = 0 when r vanishes on the free DOFs. */
 HX_API hx_status hx_net_apply(hx_ctx *ctx, const double *r_dev, double *z_dev);

@@ -388,3 +388,25 @@ def test_mixed_precision_learned_fcg(ctx, hx):
     assert err < 1e-4
     c64, c = float(f_d @ u64), float(f_d @ u)
     assert abs(c - c64) <= 1e-5 * abs(c64)
+
+
+def test_conv_wait_timeout_is_reported(ctx, hx):
+    """Failure detection without a fault: a convolution CTA whose barrier is
+    never armed gives up after its bounded wait, the host reads the error,
+    and the context keeps working (the preconditioner gives the same result
+    as before the test, so the weights were restored)."""
+    import time
+    import torch
+    dims = (24, 8, 8)
+    f_d, fac_d = _problem(ctx, hx, dims, seed=5)
+    ctx.solve_device(f_d.data_ptr(), fac_d.data_ptr(), torch.zeros_like(f_d).data_ptr(),
+                     opts=hx.default_opts(tol=1e-3))
+    ctx.net_init(seed=8)
+    ctx.net_prepare(fac_d.data_ptr())
+    z0, z1 = torch.empty_like(f_d), torch.empty_like(f_d)
+    ctx.net_apply(f_d.data_ptr(), z0.data_ptr())
+    t0 = time.time()
+    assert ctx.selftest_wait_timeout()
+    assert time.time() - t0 < 30.0
+    ctx.net_apply(f_d.data_ptr(), z1.data_ptr())
+    assert torch.equal(z0, z1)
