@@ -256,54 +256,108 @@ __device__ __forceinline__ double field_coef(const CgState* sst, const CgState* 
   return den > 0.0 ? 2.0 * s / den : 0.0;
 }
 
+// The mesh-grid passes below run one CTA per coarse row: blockIdx.x is a
+// chunk of at most ROW_CX coarse x-cells (chunk width from row_chunk), y the
+// coarse y-row j, z the coarse z-plane k.  Every global access walks a fine
+// row as a contiguous run of DOFs (lane = DOF), so it is coalesced whatever
+// the row's alignment.
+constexpr int ROW_CX = 256;
+
+// D^-1/2 entry from an M^-1 entry: sqrt(m) as m rsqrt(m) (branch-free, a
+// few ulp; the field it scales is rounded to BF16), exactly 0 on fixed DOFs
+// (m = 0).  Both mesh-grid passes use it, so the preconditioner stays
+// symmetric.
+__device__ __forceinline__ float dinv_sqrt(float m) { return m > 0.f ? m * rsqrtf(m) : 0.f; }
+
+// Coarse x-cells per chunk: the coarse row split into near-equal chunks of at
+// most ROW_CX cells.
+static int row_chunk(int ncx) {
+  const int n = (int)cdiv(ncx, ROW_CX);
+  return (int)cdiv(ncx, n);
+}
+
 // Level-1 field of a DOF vector in one pass: out = R (k D^-1/2 v) with
 // D^-1/2 = sqrt(minv) (0 on fixed DOFs), R the full-weighting restriction
 // of k_restrict; the scaled field on the mesh's node grid is never stored.
 // T: the precision of the solver's vectors; the field is FP32 (it feeds the
 // BF16 network), so it is formed in FP32 whatever T is.
+//
+// Per CTA (coarse row (j, k), cells cx0 .. cx0+w-1, w <= RES_CX): the 9 fine
+// rows (2j+dy, 2k+dz), |dy|, |dz| <= 1, of v and minv are staged in shared
+// memory with cp.async (every copy of the CTA in flight at once; rows
+// outside the grid are read at a clamped index with weight 0), collapsed
+// with their y-z weights per fine DOF, then the x weights are applied.
+constexpr int RES_CX = 128;
+
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T* sdst, const T* gsrc) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(
+                   (unsigned)__cvta_generic_to_shared(sdst)),
+               "l"(gsrc), "n"(sizeof(T)));
+}
+
+// Dynamic shared memory of k_restrict_dof for chunk width cxw.
+template <typename T>
+static size_t restrict_smem(int cxw) {
+  const size_t seg = 3 * (2 * (size_t)cxw + 1);  // DOFs per staged row
+  return 18 * seg * sizeof(T) + seg * sizeof(float);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256)
     k_restrict_dof(const T* __restrict__ v, const T* __restrict__ minv, const CgState* sst,
                    const CgState* lst, int mode, double scale_mul, float* __restrict__ out,
-                   GridN gf, GridN gc) {
-  // one coarse node per thread; the 27 fine neighbours are read at clamped
-  // indices with weight 0 outside the grid, so every load is unconditional
-  // and they can all be in flight together
-  const int64_t nc = (int64_t)gc.nx * gc.ny * gc.nz;
-  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (n >= nc) return;
-  const float kc = (float)field_coef(sst, lst, mode, scale_mul);
-  const unsigned un = (unsigned)n, t = un / (unsigned)gc.nx;
-  const int i = (int)(un - t * (unsigned)gc.nx);
-  const int j = (int)(t % (unsigned)gc.ny), k = (int)(t / (unsigned)gc.ny);
-  float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+                   GridN gf, GridN gc, int cxw) {
+  extern __shared__ __align__(16) unsigned char rsm[];
+  const int seg = 3 * (2 * cxw + 1);
+  T* sm_m = reinterpret_cast<T*>(rsm);  // [9][seg]
+  T* sm_v = sm_m + 9 * seg;             // [9][seg]
+  float* srow = reinterpret_cast<float*>(sm_v + 9 * seg);  // [seg]
+  const int cx0 = blockIdx.x * cxw, w = min(cxw, gc.nx - cx0);
+  const int j = blockIdx.y, k = blockIdx.z;
+  // fine nodes 2 cx0 - 1 .. 2 (cx0 + w - 1) + 1, clipped to the grid
+  // (at most 2 w + 1 <= 2 cxw + 1 nodes)
+  const int fxa = max(2 * cx0 - 1, 0);
+  const int fxb = min(2 * (cx0 + w - 1) + 1, gf.nx - 1);
+  const int L = 3 * (fxb - fxa + 1);
+  float rw[9];
 #pragma unroll
-  for (int dz = -1; dz <= 1; ++dz) {
-    const int fz0 = 2 * k + dz;
-    const bool okz = fz0 >= 0 && fz0 < gf.nz;
-    const int fz = min(max(fz0, 0), gf.nz - 1);
+  for (int dz = -1; dz <= 1; ++dz)
 #pragma unroll
     for (int dy = -1; dy <= 1; ++dy) {
-      const int fy0 = 2 * j + dy;
-      const bool oky = okz && fy0 >= 0 && fy0 < gf.ny;
-      const int fy = min(max(fy0, 0), gf.ny - 1);
-      const int64_t fr = ((int64_t)fz * gf.ny + fy) * gf.nx;
-#pragma unroll
-      for (int dx = -1; dx <= 1; ++dx) {
-        const int fx0 = 2 * i + dx;
-        const bool ok = oky && fx0 >= 0 && fx0 < gf.nx;
-        const int fx = min(max(fx0, 0), gf.nx - 1);
-        const float w = ok ? fw(dz) * fw(dy) * fw(dx) : 0.f;
-        const int64_t f = 3 * (fr + fx);
-        a0 += w * sqrtf((float)minv[f + 0]) * (float)v[f + 0];
-        a1 += w * sqrtf((float)minv[f + 1]) * (float)v[f + 1];
-        a2 += w * sqrtf((float)minv[f + 2]) * (float)v[f + 2];
+      const int q = (dz + 1) * 3 + (dy + 1);
+      const int fz0 = 2 * k + dz, fy0 = 2 * j + dy;
+      const bool ok = fz0 >= 0 && fz0 < gf.nz && fy0 >= 0 && fy0 < gf.ny;
+      const int fz = min(max(fz0, 0), gf.nz - 1), fy = min(max(fy0, 0), gf.ny - 1);
+      const int64_t rb = 3 * (((int64_t)fz * gf.ny + fy) * gf.nx + fxa);
+      rw[q] = ok ? fw(dz) * fw(dy) : 0.f;
+      for (int dl = threadIdx.x; dl < L; dl += blockDim.x) {
+        cp_async_elem(sm_m + q * seg + dl, minv + rb + dl);
+        cp_async_elem(sm_v + q * seg + dl, v + rb + dl);
       }
     }
+  asm volatile("cp.async.commit_group;\n" ::);
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+  __syncthreads();
+  for (int dl = threadIdx.x; dl < L; dl += blockDim.x) {
+    float acc = 0.f;
+#pragma unroll
+    for (int q = 0; q < 9; ++q)
+      acc += rw[q] * (dinv_sqrt((float)sm_m[q * seg + dl]) * (float)sm_v[q * seg + dl]);
+    srow[dl] = acc;
   }
-  out[3 * n + 0] = kc * a0;
-  out[3 * n + 1] = kc * a1;
-  out[3 * n + 2] = kc * a2;
+  __syncthreads();
+  const float kc = (float)field_coef(sst, lst, mode, scale_mul);
+  const int64_t ob = 3 * (((int64_t)k * gc.ny + j) * gc.nx + cx0);
+  for (int e = threadIdx.x; e < 3 * w; e += blockDim.x) {
+    const int cl = e / 3, c = e - 3 * cl;
+    const int fx = 2 * (cx0 + cl);  // the coincident fine node
+    const int l = fx - fxa;
+    float a = srow[3 * l + c];
+    if (fx >= 1) a += 0.5f * srow[3 * (l - 1) + c];
+    if (fx + 1 < gf.nx) a += 0.5f * srow[3 * (l + 1) + c];
+    out[ob + e] = kc * a;
+  }
 }
 
 // Prolongation, the exact transpose of k_restrict (without normalisation):
@@ -390,61 +444,82 @@ __global__ void k_unlift(const __nv_bfloat16* __restrict__ Y, const float* __res
 // D^-1/2 = sqrt(minv) (masked DOFs have minv = 0).  With q_old: reduces
 // z.q_old and sets the flexible-CG coefficient st->beta = -(z.q_old) /
 // (p_old.q_old) (0 without a previous step).  T: vector precision.
-constexpr int OUT_NPT = 4;  // fine nodes per thread of k_net_output
-
+//
+// Per CTA (coarse row (j, k), cells cx0 .. cx0+w-1): the fine nodes
+// fx in [2 cx0, 2 (cx0 + w)), fy in {2j, 2j+1}, fz in {2k, 2k+1}.  The
+// coarse rows j, j+1 x k, k+1 are first interpolated in y and z into shared
+// memory (one row per fine (fy, fz)); each fine DOF then needs two shared
+// loads for its x interpolation.
 template <typename T>
 __global__ void __launch_bounds__(256)
     k_net_output(const T* __restrict__ r, const T* __restrict__ minv, const float* __restrict__ t,
-                 GridN gf, GridN gc, CgState* st, double scale_mul, T* __restrict__ z,
+                 GridN gf, GridN gc, int cxw, CgState* st, double scale_mul, T* __restrict__ z,
                  const T* __restrict__ q_old, double* partials) {
-  // OUT_NPT fine nodes per thread, each a block-wide coalesced chunk, with
-  // no dependence between them (one block partial of z.q_old per 1024
-  // nodes); the 8 coarse neighbours are read at valid indices with weight
-  // 0 where they do not exist, so every load is unconditional
+  __shared__ float cyz[4][(ROW_CX + 1) * 3];  // [oy + 2 oz][cell][c]
   if (st->status != HX_RUNNING) return;
   const double s = sqrt(st->rz * scale_mul);
-  const int64_t nf = (int64_t)gf.nx * gf.ny * gf.nz;
-  double zq = 0.0;
+  const int cx0 = blockIdx.x * cxw, w = min(cxw, gc.nx - cx0);
+  const int j = blockIdx.y, k = blockIdx.z;
+  {
+    // cells cx0 .. cx0 + w: the last is the right neighbour of the chunk's
+    // last odd fine node (0 past the grid, like rows j+1 and planes k+1)
+    const bool jn = j + 1 < gc.ny, kn = k + 1 < gc.nz;
+    const int64_t r00 = ((int64_t)k * gc.ny + j) * gc.nx;
+    const int64_t r10 = r00 + (jn ? gc.nx : 0);
+    const int64_t r01 = r00 + (kn ? (int64_t)gc.nx * gc.ny : 0);
+    const int64_t r11 = r01 + (jn ? gc.nx : 0);
+    const float wj = jn ? 0.5f : 0.f, wk = kn ? 0.5f : 0.f;
+    for (int e = threadIdx.x; e < 3 * (w + 1); e += blockDim.x) {
+      const int cl = e / 3, c = e - 3 * cl;
+      const int cx = cx0 + cl;
+      const float m = cx < gc.nx ? 1.f : 0.f;
+      const int64_t o = 3 * (int64_t)min(cx, gc.nx - 1) + c;
+      const float t00 = t[3 * r00 + o], t10 = t[3 * r10 + o];
+      const float t01 = t[3 * r01 + o], t11 = t[3 * r11 + o];
+      cyz[0][e] = m * t00;
+      cyz[1][e] = m * (0.5f * t00 + wj * t10);
+      cyz[2][e] = m * (0.5f * t00 + wk * t01);
+      cyz[3][e] = m * (0.25f * t00 + 0.5f * (wj * t10 + wk * t01) + wj * wk * t11);
+    }
+  }
+  __syncthreads();
+  // the (up to) 4 fine rows, each L DOFs: a thread takes the same DOF
+  // offset in every row (12 loads in flight); rows past the grid are read at
+  // row 0 and not stored
+  const int fx0 = 2 * cx0;
+  const int L = 3 * (min(2 * (cx0 + w), gf.nx) - fx0);
+  int64_t rowb[4];
+  bool rowok[4];
 #pragma unroll
-  for (int u = 0; u < OUT_NPT; ++u) {
-    const int64_t n = ((int64_t)blockIdx.x * OUT_NPT + u) * blockDim.x + threadIdx.x;
-    if (n >= nf) continue;
-    const unsigned un = (unsigned)n, tt = un / (unsigned)gf.nx;
-    const int fx = (int)(un - tt * (unsigned)gf.nx);
-    const int fy = (int)(tt % (unsigned)gf.ny), fz = (int)(tt / (unsigned)gf.ny);
-    int ix[2], iy[2], iz[2];
-    float wx[2], wy[2], wz[2];
-    prolong_axis(fx, gc.nx, ix, wx);
-    prolong_axis(fy, gc.ny, iy, wy);
-    prolong_axis(fz, gc.nz, iz, wz);
-    float a[3] = {0.f, 0.f, 0.f};
+  for (int q = 0; q < 4; ++q) {
+    const int fy = 2 * j + (q & 1), fz = 2 * k + (q >> 1);
+    rowok[q] = fy < gf.ny && fz < gf.nz;
+    rowb[q] = rowok[q] ? 3 * (((int64_t)fz * gf.ny + fy) * gf.nx + fx0) : rowb[0];
+  }
+  const float sf = (float)s;
+  T zq = T(0);  // per-thread partial in the vectors' precision
+  for (int dl = threadIdx.x; dl < L; dl += blockDim.x) {
+    const int fl = dl / 3, c = dl - 3 * fl;
+    const int ce = 3 * (fl >> 1) + c;
+    T mv[4], rv[4], qv[4];
 #pragma unroll
-    for (int az = 0; az < 2; ++az)
+    for (int q = 0; q < 4; ++q) {
+      mv[q] = minv[rowb[q] + dl];
+      rv[q] = r[rowb[q] + dl];
+      qv[q] = q_old ? q_old[rowb[q] + dl] : T(0);
+    }
 #pragma unroll
-      for (int ay = 0; ay < 2; ++ay) {
-        const int64_t cr = ((int64_t)iz[az] * gc.ny + iy[ay]) * gc.nx;
-        const float wyz = wz[az] * wy[ay];
-#pragma unroll
-        for (int ax = 0; ax < 2; ++ax) {
-          const float w = wyz * wx[ax];
-          const int64_t c3 = 3 * (cr + ix[ax]);
-          a[0] += w * t[c3 + 0];
-          a[1] += w * t[c3 + 1];
-          a[2] += w * t[c3 + 2];
-        }
-      }
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const int64_t i = 3 * n + c;
-      const T m = minv[i];
-      // the correction is BF16-accurate: its scale sqrt(minv) in FP32
-      const T zi = m * r[i] + (T)(s * (double)(sqrtf((float)m) * a[c]));
-      z[i] = zi;
-      if (q_old) zq += (double)zi * (double)q_old[i];
+    for (int q = 0; q < 4; ++q) {
+      if (!rowok[q]) continue;
+      const float a = (fl & 1) ? 0.5f * (cyz[q][ce] + cyz[q][ce + 3]) : cyz[q][ce];
+      // the correction is BF16-accurate: formed in FP32
+      const T zi = mv[q] * rv[q] + (T)(sf * dinv_sqrt((float)mv[q]) * a);
+      z[rowb[q] + dl] = zi;
+      zq += zi * qv[q];
     }
   }
   if (!q_old) return;
-  double v[1] = {zq};
+  double v[1] = {(double)zq};
   if (grid_reduce<1>(v, partials, &st->ticket[TK_AUX2]) && threadIdx.x == 0) {
     const double pq = st->pq;
     st->beta = (pq > 0.0 && isfinite(v[0])) ? -v[0] / pq : 0.0;
@@ -516,9 +591,16 @@ template <typename T>
 void launch_restrict_dof(cudaStream_t s, const T* v, const T* minv, const CgState* sst,
                          const CgState* lst, int mode, double scale_mul, float* out,
                          const GridN& gf, const GridN& gc) {
-  const int64_t nc = (int64_t)gc.nx * gc.ny * gc.nz;
-  k_restrict_dof<T><<<(unsigned)cdiv(nc, 256), 256, 0, s>>>(v, minv, sst, lst, mode, scale_mul,
-                                                            out, gf, gc);
+  static bool configured = false;  // per instantiation
+  if (!configured) {
+    HX_CUDA(cudaFuncSetAttribute(k_restrict_dof<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)restrict_smem<T>(RES_CX)));
+    configured = true;
+  }
+  const int cxw = (int)cdiv(gc.nx, cdiv(gc.nx, RES_CX));  // near-equal chunks <= RES_CX
+  const dim3 grid((unsigned)cdiv(gc.nx, cxw), (unsigned)gc.ny, (unsigned)gc.nz);
+  k_restrict_dof<T><<<grid, 256, restrict_smem<T>(cxw), s>>>(v, minv, sst, lst, mode, scale_mul,
+                                                             out, gf, gc, cxw);
   HX_CHECK_LAUNCH();
 }
 template void launch_restrict_dof<double>(cudaStream_t, const double*, const double*,
@@ -562,15 +644,18 @@ template <typename T>
 void launch_net_output(cudaStream_t s, const T* r, const T* minv, const float* t, const GridN& gf,
                        const GridN& gc, CgState* st, double scale_mul, T* z, const T* q_old,
                        double* partials) {
-  // one block partial per 256 * OUT_NPT nodes: `partials` must hold
+  // one block partial per coarse row chunk: `partials` must hold
   // net_output_blocks(gf)
-  k_net_output<T><<<(unsigned)net_output_blocks(gf), 256, 0, s>>>(r, minv, t, gf, gc, st,
-                                                                  scale_mul, z, q_old, partials);
+  const int cxw = row_chunk(gc.nx);
+  const dim3 grid((unsigned)cdiv(gc.nx, cxw), (unsigned)gc.ny, (unsigned)gc.nz);
+  k_net_output<T><<<grid, 256, 0, s>>>(r, minv, t, gf, gc, cxw, st, scale_mul, z, q_old,
+                                       partials);
   HX_CHECK_LAUNCH();
 }
 
 size_t net_output_blocks(const GridN& gf) {
-  return (size_t)cdiv((int64_t)gf.nx * gf.ny * gf.nz, 256 * OUT_NPT);
+  const GridN gc{(gf.nx - 1) / 2 + 1, (gf.ny - 1) / 2 + 1, (gf.nz - 1) / 2 + 1};
+  return (size_t)cdiv(gc.nx, row_chunk(gc.nx)) * gc.ny * gc.nz;
 }
 template void launch_net_output<double>(cudaStream_t, const double*, const double*, const float*,
                                         const GridN&, const GridN&, CgState*, double, double*,

@@ -13,8 +13,9 @@
 //    column, recomputing the one-element halo in x and y (atomic-free and
 //    deterministic);
 //  * node planes (tile + one-node halo) are staged into shared memory with
-//    cp.async into a 4-slot ring: plane k+3 loads while plane k+2 is
-//    transformed in place and planes k, k+1 feed the element products;
+//    cp.async into a ring of PF+1 slots: planes k+3 .. k+PF are in flight
+//    while plane k+2 is transformed in place and planes k, k+1 feed the
+//    element products (PF = mv_prefetch<T>, planes requested ahead);
 //  * the element product runs in the per-axis sum/difference (Haar) basis
 //    (45 nonzeros, see hx_common.cuh), one displacement component at a
 //    time to bound register pressure; the top-face outputs are carried in
@@ -35,6 +36,20 @@ namespace {
 
 constexpr int MV_BX = 32;
 constexpr int MV_BY = 8;
+constexpr int MV_RESIDENT = 2;  // CTAs per SM (the __launch_bounds__ minimum)
+
+// Planes requested ahead of the layer being computed (>= 3).  A deeper ring
+// keeps more bytes in flight per SM: FP32 runs 2% faster at depth 5 than 3
+// at 320x160x160; the FP64 fused ring at depth 4 (106 KB) drops to one CTA
+// per SM and runs 50% slower, so FP64 stays at 3.
+#ifndef HX_PF32
+#define HX_PF32 5
+#endif
+#ifndef HX_PF64
+#define HX_PF64 3
+#endif
+template <typename T>
+constexpr int mv_prefetch() { return sizeof(T) == 4 ? HX_PF32 : HX_PF64; }
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
   return (unsigned)__cvta_generic_to_shared(p);
@@ -47,18 +62,23 @@ __device__ __forceinline__ void cp_async_zfill(unsigned sdst, const void* gsrc, 
                "n"(BYTES), "r"(n));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
 // Shared-memory layout (dynamic).  Planes are component-major
 // ([c][row][node]) so the lanes of a warp touch consecutive words.
 template <typename T, int BY, bool FUSED>
 struct OpSmem {
   static constexpr int PLANE = 3 * (BY + 1) * (MV_BX + 1);
-  T p[4][PLANE];                   // x or p, 4-slot ring
-  T r[FUSED ? 2 : 1][PLANE];       // r (FUSED), 2-slot ring
-  T m[FUSED ? 2 : 1][PLANE];       // M^-1 (FUSED), 2-slot ring
-  T x[FUSED ? 2 : 1][PLANE];       // x (FUSED), 2-slot ring
-  T red[BY][3][MV_BX];             // y-direction partials
+  static constexpr int PF = mv_prefetch<T>();
+  static constexpr int NP = PF + 1;             // slots: k, k+1, k+2, k+3 .. k+PF
+  static constexpr int NR = FUSED ? PF - 1 : 1;  // slots: k+2 .. k+PF
+  static_assert(PF >= 3, "the ring needs planes k .. k+3");
+  T p[NP][PLANE];   // x or p
+  T r[NR][PLANE];   // r (FUSED)
+  T m[NR][PLANE];   // M^-1, or z in MODE 4 (FUSED)
+  T x[NR][PLANE];   // x (FUSED)
+  T red[BY][3][MV_BX];  // y-direction partials
 };
 
 template <typename T>
@@ -80,8 +100,9 @@ struct OpArgs {
   double* out;
 };
 
-__device__ __forceinline__ int ring4(int k) { return (k + 4) & 3; }
-__device__ __forceinline__ int ring2(int k) { return (k + 2) & 1; }
+// Ring slot of plane k >= -1.
+template <int N>
+__device__ __forceinline__ int ring(int k) { return (k + N) % N; }
 
 // 2D sum/difference transform of a node-plane face: v = corners (bx + 2by)
 // -> P = coefficients (sigma_x + 2 sigma_y).
@@ -128,6 +149,9 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
   constexpr int RW = MV_BX + 1;          // nodes per staged row
   constexpr int CPL = (BY + 1) * RW;      // staged nodes per component
   constexpr int NCP = (PLANE + NT - 1) / NT;
+  constexpr int PF = OpSmem<T, BY, FUSED>::PF;
+  constexpr int NP = OpSmem<T, BY, FUSED>::NP;
+  constexpr int NR = OpSmem<T, BY, FUSED>::NR;
   if (MODE >= 2 && A.st->status != HX_RUNNING) return;
   extern __shared__ __align__(16) unsigned char smraw[];
   OpSmem<T, BY, FUSED>& sm = *reinterpret_cast<OpSmem<T, BY, FUSED>*>(smraw);
@@ -165,13 +189,19 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
     flags |= (own ? 1u : 0u) << (8 + q);
   }
 
+  // One commit group per call, empty for planes past k1, so that the
+  // wait counts below hold to the end of the chunk.
   auto issue = [&](int kp) {
+    if (kp > k1) {
+      cp_async_commit();
+      return;
+    }
     const bool kin = kp >= 0 && kp < g.nzn;
     const int64_t base = (int64_t)kp * nplane * 3;
-    const unsigned sp = smem_u32(&sm.p[ring4(kp)][0]);
-    const unsigned sr = smem_u32(&sm.r[FUSED ? ring2(kp) : 0][0]);
-    const unsigned smv = smem_u32(&sm.m[FUSED ? ring2(kp) : 0][0]);
-    const unsigned sx = smem_u32(&sm.x[FUSED ? ring2(kp) : 0][0]);
+    const unsigned sp = smem_u32(&sm.p[ring<NP>(kp)][0]);
+    const unsigned sr = smem_u32(&sm.r[FUSED ? ring<NR>(kp) : 0][0]);
+    const unsigned smv = smem_u32(&sm.m[FUSED ? ring<NR>(kp) : 0][0]);
+    const unsigned sx = smem_u32(&sm.x[FUSED ? ring<NR>(kp) : 0][0]);
 #pragma unroll
     for (int q = 0; q < NCP; ++q) {
       const int idx = tid + q * NT;
@@ -196,10 +226,10 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
     if (!FUSED) return;
     const bool kown = kp >= k0 && kp < k1;
     const int64_t base = (int64_t)kp * nplane * 3;
-    T* ps = &sm.p[ring4(kp)][0];
-    const T* rs = &sm.r[ring2(kp)][0];
-    const T* ms = &sm.m[ring2(kp)][0];
-    const T* xs = &sm.x[ring2(kp)][0];
+    T* ps = &sm.p[ring<NP>(kp)][0];
+    const T* rs = &sm.r[ring<NR>(kp)][0];
+    const T* ms = &sm.m[ring<NR>(kp)][0];
+    const T* xs = &sm.x[ring<NR>(kp)][0];
 #pragma unroll
     for (int q = 0; q < NCP; ++q) {
       const int idx = tid + q * NT;
@@ -217,21 +247,23 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
   };
 
   auto face = [&](int kp, int c, T (&v)[4]) {
-    const T* ps = &sm.p[ring4(kp)][(c * (BY + 1) + ly) * RW + lx];
+    const T* ps = &sm.p[ring<NP>(kp)][(c * (BY + 1) + ly) * RW + lx];
     v[0] = ps[0];
     v[1] = ps[1];
     v[2] = ps[RW];
     v[3] = ps[RW + 1];
   };
 
-  // prologue: planes k0-1 and k0 staged (and transformed), k0+1 in flight
-  issue(k0 - 1);
-  issue(k0);
-  cp_async_wait_all();
+  // prologue: planes k0-1 .. k0+PF-3 requested (one group each); k0-1 and
+  // k0 staged and transformed; then k0+PF-2 into the r/M^-1/x slot of k0-1
+#pragma unroll
+  for (int d = -1; d <= PF - 3; ++d) issue(k0 + d);
+  cp_async_wait<PF - 3>();
   __syncthreads();
   transform(k0 - 1);
   transform(k0);
-  if (k0 + 1 <= k1) issue(k0 + 1);
+  __syncthreads();
+  issue(k0 + PF - 2);
   T Ytp[3][4];
 #pragma unroll
   for (int c = 0; c < 3; ++c)
@@ -275,10 +307,10 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
     } else {
       f = load_fac(ke);
     }
-    cp_async_wait_all();
-    __syncthreads();  // A: planes ke, ke+1 ready; ke+2 landed; red consumed
+    cp_async_wait<PF - 3>();  // groups up to ke+2 complete
+    __syncthreads();  // A: planes ke, ke+1 ready; ke+2 landed; ke-1 and red consumed
     if (ke + 2 <= k1) transform(ke + 2);
-    if (ke + 3 <= k1) issue(ke + 3);
+    issue(ke + PF);  // into the slot of plane ke-1
 
     T U[3][8];
 #pragma unroll
@@ -326,7 +358,7 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
     if (ke >= k0 && out_ok) {
       const int64_t node = (int64_t)ke * nplane + (int64_t)jn * g.nxn + in;
       const unsigned m = PREFETCH ? m_pre : (A.nmask ? A.nmask[node] : 7u);
-      const T* own = &sm.p[ring4(ke)][ly * RW + lx];
+      const T* own = &sm.p[ring<NP>(ke)][ly * RW + lx];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         T v = rowA[c] + sm.red[ly - 1][c][lx];
@@ -439,14 +471,23 @@ void launch_struct(cudaStream_t s, const OpArgs<T>& a) {
 }  // namespace
 
 int mv_kchunk(const Grid& g) {
-  // About eight resident CTAs per SM's worth of work, at least 8 planes per
-  // chunk so the recomputed halo layer stays small.
+  // Node planes per CTA: the chunk length kc (at least 8, so the two staged
+  // halo planes stay a small share) that minimises (waves of resident CTAs)
+  // x (planes each CTA stages, kc + 2).  A last wave that fills few SMs
+  // costs as much as a full one; ties go to the longer chunk.
   const int64_t cols = (int64_t)cdiv(g.nxn, MV_BX - 1) * cdiv(g.nyn, MV_BY - 1);
-  const int64_t want = 8LL * sm_count();
-  int nch = (int)std::max<int64_t>(1, (want + cols - 1) / cols);
-  int kc = (int)cdiv(g.nzn, nch);
-  if (kc < 8) kc = std::min(8, g.nzn);
-  return kc;
+  const int64_t slots = (int64_t)MV_RESIDENT * sm_count();
+  int best_kc = g.nzn;
+  int64_t best = INT64_MAX;
+  for (int kc = std::min(8, g.nzn); kc <= g.nzn; ++kc) {
+    const int64_t waves = cdiv(cols * cdiv(g.nzn, kc), slots);
+    const int64_t cost = waves * (kc + 2);
+    if (cost <= best) {
+      best = cost;
+      best_kc = kc;
+    }
+  }
+  return best_kc;
 }
 
 size_t mv_num_blocks(const Grid& g) {
