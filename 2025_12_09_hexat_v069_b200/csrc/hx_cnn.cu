@@ -263,11 +263,6 @@ __device__ __forceinline__ double field_coef(const CgState* sst, const CgState* 
 // the row's alignment.
 constexpr int ROW_CX = 256;
 
-// D^-1/2 entry from an M^-1 entry: sqrt(m) as m rsqrt(m) (branch-free, a
-// few ulp; the field it scales is rounded to BF16), exactly 0 on fixed DOFs
-// (m = 0).  Both mesh-grid passes use it, so the preconditioner stays
-// symmetric.
-__device__ __forceinline__ float dinv_sqrt(float m) { return m > 0.f ? m * rsqrtf(m) : 0.f; }
 
 // Coarse x-cells per chunk: the coarse row split into near-equal chunks of at
 // most ROW_CX cells.
@@ -360,6 +355,72 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// The same level-1 field from ys = BF16(D^-1/2 v) (k_cg_update2 writes it
+// with the residual): out = k R ys, one staged array of 2-byte entries.
+// cp.async copies 4-byte words, so each row is staged from the word holding
+// its first entry (a shift of 0 or 1 entries); the last word of the last row
+// may reach one entry past n, so ys holds n + 2 entries.
+__global__ void __launch_bounds__(256)
+    k_restrict_ys(const __nv_bfloat16* __restrict__ ys, const CgState* sst, double scale_mul,
+                  float* __restrict__ out, GridN gf, GridN gc, int cxw) {
+  extern __shared__ __align__(16) unsigned char rsm[];
+  const int seg = 3 * (2 * cxw + 1);
+  const int segw = seg / 2 + 2;  // words per staged row
+  uint32_t* sw = reinterpret_cast<uint32_t*>(rsm);  // [9][segw]
+  float* srow = reinterpret_cast<float*>(sw + 9 * segw);  // [seg]
+  const int cx0 = blockIdx.x * cxw, w = min(cxw, gc.nx - cx0);
+  const int j = blockIdx.y, k = blockIdx.z;
+  const int fxa = max(2 * cx0 - 1, 0);
+  const int fxb = min(2 * (cx0 + w - 1) + 1, gf.nx - 1);
+  const int L = 3 * (fxb - fxa + 1);
+  float rw[9];
+  int sh[9];
+  const uint32_t* yw = reinterpret_cast<const uint32_t*>(ys);
+#pragma unroll
+  for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+    for (int dy = -1; dy <= 1; ++dy) {
+      const int q = (dz + 1) * 3 + (dy + 1);
+      const int fz0 = 2 * k + dz, fy0 = 2 * j + dy;
+      const bool ok = fz0 >= 0 && fz0 < gf.nz && fy0 >= 0 && fy0 < gf.ny;
+      const int fz = min(max(fz0, 0), gf.nz - 1), fy = min(max(fy0, 0), gf.ny - 1);
+      const int64_t e0 = 3 * (((int64_t)fz * gf.ny + fy) * gf.nx + fxa);  // first entry
+      const int64_t w0 = e0 >> 1, w1 = (e0 + L + 1) >> 1;  // words [w0, w1)
+      rw[q] = ok ? fw(dz) * fw(dy) : 0.f;
+      sh[q] = (int)(e0 & 1);
+      const int nw = (int)(w1 - w0);
+      for (int t = threadIdx.x; t < nw; t += blockDim.x)
+        cp_async_elem(sw + q * segw + t, yw + w0 + t);
+    }
+  asm volatile("cp.async.commit_group;\n" ::);
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+  __syncthreads();
+  const __nv_bfloat16* sy = reinterpret_cast<const __nv_bfloat16*>(sw);
+  for (int dl = threadIdx.x; dl < L; dl += blockDim.x) {
+    float acc = 0.f;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) acc += rw[q] * __bfloat162float(sy[2 * q * segw + sh[q] + dl]);
+    srow[dl] = acc;
+  }
+  __syncthreads();
+  const float kc = (float)field_coef(sst, nullptr, 0, scale_mul);
+  const int64_t ob = 3 * (((int64_t)k * gc.ny + j) * gc.nx + cx0);
+  for (int e = threadIdx.x; e < 3 * w; e += blockDim.x) {
+    const int cl = e / 3, c = e - 3 * cl;
+    const int fx = 2 * (cx0 + cl);
+    const int l = fx - fxa;
+    float a = srow[3 * l + c];
+    if (fx >= 1) a += 0.5f * srow[3 * (l - 1) + c];
+    if (fx + 1 < gf.nx) a += 0.5f * srow[3 * (l + 1) + c];
+    out[ob + e] = kc * a;
+  }
+}
+
+static size_t restrict_ys_smem(int cxw) {
+  const size_t seg = 3 * (2 * (size_t)cxw + 1);
+  return 9 * (seg / 2 + 2) * sizeof(uint32_t) + seg * sizeof(float);
+}
+
 // Prolongation, the exact transpose of k_restrict (without normalisation):
 // fine[j][c] = (accumulate ? fine[j][c] : 0) + sum_{i: |j - 2i| <= 1} w(j - 2i) coarse[i][c].
 __global__ void k_prolong(const float* __restrict__ coarse, float* __restrict__ fine, GridN gf,
@@ -442,8 +503,9 @@ __global__ void k_unlift(const __nv_bfloat16* __restrict__ Y, const float* __res
 // z = M^-1 r + s D^-1/2 (R^T t)  with t the level-1 correction field (FP32
 // [node][3]), R^T the prolongation of k_prolong computed on the fly and
 // D^-1/2 = sqrt(minv) (masked DOFs have minv = 0).  With q_old: reduces
-// z.q_old and sets the flexible-CG coefficient st->beta = -(z.q_old) /
-// (p_old.q_old) (0 without a previous step).  T: vector precision.
+// z.q_old and z.r, sets the flexible-CG coefficient st->beta = -(z.q_old) /
+// (p_old.q_old) (0 without a previous step) and st->aux[3] = z.r (the
+// numerator of the step length, see k_struct MODE 4).  T: vector precision.
 //
 // Per CTA (coarse row (j, k), cells cx0 .. cx0+w-1): the fine nodes
 // fx in [2 cx0, 2 (cx0 + w)), fy in {2j, 2j+1}, fz in {2k, 2k+1}.  The
@@ -497,7 +559,7 @@ __global__ void __launch_bounds__(256)
     rowb[q] = rowok[q] ? 3 * (((int64_t)fz * gf.ny + fy) * gf.nx + fx0) : rowb[0];
   }
   const float sf = (float)s;
-  T zq = T(0);  // per-thread partial in the vectors' precision
+  T zq = T(0), zr = T(0);  // per-thread partials in the vectors' precision
   for (int dl = threadIdx.x; dl < L; dl += blockDim.x) {
     const int fl = dl / 3, c = dl - 3 * fl;
     const int ce = 3 * (fl >> 1) + c;
@@ -516,13 +578,15 @@ __global__ void __launch_bounds__(256)
       const T zi = mv[q] * rv[q] + (T)(sf * dinv_sqrt((float)mv[q]) * a);
       z[rowb[q] + dl] = zi;
       zq += zi * qv[q];
+      zr += zi * rv[q];
     }
   }
   if (!q_old) return;
-  double v[1] = {(double)zq};
-  if (grid_reduce<1>(v, partials, &st->ticket[TK_AUX2]) && threadIdx.x == 0) {
+  double v[2] = {(double)zq, (double)zr};
+  if (grid_reduce<2>(v, partials, &st->ticket[TK_AUX2]) && threadIdx.x == 0) {
     const double pq = st->pq;
     st->beta = (pq > 0.0 && isfinite(v[0])) ? -v[0] / pq : 0.0;
+    st->aux[3] = v[1];
   }
 }
 
@@ -610,6 +674,20 @@ template void launch_restrict_dof<float>(cudaStream_t, const float*, const float
                                          const CgState*, int, double, float*, const GridN&,
                                          const GridN&);
 
+void launch_restrict_ys(cudaStream_t s, const __nv_bfloat16* ys, const CgState* sst,
+                        double scale_mul, float* out, const GridN& gf, const GridN& gc) {
+  static bool configured = false;
+  if (!configured) {
+    HX_CUDA(cudaFuncSetAttribute(k_restrict_ys, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)restrict_ys_smem(RES_CX)));
+    configured = true;
+  }
+  const int cxw = (int)cdiv(gc.nx, cdiv(gc.nx, RES_CX));
+  const dim3 grid((unsigned)cdiv(gc.nx, cxw), (unsigned)gc.ny, (unsigned)gc.nz);
+  k_restrict_ys<<<grid, 256, restrict_ys_smem(cxw), s>>>(ys, sst, scale_mul, out, gf, gc, cxw);
+  HX_CHECK_LAUNCH();
+}
+
 void launch_restrict(cudaStream_t s, int ch, const float* in, float* out, const GridN& gf,
                      const GridN& gc, bool normalise) {
   const int64_t nc = (int64_t)gc.nx * gc.ny * gc.nz;
@@ -644,8 +722,8 @@ template <typename T>
 void launch_net_output(cudaStream_t s, const T* r, const T* minv, const float* t, const GridN& gf,
                        const GridN& gc, CgState* st, double scale_mul, T* z, const T* q_old,
                        double* partials) {
-  // one block partial per coarse row chunk: `partials` must hold
-  // net_output_blocks(gf)
+  // two block partials per coarse row chunk: `partials` must hold
+  // 2 net_output_blocks(gf) values
   const int cxw = row_chunk(gc.nx);
   const dim3 grid((unsigned)cdiv(gc.nx, cxw), (unsigned)gc.ny, (unsigned)gc.nz);
   k_net_output<T><<<grid, 256, 0, s>>>(r, minv, t, gf, gc, cxw, st, scale_mul, z, q_old,

@@ -102,6 +102,12 @@ enum : int {
 // in a fixed order by whichever block finishes last.  The result does not
 // depend on block scheduling, so repeated runs are bit-identical.
 // ---------------------------------------------------------------------------
+// D^-1/2 entry from an M^-1 entry: sqrt(m) as m rsqrt(m) (branch-free, a
+// few ulp; the fields it scales feed BF16 networks), exactly 0 on fixed
+// DOFs (m = 0).  Every pass of the learned preconditioner uses it, so the
+// preconditioner stays symmetric.
+__device__ __forceinline__ float dinv_sqrt(float m) { return m > 0.f ? m * rsqrtf(m) : 0.f; }
+
 template <int NV>
 __device__ __forceinline__ void warp_sum(double (&v)[NV]) {
 #pragma unroll

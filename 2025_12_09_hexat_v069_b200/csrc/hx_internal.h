@@ -63,11 +63,12 @@ void launch_pcg_step(cudaStream_t s, const T* pin, T* pout, const T* r, const T*
                      const T* fac, const uint8_t* nmask, const Grid& g, const ElemCoef<T>& K,
                      T shift, CgState* st, double* partials);
 // Flexible-CG step: p_out = z + beta p_in, x += alpha_old p_in (owned
-// nodes), q = mask(K p_out + s p_out), st->alpha = (p_out . r) / (p_out . q).
+// nodes), q = mask(K p_out + s p_out), st->alpha = (z . r) / (p_out . q)
+// with z . r in st->aux[3] (the preconditioner's output pass reduces it).
 template <typename T>
-void launch_fcg_step(cudaStream_t s, const T* pin, T* pout, const T* z, const T* r, T* x, T* q,
-                     const T* fac, const uint8_t* nmask, const Grid& g, const ElemCoef<T>& K,
-                     T shift, CgState* st, double* partials);
+void launch_fcg_step(cudaStream_t s, const T* pin, T* pout, const T* z, T* x, T* q, const T* fac,
+                     const uint8_t* nmask, const Grid& g, const ElemCoef<T>& K, T shift,
+                     CgState* st, double* partials);
 template <typename T>
 void launch_node_diag(cudaStream_t s, const T* fac, const uint8_t* bcfree, uint8_t* nmask, T* diag,
                       const Grid& g, const ElemCoef<double>& K, double* partials, CgState* st,
@@ -87,9 +88,13 @@ void launch_cg_update(cudaStream_t s, T* x, const T* p, T* r, const T* q, const 
                       CgState* st, double* partials);
 template <typename T>
 void launch_cg_pupdate(cudaStream_t s, T* p, const T* r, const T* minv, int64_t n, CgState* st);
+// ys (optional, n + 2 entries): BF16(D^-1/2 r) of the new residual, the
+// learned preconditioner's input
 template <typename T>
 void launch_cg_update2(cudaStream_t s, T* r, const T* q, const T* minv, int64_t n, CgState* st,
-                       double* partials);
+                       double* partials, __nv_bfloat16* ys = nullptr);
+template <typename T>
+void launch_dinv_bf16(cudaStream_t s, const T* r, const T* minv, __nv_bfloat16* ys, int64_t n);
 template <typename T>
 void launch_axpy_state(cudaStream_t s, T* dst, const T* x, const T* p, int64_t n,
                        const CgState* st, int when_snap);
@@ -216,6 +221,7 @@ struct hx_ctx {
     cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
     hx::DevBuf<double> z, scal, facbuf;
     hx::DevBuf<float> z32, s32;  // mixed-precision FCG: preconditioned vector, scratch
+    hx::DevBuf<__nv_bfloat16> ys;  // FCG: BF16(D^-1/2 r), n + 2 entries
     hx::DevBuf<int> err;         // set by a conv CTA whose bounded wait ran out
     const double* fac_last = nullptr;  // factors the operator inputs were built for
     int64_t prepared_dofs = -1;        // DOF count of the mesh they were built on

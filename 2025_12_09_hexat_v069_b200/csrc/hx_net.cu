@@ -123,7 +123,7 @@ void net_buffers(hx_ctx* c, bool train) {
   N.tmp[1].ensure(a1);
   N.lv[0].feat.ensure((size_t)nodes_of(level_grid(c->g, 0)));  // only the feature on level 0
   ensure_workspace(c);
-  const size_t need = net_output_blocks(level_grid(c->g, 0));
+  const size_t need = 2 * net_output_blocks(level_grid(c->g, 0));
   if (c->d_partials.n < need) c->d_partials.ensure(need);
   for (int l = 1; l <= NET_TOP; ++l) {
     const size_t nl = (size_t)nodes_of(level_grid(c->g, l));
@@ -215,17 +215,26 @@ void stack_backward_train(hx_ctx* c, int k, const GridN& g, const __nv_bfloat16*
 
 // z = M^-1 r + s D^-1/2 sum_l R_l^T E_l^T G_l^T G_l E_l R_l (D^-1/2 r / s).
 // The mesh-grid passes are fused: the level-1 field is restricted straight
-// from r (k_restrict_dof) and the level-1 correction is prolongated inside
-// the output kernel, so no field is stored on the mesh's node grid.  `train`
+// from BF16(D^-1/2 r) (k_restrict_ys) and the level-1 correction is
+// prolongated inside the output kernel, so no FP32 field is stored on the
+// mesh's node grid.  `train`
 // keeps the activations; q_old: FCG beta reduction (see k_net_output).
+// The level-1 field is restricted from ys = BF16(D^-1/2 r): passed in when
+// already formed (FCG loops: by the residual update), else formed here.
 // T: precision of r, minv, z, q_old (the solver's vectors).
 template <typename T>
 void precond_z(hx_ctx* c, const T* r, const T* minv, CgState* st, double scale_mul, T* z,
-               const T* q_old, bool train) {
+               const T* q_old, bool train, const __nv_bfloat16* ys = nullptr) {
   auto& N = c->net;
   GridN gl[NET_TOP + 1];
   for (int l = 0; l <= NET_TOP; ++l) gl[l] = level_grid(c->g, l);
-  launch_restrict_dof<T>(c->stream, r, minv, st, nullptr, 0, scale_mul, N.lv[1].x.p, gl[0], gl[1]);
+  if (!ys) {
+    const int64_t n = c->g.dofs();
+    __nv_bfloat16* y = N.ys.ensure(n + 2);
+    launch_dinv_bf16<T>(c->stream, r, minv, y, n);
+    ys = y;
+  }
+  launch_restrict_ys(c->stream, ys, st, scale_mul, N.lv[1].x.p, gl[0], gl[1]);
   for (int l = 2; l <= NET_TOP; ++l)
     launch_restrict(c->stream, 3, N.lv[l - 1].x.p, N.lv[l].x.p, gl[l - 1], gl[l], false);
   if (train) {
@@ -537,9 +546,12 @@ std::function<void()> net_time_body(hx_ctx* c, int which) {
   launch_cg_init<double>(c->stream, c->d_b.p, nullptr, c->d_minv.p, c->d_aux1.ensure(n),
                          c->d_aux2.ensure(n), n, s3, c->d_partials.p);
   double* z = N.z.ensure(n);
-  return [c, s3, z, n] {
+  // as in the FCG loops: the restriction reads BF16(D^-1/2 b)
+  __nv_bfloat16* ys = N.ys.ensure(n + 2);
+  launch_dinv_bf16<double>(c->stream, c->d_b.p, c->d_minv.p, ys, n);
+  return [c, s3, z, n, ys] {
     const double scale_mul = 1.0 / (double)n;
-    precond_z<double>(c, c->d_b.p, c->d_minv.p, s3, scale_mul, z, nullptr, false);
+    precond_z<double>(c, c->d_b.p, c->d_minv.p, s3, scale_mul, z, nullptr, false, ys);
   };
 }
 
@@ -579,11 +591,15 @@ static CgState learned_fcg(hx_ctx* c, const double* fac, const double* b, double
   *fallback = 0;
   *iters_out = 0;
   if (s0.status != HX_RUNNING || o.max_iter <= 0) return s0;
+  // ys = BF16(D^-1/2 r): formed here for the initial residual, then by
+  // every residual update
+  __nv_bfloat16* ys = N.ys.ensure(n + 2);
+  launch_dinv_bf16<double>(c->stream, r, minv, ys, n);
   auto one = [&](double* pin, double* pout) {
-    precond_z<double>(c, r, minv, st, scale_mul, z, q, false);
-    launch_fcg_step<double>(c->stream, pin, pout, z, r, x, q, fac, c->d_nmask.p, g, c->K, shift,
+    precond_z<double>(c, r, minv, st, scale_mul, z, q, false, ys);
+    launch_fcg_step<double>(c->stream, pin, pout, z, x, q, fac, c->d_nmask.p, g, c->K, shift,
                             st, c->d_partials.p);
-    launch_cg_update2<double>(c->stream, r, q, minv, n, st, c->d_partials.p);
+    launch_cg_update2<double>(c->stream, r, q, minv, n, st, c->d_partials.p, ys);
   };
   auto body = [&]() {
     one(P1, P0);
@@ -721,14 +737,18 @@ static CgState learned_fcg_mixed(hx_ctx* c, const double* fac, const double* b, 
   int best_it = 0;
   bool stalled = false;
   CgState sf{};
+  __nv_bfloat16* ys = N.ys.ensure(n + 2);
   for (;;) {
     float* Pin = parity ? P0 : P1;
     float* Pout = parity ? P1 : P0;
+    // ys = BF16(D^-1/2 r32) of the (replaced) residual; then every residual
+    // update keeps it current
+    launch_dinv_bf16<float>(c->stream, r32, minv32, ys, n);
     auto one = [&](float* pi, float* po) {
-      precond_z<float>(c, r32, minv32, si, scale_mul, z32, q32, false);
-      launch_fcg_step<float>(c->stream, pi, po, z32, r32, d32, q32, fac32, c->d_nmask.p, g, K32,
+      precond_z<float>(c, r32, minv32, si, scale_mul, z32, q32, false, ys);
+      launch_fcg_step<float>(c->stream, pi, po, z32, d32, q32, fac32, c->d_nmask.p, g, K32,
                              sh32, si, c->d_partials.p);
-      launch_cg_update2<float>(c->stream, r32, q32, minv32, n, si, c->d_partials.p);
+      launch_cg_update2<float>(c->stream, r32, q32, minv32, n, si, c->d_partials.p, ys);
     };
     auto body = [&]() {
       one(Pin, Pout);

@@ -22,8 +22,9 @@
 //    the Haar domain until the layer above adds its bottom face;
 //  * the four element columns around a node are summed with one warp
 //    shuffle (x) and one shared-memory exchange (y);
-//  * FUSED (the PCG step): the staged plane holds p_old, r, M^-1 and x; the
-//    in-place transform forms p = M^-1 r + beta p_old, and for owned nodes
+//  * FUSED (the PCG step): the staged plane holds p_old, r, M^-1 and x
+//    (the FCG step: p_old, z and x); the in-place transform forms
+//    p = M^-1 r + beta p_old (p = z + beta p_old), and for owned nodes
 //    stores p and updates x += alpha_old p_old.  p ping-pongs between two
 //    buffers so neighbouring CTAs never read a value another CTA rewrote.
 //    The epilogue applies the free-DOF mask and the shift and reduces p.q
@@ -84,7 +85,7 @@ struct OpSmem {
 template <typename T>
 struct OpArgs {
   const T* pin;   // vector to multiply (MODE 0-2) or p_old (FUSED)
-  const T* r;     // FUSED: residual
+  const T* r;     // MODE 3: residual
   const T* minv;  // MODE 3: Jacobi inverse diagonal; MODE 4: preconditioned z
   T* x;           // FUSED: solution (x += alpha_old p_old on owned nodes)
   T* pout;        // FUSED: new direction p
@@ -139,8 +140,11 @@ __device__ __forceinline__ void lambda_row(const ElemCoef<T>& K, const T (&U)[3]
 // MODE 0: q = mask(K x + s x);  MODE 1: also out[0] = x.q;
 // MODE 2: CG matvec, st->pq = p.q, st->alpha = rz / pq, breakdown test;
 // MODE 3: fused PCG step (see file header), then as MODE 2;
-// MODE 4: flexible-CG step: p = z + beta p_old (z from a nonlinear
-//         preconditioner), x += alpha_old p_old, q = K p; alpha = p.r / p.q.
+// MODE 4: flexible-CG step: p = z + beta p_old (z from a variable
+//         preconditioner), x += alpha_old p_old, q = K p; alpha = z.r / p.q
+//         with z.r from the preconditioner's output pass (st->aux[3]); p.r
+//         = z.r + beta p_old.r and the previous step length makes p_old.r
+//         vanish, so r is not staged.
 template <typename T, int BY, int MODE, int MINB>
 __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
   constexpr bool FUSED = MODE >= 3;
@@ -211,7 +215,7 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
       const unsigned so = (unsigned)idx * (unsigned)sizeof(T);
       cp_async_zfill<sizeof(T)>(sp + so, A.pin + gi, ok);
       if (FUSED) {
-        cp_async_zfill<sizeof(T)>(sr + so, A.r + gi, ok);
+        if (MODE == 3) cp_async_zfill<sizeof(T)>(sr + so, A.r + gi, ok);
         cp_async_zfill<sizeof(T)>(smv + so, A.minv + gi, ok);
         cp_async_zfill<sizeof(T)>(sx + so, A.x + gi, ok);
       }
@@ -221,7 +225,6 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
 
   // FUSED: p = M^-1 r + beta p_old (MODE 4: z + beta p_old) in place; owned
   // nodes of owned planes store p and advance x with the old direction.
-  double prsum = 0.0;  // MODE 4: p.r over owned DOFs
   auto transform = [&](int kp) {
     if (!FUSED) return;
     const bool kown = kp >= k0 && kp < k1;
@@ -241,7 +244,6 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
         const int64_t gi = base + goff[q];
         A.pout[gi] = pnew;
         A.x[gi] = xs[idx] + alpha_old * pold;
-        if (MODE == 4) prsum += (double)pnew * (double)rs[idx];
       }
     }
   };
@@ -371,14 +373,14 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
   }
 
   if (MODE == 4) {
-    double v[2] = {dsum, prsum};
-    if (grid_reduce<2>(v, A.partials, &A.st->ticket[TK_MATVEC]) && tid == 0) {
-      const double pq = v[0];
+    double v[1] = {dsum};
+    if (grid_reduce<1>(v, A.partials, &A.st->ticket[TK_MATVEC]) && tid == 0) {
+      const double pq = v[0], zr = A.st->aux[3];
       A.st->pq = pq;
-      if (!(pq > 0.0) || !isfinite(pq) || !isfinite(v[1]))
+      if (!(pq > 0.0) || !isfinite(pq) || !isfinite(zr))
         A.st->status = HX_ST_BREAKDOWN;
       else
-        A.st->alpha = v[1] / pq;
+        A.st->alpha = zr / pq;
     }
   } else if (MODE != 0) {
     double v[1] = {dsum};
@@ -542,13 +544,12 @@ void launch_pcg_step(cudaStream_t s, const T* pin, T* pout, const T* r, const T*
 }
 
 template <typename T>
-void launch_fcg_step(cudaStream_t s, const T* pin, T* pout, const T* z, const T* r, T* x, T* q,
-                     const T* fac, const uint8_t* nmask, const Grid& g, const ElemCoef<T>& K,
-                     T shift, CgState* st, double* partials) {
+void launch_fcg_step(cudaStream_t s, const T* pin, T* pout, const T* z, T* x, T* q, const T* fac,
+                     const uint8_t* nmask, const Grid& g, const ElemCoef<T>& K, T shift,
+                     CgState* st, double* partials) {
   OpArgs<T> a{};
   a.pin = pin;
   a.pout = pout;
-  a.r = r;
   a.minv = z;
   a.x = x;
   a.q = q;
@@ -563,13 +564,12 @@ void launch_fcg_step(cudaStream_t s, const T* pin, T* pout, const T* z, const T*
   launch_struct<T, 4>(s, a);
 }
 template void launch_fcg_step<double>(cudaStream_t, const double*, double*, const double*,
-                                      const double*, double*, double*, const double*,
-                                      const uint8_t*, const Grid&, const ElemCoef<double>&,
-                                      double, CgState*, double*);
-template void launch_fcg_step<float>(cudaStream_t, const float*, float*, const float*,
-                                     const float*, float*, float*, const float*, const uint8_t*,
-                                     const Grid&, const ElemCoef<float>&, float, CgState*,
-                                     double*);
+                                      double*, double*, const double*, const uint8_t*,
+                                      const Grid&, const ElemCoef<double>&, double, CgState*,
+                                      double*);
+template void launch_fcg_step<float>(cudaStream_t, const float*, float*, const float*, float*,
+                                     float*, const float*, const uint8_t*, const Grid&,
+                                     const ElemCoef<float>&, float, CgState*, double*);
 
 template void launch_matvec<double>(cudaStream_t, int, const double*, double*, const double*,
                                     const uint8_t*, const Grid&, const ElemCoef<double>&, double,

@@ -146,11 +146,13 @@ __global__ void k_cg_update(T* __restrict__ x, const T* __restrict__ p, T* __res
     cg_finish_iteration(st, v[0], v[1]);
 }
 
-// Second half of a fused PCG iteration: r -= alpha q, dots, tests.
+// Second half of a fused PCG iteration: r -= alpha q, dots, tests.  With
+// ys: also ys = BF16(D^-1/2 r) of the new residual (the learned
+// preconditioner's input, D^-1/2 = sqrt(minv)).
 template <typename T>
 __global__ void k_cg_update2(T* __restrict__ r, const T* __restrict__ q,
                              const T* __restrict__ minv, int64_t n, CgState* st,
-                             double* partials) {
+                             double* partials, __nv_bfloat16* __restrict__ ys) {
   if (st->status != HX_RUNNING) return;
   const T alpha = (T)st->alpha;
   double rz = 0, rr = 0;
@@ -165,6 +167,10 @@ __global__ void k_cg_update2(T* __restrict__ r, const T* __restrict__ q,
     rv.x -= alpha * qv.x;
     rv.y -= alpha * qv.y;
     r2[i] = rv;
+    if (ys)
+      reinterpret_cast<__nv_bfloat162*>(ys)[i] =
+          __floats2bfloat162_rn(dinv_sqrt((float)mv.x) * (float)rv.x,
+                                dinv_sqrt((float)mv.y) * (float)rv.y);
     rz += (double)rv.x * (double)(mv.x * rv.x) + (double)rv.y * (double)(mv.y * rv.y);
     rr += (double)rv.x * (double)rv.x + (double)rv.y * (double)rv.y;
   }
@@ -172,12 +178,22 @@ __global__ void k_cg_update2(T* __restrict__ r, const T* __restrict__ q,
     const int64_t i = n - 1;
     const T ri = r[i] - alpha * q[i];
     r[i] = ri;
+    if (ys) ys[i] = __float2bfloat16_rn(dinv_sqrt((float)minv[i]) * (float)ri);
     rz += (double)ri * (double)(minv[i] * ri);
     rr += (double)ri * (double)ri;
   }
   double v[2] = {rz, rr};
   if (grid_reduce<2>(v, partials, &st->ticket[TK_UPDATE]) && threadIdx.x == 0)
     cg_finish_iteration(st, v[0], v[1]);
+}
+
+// ys = BF16(D^-1/2 r), as k_cg_update2 writes it (for a residual that
+// another kernel produced).
+template <typename T>
+__global__ void k_dinv_bf16(const T* __restrict__ r, const T* __restrict__ minv,
+                            __nv_bfloat16* __restrict__ ys, int64_t n) {
+  for (int64_t i = gtid(); i < n; i += gstride())
+    ys[i] = __float2bfloat16_rn(dinv_sqrt((float)minv[i]) * (float)r[i]);
 }
 
 // dst = x + alpha p, with alpha from the state; `when_snap` restricts it to
@@ -314,8 +330,14 @@ void launch_cg_pupdate(cudaStream_t s, T* p, const T* r, const T* minv, int64_t 
 
 template <typename T>
 void launch_cg_update2(cudaStream_t s, T* r, const T* q, const T* minv, int64_t n, CgState* st,
-                       double* partials) {
-  k_cg_update2<T><<<vec_blocks(n), VEC_THREADS, 0, s>>>(r, q, minv, n, st, partials);
+                       double* partials, __nv_bfloat16* ys) {
+  k_cg_update2<T><<<vec_blocks(n), VEC_THREADS, 0, s>>>(r, q, minv, n, st, partials, ys);
+  HX_CHECK_LAUNCH();
+}
+
+template <typename T>
+void launch_dinv_bf16(cudaStream_t s, const T* r, const T* minv, __nv_bfloat16* ys, int64_t n) {
+  k_dinv_bf16<T><<<vec_blocks(n), VEC_THREADS, 0, s>>>(r, minv, ys, n);
   HX_CHECK_LAUNCH();
 }
 
@@ -333,7 +355,9 @@ void launch_axpy_state(cudaStream_t s, T* dst, const T* x, const T* p, int64_t n
                                     int64_t, CgState*, double*);                              \
   template void launch_cg_pupdate<T>(cudaStream_t, T*, const T*, const T*, int64_t, CgState*); \
   template void launch_cg_update2<T>(cudaStream_t, T*, const T*, const T*, int64_t, CgState*,  \
-                                     double*);                                                 \
+                                     double*, __nv_bfloat16*);                                 \
+  template void launch_dinv_bf16<T>(cudaStream_t, const T*, const T*, __nv_bfloat16*,         \
+                                    int64_t);                                                  \
   template void launch_axpy_state<T>(cudaStream_t, T*, const T*, const T*, int64_t,            \
                                      const CgState*, int);
 HX_INST_CG(double)
