@@ -356,69 +356,94 @@ __global__ void __launch_bounds__(256)
 }
 
 // The same level-1 field from ys = BF16(D^-1/2 v) (k_cg_update2 writes it
-// with the residual): out = k R ys, one staged array of 2-byte entries.
-// cp.async copies 4-byte words, so each row is staged from the word holding
-// its first entry (a shift of 0 or 1 entries); the last word of the last row
-// may reach one entry past n, so ys holds n + 2 entries.
+// with the residual): out = k R ys.  One CTA per (x-chunk of <= RES_CX
+// cells, block of YS_JB coarse y-rows j0.., coarse plane k): the fine rows
+// 2j0-1 .. 2(j0+YS_JB-1)+1 of planes 2k-1 .. 2k+1 (clamped to the grid) are
+// staged with 16-byte cp.async chunks, each row from the chunk holding its
+// first entry (a shift of 0-7 entries; the last chunk may reach 7 entries
+// past n, so ys holds n + 8 entries); each coarse row is then collapsed in
+// y and z per fine DOF and weighted in x.
+constexpr int YS_JB = 4;
+constexpr int YS_NY = 2 * YS_JB + 1;  // staged fine y-rows per plane
+
 __global__ void __launch_bounds__(256)
     k_restrict_ys(const __nv_bfloat16* __restrict__ ys, const CgState* sst, double scale_mul,
                   float* __restrict__ out, GridN gf, GridN gc, int cxw) {
   extern __shared__ __align__(16) unsigned char rsm[];
   const int seg = 3 * (2 * cxw + 1);
-  const int segw = seg / 2 + 2;  // words per staged row
-  uint32_t* sw = reinterpret_cast<uint32_t*>(rsm);  // [9][segw]
-  float* srow = reinterpret_cast<float*>(sw + 9 * segw);  // [seg]
+  const int segc = seg / 8 + 3;  // 16-byte chunks per staged row
+  uint4* sc = reinterpret_cast<uint4*>(rsm);                   // [3][YS_NY][segc]
+  float* srow = reinterpret_cast<float*>(sc + 3 * YS_NY * segc);  // [YS_JB][seg]
   const int cx0 = blockIdx.x * cxw, w = min(cxw, gc.nx - cx0);
-  const int j = blockIdx.y, k = blockIdx.z;
+  const int j0 = blockIdx.y * YS_JB, k = blockIdx.z;
+  const int jn = min(YS_JB, gc.ny - j0);  // coarse rows of this block
   const int fxa = max(2 * cx0 - 1, 0);
   const int fxb = min(2 * (cx0 + w - 1) + 1, gf.nx - 1);
   const int L = 3 * (fxb - fxa + 1);
-  float rw[9];
-  int sh[9];
-  const uint32_t* yw = reinterpret_cast<const uint32_t*>(ys);
-#pragma unroll
-  for (int dz = -1; dz <= 1; ++dz)
-#pragma unroll
-    for (int dy = -1; dy <= 1; ++dy) {
-      const int q = (dz + 1) * 3 + (dy + 1);
-      const int fz0 = 2 * k + dz, fy0 = 2 * j + dy;
-      const bool ok = fz0 >= 0 && fz0 < gf.nz && fy0 >= 0 && fy0 < gf.ny;
-      const int fz = min(max(fz0, 0), gf.nz - 1), fy = min(max(fy0, 0), gf.ny - 1);
-      const int64_t e0 = 3 * (((int64_t)fz * gf.ny + fy) * gf.nx + fxa);  // first entry
-      const int64_t w0 = e0 >> 1, w1 = (e0 + L + 1) >> 1;  // words [w0, w1)
-      rw[q] = ok ? fw(dz) * fw(dy) : 0.f;
-      sh[q] = (int)(e0 & 1);
-      const int nw = (int)(w1 - w0);
-      for (int t = threadIdx.x; t < nw; t += blockDim.x)
-        cp_async_elem(sw + q * segw + t, yw + w0 + t);
-    }
+  const int fy_lo = max(2 * j0 - 1, 0);
+  const int fy_hi = min(2 * (j0 + jn - 1) + 1, gf.ny - 1);
+  const int ny_r = fy_hi - fy_lo + 1;  // <= YS_NY
+  const uint4* yc = reinterpret_cast<const uint4*>(ys);
+  // one flat loop over (staged row, chunk) so that every thread copies
+  for (int u = threadIdx.x; u < 3 * ny_r * segc; u += blockDim.x) {
+    const int t = u / segc, cu = u - t * segc;
+    const int dz = t / ny_r - 1, yy = t - (dz + 1) * ny_r;
+    const int fz = min(max(2 * k + dz, 0), gf.nz - 1);
+    const int64_t e0 = 3 * (((int64_t)fz * gf.ny + fy_lo + yy) * gf.nx + fxa);
+    const int64_t c0 = e0 >> 3, c1 = (e0 + L + 7) >> 3;
+    if (cu < c1 - c0)
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(
+                       (unsigned)__cvta_generic_to_shared(sc + ((dz + 1) * YS_NY + yy) * segc + cu)),
+                   "l"(yc + c0 + cu));
+  }
   asm volatile("cp.async.commit_group;\n" ::);
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   __syncthreads();
-  const __nv_bfloat16* sy = reinterpret_cast<const __nv_bfloat16*>(sw);
-  for (int dl = threadIdx.x; dl < L; dl += blockDim.x) {
-    float acc = 0.f;
+  const __nv_bfloat16* sy = reinterpret_cast<const __nv_bfloat16*>(sc);
+  for (int jj = 0; jj < jn; ++jj) {
+    const int j = j0 + jj;
+    // the 9 (dz, dy) rows of coarse row j: staged index and weight (0 outside the grid)
+    int off[9];
+    float rw[9];
 #pragma unroll
-    for (int q = 0; q < 9; ++q) acc += rw[q] * __bfloat162float(sy[2 * q * segw + sh[q] + dl]);
-    srow[dl] = acc;
+    for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int q = (dz + 1) * 3 + (dy + 1);
+        const int fz0 = 2 * k + dz, fy0 = 2 * j + dy;
+        const bool ok = fz0 >= 0 && fz0 < gf.nz && fy0 >= 0 && fy0 < gf.ny;
+        const int yy = min(max(fy0, fy_lo), fy_hi) - fy_lo;
+        const int fz = min(max(fz0, 0), gf.nz - 1);
+        const int64_t e0 = 3 * (((int64_t)fz * gf.ny + fy_lo + yy) * gf.nx + fxa);
+        off[q] = 8 * ((dz + 1) * YS_NY + yy) * segc + (int)(e0 & 7);
+        rw[q] = ok ? fw(dz) * fw(dy) : 0.f;
+      }
+    float* sr = srow + jj * seg;
+    for (int dl = threadIdx.x; dl < L; dl += blockDim.x) {
+      float acc = 0.f;
+#pragma unroll
+      for (int q = 0; q < 9; ++q) acc += rw[q] * __bfloat162float(sy[off[q] + dl]);
+      sr[dl] = acc;
+    }
   }
   __syncthreads();
   const float kc = (float)field_coef(sst, nullptr, 0, scale_mul);
-  const int64_t ob = 3 * (((int64_t)k * gc.ny + j) * gc.nx + cx0);
-  for (int e = threadIdx.x; e < 3 * w; e += blockDim.x) {
-    const int cl = e / 3, c = e - 3 * cl;
+  for (int e = threadIdx.x; e < 3 * w * jn; e += blockDim.x) {
+    const int jj = e / (3 * w), ex = e - jj * 3 * w;
+    const int cl = ex / 3, c = ex - 3 * cl;
     const int fx = 2 * (cx0 + cl);
     const int l = fx - fxa;
-    float a = srow[3 * l + c];
-    if (fx >= 1) a += 0.5f * srow[3 * (l - 1) + c];
-    if (fx + 1 < gf.nx) a += 0.5f * srow[3 * (l + 1) + c];
-    out[ob + e] = kc * a;
+    const float* sr = srow + jj * seg;
+    float a = sr[3 * l + c];
+    if (fx >= 1) a += 0.5f * sr[3 * (l - 1) + c];
+    if (fx + 1 < gf.nx) a += 0.5f * sr[3 * (l + 1) + c];
+    out[3 * (((int64_t)k * gc.ny + j0 + jj) * gc.nx + cx0) + ex] = kc * a;
   }
 }
 
 static size_t restrict_ys_smem(int cxw) {
   const size_t seg = 3 * (2 * (size_t)cxw + 1);
-  return 9 * (seg / 2 + 2) * sizeof(uint32_t) + seg * sizeof(float);
+  return 3 * YS_NY * (seg / 8 + 3) * 16 + YS_JB * seg * sizeof(float);
 }
 
 // Prolongation, the exact transpose of k_restrict (without normalisation):
@@ -683,7 +708,7 @@ void launch_restrict_ys(cudaStream_t s, const __nv_bfloat16* ys, const CgState* 
     configured = true;
   }
   const int cxw = (int)cdiv(gc.nx, cdiv(gc.nx, RES_CX));
-  const dim3 grid((unsigned)cdiv(gc.nx, cxw), (unsigned)gc.ny, (unsigned)gc.nz);
+  const dim3 grid((unsigned)cdiv(gc.nx, cxw), (unsigned)cdiv(gc.ny, YS_JB), (unsigned)gc.nz);
   k_restrict_ys<<<grid, 256, restrict_ys_smem(cxw), s>>>(ys, sst, scale_mul, out, gf, gc, cxw);
   HX_CHECK_LAUNCH();
 }

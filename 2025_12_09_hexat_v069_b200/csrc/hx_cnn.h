@@ -39,7 +39,7 @@ template <typename T>
 void launch_restrict_dof(cudaStream_t s, const T* v, const T* minv, const CgState* sst,
                          const CgState* lst, int mode, double scale_mul, float* out,
                          const GridN& gf, const GridN& gc);
-// the same field (mode 0) from ys = BF16(D^-1/2 v), n + 2 entries
+// the same field (mode 0) from ys = BF16(D^-1/2 v), n + 8 entries
 void launch_restrict_ys(cudaStream_t s, const __nv_bfloat16* ys, const CgState* sst,
                         double scale_mul, float* out, const GridN& gf, const GridN& gc);
 // full-weighting restriction fine -> coarse node grid (ch 3 or 1), and its transpose

@@ -88,7 +88,7 @@ void launch_cg_update(cudaStream_t s, T* x, const T* p, T* r, const T* q, const 
                       CgState* st, double* partials);
 template <typename T>
 void launch_cg_pupdate(cudaStream_t s, T* p, const T* r, const T* minv, int64_t n, CgState* st);
-// ys (optional, n + 2 entries): BF16(D^-1/2 r) of the new residual, the
+// ys (optional, n + 8 entries): BF16(D^-1/2 r) of the new residual, the
 // learned preconditioner's input
 template <typename T>
 void launch_cg_update2(cudaStream_t s, T* r, const T* q, const T* minv, int64_t n, CgState* st,
@@ -221,7 +221,7 @@ struct hx_ctx {
     cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
     hx::DevBuf<double> z, scal, facbuf;
     hx::DevBuf<float> z32, s32;  // mixed-precision FCG: preconditioned vector, scratch
-    hx::DevBuf<__nv_bfloat16> ys;  // FCG: BF16(D^-1/2 r), n + 2 entries
+    hx::DevBuf<__nv_bfloat16> ys;  // FCG: BF16(D^-1/2 r), n + 8 entries
     hx::DevBuf<int> err;         // set by a conv CTA whose bounded wait ran out
     const double* fac_last = nullptr;  // factors the operator inputs were built for
     int64_t prepared_dofs = -1;        // DOF count of the mesh they were built on

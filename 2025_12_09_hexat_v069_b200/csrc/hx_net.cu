@@ -230,7 +230,7 @@ void precond_z(hx_ctx* c, const T* r, const T* minv, CgState* st, double scale_m
   for (int l = 0; l <= NET_TOP; ++l) gl[l] = level_grid(c->g, l);
   if (!ys) {
     const int64_t n = c->g.dofs();
-    __nv_bfloat16* y = N.ys.ensure(n + 2);
+    __nv_bfloat16* y = N.ys.ensure(n + 8);
     launch_dinv_bf16<T>(c->stream, r, minv, y, n);
     ys = y;
   }
@@ -547,7 +547,7 @@ std::function<void()> net_time_body(hx_ctx* c, int which) {
                          c->d_aux2.ensure(n), n, s3, c->d_partials.p);
   double* z = N.z.ensure(n);
   // as in the FCG loops: the restriction reads BF16(D^-1/2 b)
-  __nv_bfloat16* ys = N.ys.ensure(n + 2);
+  __nv_bfloat16* ys = N.ys.ensure(n + 8);
   launch_dinv_bf16<double>(c->stream, c->d_b.p, c->d_minv.p, ys, n);
   return [c, s3, z, n, ys] {
     const double scale_mul = 1.0 / (double)n;
@@ -593,7 +593,7 @@ static CgState learned_fcg(hx_ctx* c, const double* fac, const double* b, double
   if (s0.status != HX_RUNNING || o.max_iter <= 0) return s0;
   // ys = BF16(D^-1/2 r): formed here for the initial residual, then by
   // every residual update
-  __nv_bfloat16* ys = N.ys.ensure(n + 2);
+  __nv_bfloat16* ys = N.ys.ensure(n + 8);
   launch_dinv_bf16<double>(c->stream, r, minv, ys, n);
   auto one = [&](double* pin, double* pout) {
     precond_z<double>(c, r, minv, st, scale_mul, z, q, false, ys);
@@ -737,7 +737,7 @@ static CgState learned_fcg_mixed(hx_ctx* c, const double* fac, const double* b, 
   int best_it = 0;
   bool stalled = false;
   CgState sf{};
-  __nv_bfloat16* ys = N.ys.ensure(n + 2);
+  __nv_bfloat16* ys = N.ys.ensure(n + 8);
   for (;;) {
     float* Pin = parity ? P0 : P1;
     float* Pout = parity ? P1 : P0;
