@@ -6,32 +6,34 @@
 // The transpose (backward-data pass) is the same kernel on the flipped,
 // per-tap transposed weights.
 //
-// One CTA (4 warps) computes an 8 x 16 x 4 node tile.  Implicit GEMM per
-// z-slice: M = 128 nodes (8 x by 16 y), N = 16 output channels, K = 27 taps
-// x 16 channels, as 27 MMAs of M128 N16 K16 accumulating in 16 TMEM columns
-// (4 slices: 64 columns).
+// One CTA (4 warps) computes an 8 x 16 x TZ node tile (TZ = 2).  Implicit
+// GEMM per z-slice: M = 128 nodes (8 x by 16 y), N = 16 output channels,
+// K = 27 taps x 16 channels, as 27 MMAs of M128 N16 K16 accumulating in 16
+// TMEM columns (2 slices: 32 columns).
 //
 // Shared-memory layout.  An MMA operand descriptor (no swizzle, K-major)
 // addresses 8-row core matrices whose rows are 16 bytes apart; the stride
 // between consecutive core matrices (SBO) and between the two 8-channel
 // halves of K (LBO) are descriptor fields.  The input tile with its one-node
-// halo (10 x 18 x 6 nodes) is staged as two planes of 8 channels, 16 bytes
-// per node, x fastest: node (z, y, x) at ((z * 18 + y) * 10 + x) * 16.  The
+// halo (10 x 18 x (TZ + 2) nodes) is staged as two planes of 8 channels, 16
+// bytes per node, x fastest: node (z, y, x) at ((z * 18 + y) * 10 + x) * 16.  The
 // 128 rows of z-slice z for tap (dz, dy, dx) are then 16 core matrices, one
 // per y, of 8 consecutive x: core matrix j starts at node
 // ((z + 1 + dz) * 18 + 1 + dy + j) * 10 + 1 + dx, i.e. a fixed start plus
 // j * 160 bytes (SBO = 160).  Every tap is a start address in the same
-// staged tile, so one TMA tile load per plane (box 8 ch x 10 x 18 x 6 from
+// staged tile, so one TMA tile load per plane (box 8 ch x 10 x 18 x 4 from
 // the [z][y][x][16 ch] activation tensor; coordinates outside the grid read
 // as zero) stages all the operands.  Row m of the accumulator is node
 // (x0 + m % 8, y0 + m / 8).  The weights are staged as [tap][plane][co][8 ci]
 // (the B operand, N = 16 rows).
 //
-// One tile per CTA; with 48 KB of shared memory 4 CTAs share an SM, so the
+// One tile per CTA; with 37 KB of shared memory 6 CTAs share an SM, so the
 // loads of some overlap the MMAs and epilogues of others (a persistent
-// variant with a 2-stage load ring, at 2 CTAs per SM, measured slower).
+// variant with a 2-stage load ring, at 2 CTAs per SM, measured slower; so
+// did TZ = 4, with twice the MMAs per CTA and half the CTAs: 12.9 against
+// 11.7 us per layer on a 81 x 41 x 41 grid).
 // Thread 0 issues the tile's TMA loads and the bulk copy of the layer's
-// weights (pre-packed in this order) on one mbarrier, then the 108 MMAs
+// weights (pre-packed in this order) on one mbarrier, then the 54 MMAs
 // and a tcgen05.commit on a second.  Every wait is bounded; on timeout the
 // CTA records it in *err, waits (bounded) for its own loads, frees its TMEM
 // and returns, and the host reports the error.
@@ -47,15 +49,18 @@ namespace hx {
 
 namespace {
 
-constexpr int TX = 8, TY = 16, TZ = 4;
+#ifndef HX_CONV_TZ
+#define HX_CONV_TZ 2
+#endif
+constexpr int TX = 8, TY = 16, TZ = HX_CONV_TZ;
 constexpr int BX = TX + 2, BY = TY + 2, BZ = TZ + 2;          // staged box with halo
-constexpr int BOX_NODES = BX * BY * BZ;                       // 1080
-constexpr int PLANE_BYTES = BOX_NODES * 16;                   // 17280
-constexpr int X_BYTES = 2 * PLANE_BYTES;                      // 34560: [plane]
+constexpr int BOX_NODES = BX * BY * BZ;                       // 720
+constexpr int PLANE_BYTES = BOX_NODES * 16;                   // 11520
+constexpr int X_BYTES = 2 * PLANE_BYTES;                      // 23040: [plane]
 constexpr int W_BYTES = 27 * 2 * 16 * 16;                     // 13824: [tap][plane][co]
 constexpr int SMEM_BYTES = X_BYTES + W_BYTES + 64;            // + barriers, TMEM address
 constexpr int NTHREADS = 128;
-constexpr int TMEM_COLS = 64;                                 // TZ slices x 16 columns
+constexpr int TMEM_COLS = TZ * 16 < 32 ? 32 : TZ * 16;       // TZ slices x 16 columns
 constexpr uint32_t TMA_BYTES = (uint32_t)X_BYTES;
 constexpr long long WAIT_LIMIT = 1ll << 20;                   // polls before giving up
 
@@ -164,7 +169,7 @@ __global__ void __launch_bounds__(NTHREADS) k_conv3_tc(const __grid_constant__ C
   // selftest != 0 (hx_selftest_wait_timeout only): no load is issued, so the
   // load barrier never completes and the bounded wait must run out
   extern __shared__ __align__(1024) unsigned char smem[];
-  unsigned char* xs = smem;                        // [plane][1080 nodes][16 B]
+  unsigned char* xs = smem;                        // [plane][720 nodes][16 B]
   unsigned char* ws = smem + X_BYTES;              // [tap][plane][16 co][16 B]
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + X_BYTES + W_BYTES);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2);
@@ -174,7 +179,7 @@ __global__ void __launch_bounds__(NTHREADS) k_conv3_tc(const __grid_constant__ C
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = blockIdx.z * TZ;
 
-  if (warp == 0) {  // TMEM for the 4 accumulators
+  if (warp == 0) {  // TMEM for the TZ accumulators
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(tmem_slot)),
                  "r"(TMEM_COLS)
@@ -212,7 +217,7 @@ __global__ void __launch_bounds__(NTHREADS) k_conv3_tc(const __grid_constant__ C
     } else {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       // descriptors: a fixed part plus the start address (16-byte units, low
-      // bits), so each of the 108 MMAs adds a compile-time offset
+      // bits), so each of the 27 TZ MMAs adds a compile-time offset
       const uint64_t a0 = smem_desc(xb, PLANE_BYTES, BX * 16);
       const uint64_t b0 = smem_desc(wsb, 256, 128);
       constexpr uint32_t idesc = instr_desc(128, 16);
@@ -285,7 +290,7 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 }
 
 // Tensor map of an activation tensor [nz][ny][nx][16 ch] BF16 with the
-// staging box (8 ch, 10 x, 18 y, 6 z).
+// staging box (8 ch, 10 x, 18 y, TZ + 2 z).
 CUtensorMap activation_map(const __nv_bfloat16* X, const GridN& g) {
   auto fn = encode_fn();
   HX_REQUIRE(fn != nullptr, "cuTensorMapEncodeTiled is not available from the driver");
