@@ -29,6 +29,34 @@ struct Vec2<float> {
   using type = float2;
 };
 
+// 16 bytes of T, loaded and stored as one vector (W entries)
+template <typename T>
+struct Vec16;
+template <>
+struct Vec16<double> {
+  using type = double2;
+  static constexpr int W = 2;
+  __device__ static void get(const double2& v, double (&a)[2]) { a[0] = v.x; a[1] = v.y; }
+  __device__ static double2 make(const double (&a)[2]) { return make_double2(a[0], a[1]); }
+};
+template <>
+struct Vec16<float> {
+  using type = float4;
+  static constexpr int W = 4;
+  __device__ static void get(const float4& v, float (&a)[4]) {
+    a[0] = v.x;
+    a[1] = v.y;
+    a[2] = v.z;
+    a[3] = v.w;
+  }
+  __device__ static float4 make(const float (&a)[4]) { return make_float4(a[0], a[1], a[2], a[3]); }
+};
+
+__device__ __forceinline__ uint32_t bf16x2_bits(float a, float b) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<const uint32_t*>(&h);
+}
+
 __device__ __forceinline__ int64_t gtid() {
   return (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
 }
@@ -148,7 +176,8 @@ __global__ void k_cg_update(T* __restrict__ x, const T* __restrict__ p, T* __res
 
 // Second half of a fused PCG iteration: r -= alpha q, dots, tests.  With
 // ys: also ys = BF16(D^-1/2 r) of the new residual (the learned
-// preconditioner's input, D^-1/2 = sqrt(minv)).
+// preconditioner's input, D^-1/2 = sqrt(minv)).  16-byte vector accesses
+// (4 FP32 or 2 FP64 entries per thread and step), then a scalar tail.
 template <typename T>
 __global__ void k_cg_update2(T* __restrict__ r, const T* __restrict__ q,
                              const T* __restrict__ minv, int64_t n, CgState* st,
@@ -156,26 +185,36 @@ __global__ void k_cg_update2(T* __restrict__ r, const T* __restrict__ q,
   if (st->status != HX_RUNNING) return;
   const T alpha = (T)st->alpha;
   double rz = 0, rr = 0;
-  using V = typename Vec2<T>::type;
-  const int64_t n2 = n >> 1;
-  V* r2 = reinterpret_cast<V*>(r);
-  const V* q2 = reinterpret_cast<const V*>(q);
-  const V* m2 = reinterpret_cast<const V*>(minv);
-  for (int64_t i = gtid(); i < n2; i += gstride()) {
-    V rv = r2[i];
-    const V qv = q2[i], mv = m2[i];
-    rv.x -= alpha * qv.x;
-    rv.y -= alpha * qv.y;
-    r2[i] = rv;
-    if (ys)
-      reinterpret_cast<__nv_bfloat162*>(ys)[i] =
-          __floats2bfloat162_rn(dinv_sqrt((float)mv.x) * (float)rv.x,
-                                dinv_sqrt((float)mv.y) * (float)rv.y);
-    rz += (double)rv.x * (double)(mv.x * rv.x) + (double)rv.y * (double)(mv.y * rv.y);
-    rr += (double)rv.x * (double)rv.x + (double)rv.y * (double)rv.y;
+  using VT = Vec16<T>;
+  using V = typename VT::type;
+  constexpr int W = VT::W;
+  const int64_t nv = n / W;
+  V* rV = reinterpret_cast<V*>(r);
+  const V* qV = reinterpret_cast<const V*>(q);
+  const V* mV = reinterpret_cast<const V*>(minv);
+  for (int64_t i = gtid(); i < nv; i += gstride()) {
+    T ra[W], qa[W], ma[W];
+    VT::get(rV[i], ra);
+    VT::get(qV[i], qa);
+    VT::get(mV[i], ma);
+    float ya[W];
+#pragma unroll
+    for (int e = 0; e < W; ++e) {
+      ra[e] -= alpha * qa[e];
+      ya[e] = dinv_sqrt((float)ma[e]) * (float)ra[e];
+      rz += (double)ra[e] * (double)(ma[e] * ra[e]);
+      rr += (double)ra[e] * (double)ra[e];
+    }
+    rV[i] = VT::make(ra);
+    if (ys) {
+      if constexpr (W == 4)
+        reinterpret_cast<uint2*>(ys)[i] =
+            make_uint2(bf16x2_bits(ya[0], ya[1]), bf16x2_bits(ya[2], ya[3]));
+      else
+        reinterpret_cast<uint32_t*>(ys)[i] = bf16x2_bits(ya[0], ya[1]);
+    }
   }
-  if ((n & 1) && gtid() == 0) {
-    const int64_t i = n - 1;
+  for (int64_t i = nv * W + gtid(); i < n; i += gstride()) {
     const T ri = r[i] - alpha * q[i];
     r[i] = ri;
     if (ys) ys[i] = __float2bfloat16_rn(dinv_sqrt((float)minv[i]) * (float)ri);
