@@ -217,20 +217,28 @@ __global__ void k_restrict(const float* __restrict__ in, float* __restrict__ out
     const int i = (int)(n % gc.nx);
     const int64_t t = n / gc.nx;
     const int j = (int)(t % gc.ny), k = (int)(t / gc.ny);
+    // the 27 fine neighbours at clamped indices, weight 0 outside the grid:
+    // every load is unconditional, so they can all be in flight together
     float acc[CH];
 #pragma unroll
     for (int c = 0; c < CH; ++c) acc[c] = 0.f;
     float wsum = 0.f;
+#pragma unroll
     for (int dz = -1; dz <= 1; ++dz) {
-      const int fz = 2 * k + dz;
-      if (fz < 0 || fz >= gf.nz) continue;
+      const int fz0 = 2 * k + dz;
+      const bool okz = fz0 >= 0 && fz0 < gf.nz;
+      const int fz = min(max(fz0, 0), gf.nz - 1);
+#pragma unroll
       for (int dy = -1; dy <= 1; ++dy) {
-        const int fy = 2 * j + dy;
-        if (fy < 0 || fy >= gf.ny) continue;
+        const int fy0 = 2 * j + dy;
+        const bool oky = okz && fy0 >= 0 && fy0 < gf.ny;
+        const int fy = min(max(fy0, 0), gf.ny - 1);
+#pragma unroll
         for (int dx = -1; dx <= 1; ++dx) {
-          const int fx = 2 * i + dx;
-          if (fx < 0 || fx >= gf.nx) continue;
-          const float w = fw(dz) * fw(dy) * fw(dx);
+          const int fx0 = 2 * i + dx;
+          const bool ok = oky && fx0 >= 0 && fx0 < gf.nx;
+          const int fx = min(max(fx0, 0), gf.nx - 1);
+          const float w = ok ? fw(dz) * fw(dy) * fw(dx) : 0.f;
           const int64_t f = ((int64_t)fz * gf.ny + fy) * gf.nx + fx;
 #pragma unroll
           for (int c = 0; c < CH; ++c) acc[c] += w * in[f * CH + c];
@@ -468,8 +476,8 @@ __global__ void k_prolong(const float* __restrict__ coarse, float* __restrict__ 
       for (int ay = 0; ay < 2; ++ay)
 #pragma unroll
         for (int ax = 0; ax < 2; ++ax) {
+          // absent neighbours have index 0 and weight 0 (prolong_axis): no branch
           const float w = wz[az] * wy[ay] * wx[ax];
-          if (w == 0.f) continue;
           const int64_t c = ((int64_t)iz[az] * gc.ny + iy[ay]) * gc.nx + ix[ax];
           a0 += w * coarse[3 * c + 0];
           a1 += w * coarse[3 * c + 1];
