@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(HERE, "libhexat_b200.so")
 HX_OK, HX_NOT_CONVERGED, HX_STALLED, HX_BREAKDOWN, HX_NONFINITE = 0, 1, 2, 3, 4
 HX_OOM, HX_BAD_ARG, HX_CUDA_ERROR, HX_NO_DEVICE, HX_DIVERGED = 5, 6, 7, 8, 9
 HX_F32, HX_F64 = 0, 1
-HX_PREC_FP64, HX_PREC_MIXED32, HX_PREC_MIXED_BF16 = 0, 1, 2
+HX_PREC_FP64, HX_PREC_MIXED32 = 0, 1
 HX_PC_JACOBI, HX_PC_LEARNED, HX_PC_NONE = 0, 1, 2
 (HX_KERNEL_PCG_STEP_FP64, HX_KERNEL_PCG_UPDATE_FP64, HX_KERNEL_APPLY_FP64, HX_KERNEL_PCG_STEP_FP32,
  HX_KERNEL_FILTER_MATVEC, HX_KERNEL_CONV3, HX_KERNEL_NET_APPLY) = range(7)

@@ -52,8 +52,9 @@ hx_status guard(hx_ctx* c, F&& f) {
 void set_grid_impl(hx_ctx* c, int64_t nx, int64_t ny, int64_t nz, double dx, double dy,
                    double dz) {
   HX_REQUIRE(nx >= 1 && ny >= 1 && nz >= 1, "grid needs at least one element per axis");
-  HX_REQUIRE(nx < (1 << 20) && ny < (1 << 20) && nz < (1 << 20), "grid axis too long");
-  HX_REQUIRE((nx + 1) * (ny + 1) * (nz + 1) * 3 < (int64_t(1) << 40), "grid too large");
+  HX_REQUIRE(hx::grid_extent_ok(nx, ny, nz),
+             "grid too large (axes below 2^20 nodes, 3 x nodes per z-plane below 2^31, "
+             "DOFs below 2^40)");
   HX_REQUIRE(dx > 0 && dy > 0 && dz > 0, "element size must be positive");
   c->g.nxe = (int)nx;
   c->g.nye = (int)ny;
@@ -105,6 +106,7 @@ void set_mesh_impl(hx_ctx* c, const float* nodes, int64_t nN, const int64_t* el,
     dims[d] = (int64_t)std::llround((mx[d] - mn[d]) / h[d]);
     HX_REQUIRE(dims[d] >= 1, "mesh is flat along an axis");
   }
+  HX_REQUIRE(hx::grid_extent_ok(dims[0], dims[1], dims[2]), "mesh bounding grid too large");
   // node -> lattice position
   Grid g{};
   g.nxe = (int)dims[0];
@@ -617,6 +619,7 @@ HX_API hx_status hx_apply_gpu_filter(hx_ctx* c, const float* density, int64_t nx
   return guard(c, [&] {
     HX_REQUIRE(density && filtered, "null argument");
     HX_REQUIRE(nx >= 1 && ny >= 1 && nz >= 1 && dx > 0 && dy > 0 && dz > 0, "bad grid");
+    HX_REQUIRE(hx::grid_extent_ok(nx, ny, nz), "grid too large");
     Grid g{};
     g.nxe = (int)nx;
     g.nye = (int)ny;

@@ -657,12 +657,11 @@ size_t conv_num_tiles(const GridN& g) {
 void launch_conv3_wgrad(cudaStream_t s, const __nv_bfloat16* X, const __nv_bfloat16* D,
                         float* part, float* grad, bool accumulate, const GridN& g) {
   const size_t smem = (HNODES + TX * TY * TZ) * C * sizeof(__nv_bfloat16);
-  static bool cfg = false;
-  if (!cfg) {
+  static PerDeviceOnce cfg;
+  cfg.run([&] {
     HX_CUDA(cudaFuncSetAttribute(k_conv3_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem));
-    cfg = true;
-  }
+  });
   k_conv3_wgrad<<<conv_grid(g), NTHREADS, smem, s>>>(X, D, part, g);
   HX_CHECK_LAUNCH();
   const int len = 27 * 256;
@@ -688,12 +687,11 @@ template <typename T>
 void launch_restrict_dof(cudaStream_t s, const T* v, const T* minv, const CgState* sst,
                          const CgState* lst, int mode, double scale_mul, float* out,
                          const GridN& gf, const GridN& gc) {
-  static bool configured = false;  // per instantiation
-  if (!configured) {
+  static PerDeviceOnce configured;  // per instantiation and device
+  configured.run([&] {
     HX_CUDA(cudaFuncSetAttribute(k_restrict_dof<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)restrict_smem<T>(RES_CX)));
-    configured = true;
-  }
+  });
   const int cxw = (int)cdiv(gc.nx, cdiv(gc.nx, RES_CX));  // near-equal chunks <= RES_CX
   const dim3 grid((unsigned)cdiv(gc.nx, cxw), (unsigned)gc.ny, (unsigned)gc.nz);
   k_restrict_dof<T><<<grid, 256, restrict_smem<T>(cxw), s>>>(v, minv, sst, lst, mode, scale_mul,
@@ -709,12 +707,11 @@ template void launch_restrict_dof<float>(cudaStream_t, const float*, const float
 
 void launch_restrict_ys(cudaStream_t s, const __nv_bfloat16* ys, const CgState* sst,
                         double scale_mul, float* out, const GridN& gf, const GridN& gc) {
-  static bool configured = false;
-  if (!configured) {
+  static PerDeviceOnce configured;
+  configured.run([&] {
     HX_CUDA(cudaFuncSetAttribute(k_restrict_ys, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)restrict_ys_smem(RES_CX)));
-    configured = true;
-  }
+  });
   const int cxw = (int)cdiv(gc.nx, cdiv(gc.nx, RES_CX));
   const dim3 grid((unsigned)cdiv(gc.nx, cxw), (unsigned)cdiv(gc.ny, YS_JB), (unsigned)gc.nz);
   k_restrict_ys<<<grid, 256, restrict_ys_smem(cxw), s>>>(ys, sst, scale_mul, out, gf, gc, cxw);

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <string>
 
 #include "../../include/hexat_b200.h"
@@ -325,7 +326,41 @@ ElemCoef<float> to_float(const ElemCoef<double>& k);
 // Launch geometry helpers.
 inline unsigned cdiv(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
 
-// Number of SMs of the current device (cached per process).
+// Number of SMs of the current device (cached per device, thread-safe).
 int sm_count();
+
+// Ordinal of the calling thread's current device.
+int current_device();
+
+// Runs a per-device set-up step (a kernel attribute such as the dynamic
+// shared-memory opt-in, which CUDA keeps per device) once for each device it
+// is used on.  Thread-safe: concurrent first calls may both run the step,
+// which must therefore be idempotent.  Devices beyond the 64 tracked ones
+// run it on every call.
+class PerDeviceOnce {
+ public:
+  template <typename F>
+  void run(F&& step) {
+    const int dev = current_device();
+    const bool tracked = dev >= 0 && dev < 64;
+    const uint64_t bit = tracked ? (uint64_t(1) << dev) : 0;
+    if (tracked && (done_.load(std::memory_order_acquire) & bit)) return;
+    step();
+    if (tracked) done_.fetch_or(bit, std::memory_order_acq_rel);
+  }
+
+ private:
+  std::atomic<uint64_t> done_{0};
+};
+
+// Largest grids the structured kernels index: nodes per axis below 2^20, a
+// node plane's DOFs (3 * nxn * nyn) below 2^31 (in-plane offsets are 32-bit)
+// and all DOFs below 2^40.  True when nx x ny x nz elements fit.
+inline bool grid_extent_ok(int64_t nx, int64_t ny, int64_t nz) {
+  if (nx < 1 || ny < 1 || nz < 1) return false;
+  if (nx >= (1 << 20) || ny >= (1 << 20) || nz >= (1 << 20)) return false;
+  if (3 * (nx + 1) * (ny + 1) >= (int64_t(1) << 31)) return false;
+  return 3 * (nx + 1) * (ny + 1) * (nz + 1) < (int64_t(1) << 40);
+}
 
 }  // namespace hx

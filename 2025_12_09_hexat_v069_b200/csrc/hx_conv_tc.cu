@@ -34,9 +34,13 @@
 // 11.7 us per layer on a 81 x 41 x 41 grid).
 // Thread 0 issues the tile's TMA loads and the bulk copy of the layer's
 // weights (pre-packed in this order) on one mbarrier, then the 54 MMAs
-// and a tcgen05.commit on a second.  Every wait is bounded; on timeout the
-// CTA records it in *err, waits (bounded) for its own loads, frees its TMEM
-// and returns, and the host reports the error.
+// and a tcgen05.commit on a second.  Every wait is bounded (1 s of
+// %globaltimer time); on timeout the CTA records it in *err, waits once more
+// (bounded) for its own loads or MMAs, frees its TMEM and returns, and the
+// host reports the error.  Residual hazard: if that second wait also runs
+// out, the CTA returns with its TMA writes or MMAs still in flight, and a
+// later CTA on the SM could see its shared memory or TMEM overwritten; the
+// error flag has then already failed the call.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
@@ -62,7 +66,11 @@ constexpr int SMEM_BYTES = X_BYTES + W_BYTES + 64;            // + barriers, TME
 constexpr int NTHREADS = 128;
 constexpr int TMEM_COLS = TZ * 16 < 32 ? 32 : TZ * 16;       // TZ slices x 16 columns
 constexpr uint32_t TMA_BYTES = (uint32_t)X_BYTES;
-constexpr long long WAIT_LIMIT = 1ll << 20;                   // polls before giving up
+// Bounded waits: a wait gives up after WAIT_NS of %globaltimer time or
+// WAIT_POLLS polls, whichever comes first (the poll count only backs up the
+// clock).
+constexpr unsigned long long WAIT_NS = 1000000000ull;  // 1 s
+constexpr long long WAIT_POLLS = 1ll << 24;
 
 static_assert(TX == 8 && TX * TY == 128, "a z-slice is 16 core matrices of 8 x-nodes");
 static_assert(PLANE_BYTES % 128 == 0, "TMA destinations 128-byte aligned");
@@ -114,10 +122,19 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t phase) {
   return done != 0;
 }
 
-// bounded wait; false when the limit was reached
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// bounded wait; false when the time (or poll) limit was reached
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
-  for (long long i = 0; i < WAIT_LIMIT; ++i)
+  const unsigned long long t0 = global_ns();
+  for (long long i = 0; i < WAIT_POLLS; ++i) {
     if (mbar_try_wait(bar, phase)) return true;
+    if (global_ns() - t0 > WAIT_NS) return false;
+  }
   return false;
 }
 
@@ -239,6 +256,9 @@ __global__ void __launch_bounds__(NTHREADS) k_conv3_tc(const __grid_constant__ C
   if (ok && !mbar_wait(mma_bar, 0)) {
     ok = false;
     atomicExch(err, 1);
+    // the committed MMAs may still be writing TMEM: give them another
+    // bounded wait before the allocation is released below
+    mbar_wait(mma_bar, 0);
   }
   if (ok) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -314,13 +334,12 @@ static void conv3_launch(cudaStream_t s, int cout, const __nv_bfloat16* X, __nv_
                          const __nv_bfloat16* W, const GridN& g, int* err, int selftest) {
   HX_REQUIRE(cout == 16 || cout == 8, "unsupported conv configuration");
   HX_REQUIRE(err != nullptr, "conv error flag missing");
-  static bool cfg[2] = {false, false};
+  static PerDeviceOnce cfg[2];  // per output width and device
   const int idx = cout == 16 ? 0 : 1;
-  if (!cfg[idx]) {
+  cfg[idx].run([&] {
     HX_CUDA(cudaFuncSetAttribute(cout == 16 ? k_conv3_tc<16> : k_conv3_tc<8>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
-    cfg[idx] = true;
-  }
+  });
   const CUtensorMap map = activation_map(X, g);
   const dim3 grid((unsigned)cdiv(g.nx, TX), (unsigned)cdiv(g.ny, TY), (unsigned)cdiv(g.nz, TZ));
   if (cout == 16)

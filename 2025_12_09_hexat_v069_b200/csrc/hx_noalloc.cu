@@ -68,10 +68,16 @@ extern "C" HX_API hx_status hx_apply_stiffness_noalloc(int64_t nx, int64_t ny, i
                                                        const double* x, const double* factor,
                                                        double* y, double* xKx, void* stream) {
   if (!x || !factor || !y || !xKx) return HX_BAD_ARG;
-  // the operator stages x with 8-byte copies
-  if ((reinterpret_cast<uintptr_t>(x) & 7u) != 0) return HX_BAD_ARG;
-  if (nx < 1 || ny < 1 || nz < 1 || nx >= (1 << 20) || ny >= (1 << 20) || nz >= (1 << 20))
+  // Every array is read or written as FP64 words, and the operator stages x
+  // in 16-byte chunks: a misaligned pointer is refused here, before anything
+  // reaches the GPU, rather than becoming a misaligned-address fault that
+  // would end the caller's CUDA context.
+  const auto misaligned = [](const void* p, uintptr_t a) {
+    return (reinterpret_cast<uintptr_t>(p) & (a - 1)) != 0;
+  };
+  if (misaligned(x, 16) || misaligned(factor, 8) || misaligned(y, 8) || misaligned(xKx, 8))
     return HX_BAD_ARG;
+  if (!hx::grid_extent_ok(nx, ny, nz)) return HX_BAD_ARG;
   if (!(dx > 0 && dy > 0 && dz > 0) || !(nu > -1.0 && nu < 0.5)) return HX_BAD_ARG;
   hx::Grid g{};
   g.nxe = (int)nx;
@@ -80,7 +86,6 @@ extern "C" HX_API hx_status hx_apply_stiffness_noalloc(int64_t nx, int64_t ny, i
   g.nxn = g.nxe + 1;
   g.nyn = g.nye + 1;
   g.nzn = g.nze + 1;
-  if (g.dofs() >= (int64_t(1) << 40)) return HX_BAD_ARG;
   // The reduction writes one partial sum per CTA of the operator kernel.
   if (hx::mv_num_blocks(g) > (size_t)HX_NOALLOC_MAX_BLOCKS) return HX_BAD_ARG;
   unsigned char* base = nullptr;

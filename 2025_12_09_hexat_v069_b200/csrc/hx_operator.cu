@@ -2,9 +2,9 @@
 // fused with the CG direction/solution updates.
 //
 // Layout in HBM: node n = i + NXn*(j + NYn*k) (i fastest, src/Mesh/Mesh.jl:
-// 114-116), vectors interleaved 3 per node (dof = 3n + c), element
-// e = i + NXe*(j + NYe*k) (Mesh.jl:145-156), one factor per element, one
-// byte of free-DOF bits per node.
+// 13-15), vectors interleaved 3 per node (dof = 3n + c), element
+// e = i + NXe*(j + NYe*k) (the element loop of Mesh.jl:44-55), one factor
+// per element, one byte of free-DOF bits per node.
 //
 // Kernel design (replaces the one-thread-per-element, 24-atomics kernel of
 // src/Solvers/GPUSolver.jl:37-79 and the broadcast kernels around it):
@@ -460,12 +460,11 @@ void launch_struct(cudaStream_t s, const OpArgs<T>& a) {
   constexpr bool FUSED = MODE >= 3;
   constexpr int MINB = 2;
   const size_t smem = sizeof(OpSmem<T, MV_BY, FUSED>);
-  static bool configured = false;  // per instantiation
-  if (!configured) {
+  static PerDeviceOnce configured;  // per instantiation and device
+  configured.run([&] {
     HX_CUDA(cudaFuncSetAttribute(k_struct<T, MV_BY, MODE, MINB>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    configured = true;
-  }
+  });
   k_struct<T, MV_BY, MODE, MINB><<<mv_grid(a.g, a.kchunk), dim3(MV_BX, MV_BY), smem, s>>>(a);
   HX_CHECK_LAUNCH();
 }

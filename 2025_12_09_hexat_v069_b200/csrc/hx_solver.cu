@@ -16,14 +16,30 @@ int64_t& launch_counter() {
   return n;
 }
 
-int sm_count() {
-  static int n = 0;
-  if (n == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    if (n <= 0) n = 148;
+int current_device() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
   }
+  return dev;
+}
+
+int sm_count() {
+  static std::atomic<int> cache[64];  // 0: not yet queried
+  const int dev = current_device();
+  const bool tracked = dev >= 0 && dev < 64;
+  if (tracked) {
+    const int n = cache[dev].load(std::memory_order_relaxed);
+    if (n > 0) return n;
+  }
+  int n = 0;
+  if (dev < 0 || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return 148;  // not cached: the next call asks again
+  }
+  if (n <= 0) return 148;
+  if (tracked) cache[dev].store(n, std::memory_order_relaxed);
   return n;
 }
 

@@ -47,10 +47,10 @@ typedef enum hx_status {
 typedef enum hx_dtype { HX_F32 = 0, HX_F64 = 1 } hx_dtype;
 
 typedef enum hx_precision {
-  HX_PREC_FP64 = 0,      /* plain FP64 Jacobi-PCG */
-  HX_PREC_MIXED32 = 1,   /* FP32 PCG with FP64 reliable updates (true-residual
-                            replacement, FP64 dots, FP64 convergence test) */
-  HX_PREC_MIXED_BF16 = 2 /* as MIXED32 with the search direction stored in BF16 */
+  HX_PREC_FP64 = 0,     /* plain FP64 Jacobi-PCG */
+  HX_PREC_MIXED32 = 1   /* FP32 PCG with FP64 reliable updates (true-residual
+                           replacement, FP64 dots, FP64 convergence test);
+                           any other value returns HX_BAD_ARG */
 } hx_precision;
 
 typedef enum hx_preconditioner {
@@ -153,8 +153,9 @@ HX_API hx_status hx_apply_stiffness(hx_ctx *ctx, int32_t dtype, const void *x,
  * device, so a foreign allocation fails.  This entry point computes
  * y = K(f)x on the structured nx*ny*nz grid (no boundary conditions, no
  * shift, as hx_apply_stiffness) and *xKx = x.y (FP64, deterministic), all
- * arrays FP64 DEVICE pointers in grid numbering (8-byte aligned), on `stream` (a
- * cudaStream_t; NULL = default stream).  It allocates nothing: its scratch
+ * arrays FP64 DEVICE pointers in grid numbering (x 16-byte aligned; factor,
+ * y and xKx 8-byte aligned; a misaligned pointer returns HX_BAD_ARG before
+ * any GPU work), on `stream` (a cudaStream_t; NULL = default stream).  It allocates nothing: its scratch
  * (one partial sum per CTA plus a completion counter) lives in a static
  * device array of 256 + 8*HX_NOALLOC_MAX_BLOCKS bytes that every GPU
  * loading the library holds until exit.  Grids needing more than

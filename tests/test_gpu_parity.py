@@ -147,6 +147,11 @@ def test_solve_edge_cases(ctx, hx):
     fn[5] = np.nan
     _, r4 = ctx.solve(fn, fac, ok=(4,))
     assert r4.status == 4
+    # precision codes other than FP64 (0) and FP32-in-FP64 (1) are refused
+    _, r5 = ctx.solve(f, fac, precision=2, ok=(6,))
+    # a grid whose z-plane holds 3 x nodes >= 2^31 DOFs is refused by the
+    # host check (32-bit in-plane offsets), before anything is allocated
+    assert ctx.lib.hx_set_grid(ctx.h, 30000, 30000, 1, 1.0, 1.0, 1.0) == 6
 
 
 def test_solve_deterministic(ctx, hx):

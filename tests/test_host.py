@@ -37,7 +37,7 @@ def test_generate_mesh_layout(hx):
     nodes, el, dims = hx.mesh.generate_mesh(3, 2, 2)
     assert dims == (4, 3, 3)
     assert nodes.shape == (36, 3) and el.shape == (12, 8)
-    # node_index(i,j,k) = i + (j-1)nx + (k-1)nx ny (Mesh.jl:114-116), 1-based
+    # node_index(i,j,k) = i + (j-1)nx + (k-1)nx ny (Mesh.jl:13-15), 1-based
     assert hx.mesh.node_index(2, 3, 2, 4, 3) == 2 + 2 * 4 + 1 * 12
     assert list(nodes[hx.mesh.node_index(2, 3, 2, 4, 3) - 1]) == [1.0, 2.0, 1.0]
     # element 1 corners follow NAT_COORDS
@@ -98,3 +98,31 @@ def test_cantilever_and_mbb(hx):
     nodes, el, bc, f = hx.workloads.mbb_half_beam(12, 4, 4)
     assert bc[:, 0].sum() == 5 * 5 and bc[:, 1].sum() == 5 and bc[:, 2].sum() == 0
     assert f.sum() == pytest.approx(-1.0)
+
+
+def test_noalloc_rejects_bad_arguments_before_the_device(hx):
+    """hx_apply_stiffness_noalloc checks its arguments before any CUDA call:
+    misaligned pointers and grids beyond the kernels' index range return
+    HX_BAD_ARG (6).  Run where no GPU is present, so the pointers (host
+    buffers) can never reach a kernel even if a check were missing; on a GPU
+    machine the device-pointer form of this test runs with the GPU tests."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present: covered by the no-alloc GPU test")
+    L = importlib.import_module("2025_12_09_hexat_v069_b200._lib")
+    lib = L.load()
+    buf = np.zeros(64, np.float64)
+    p = buf.ctypes.data
+    assert p % 16 == 0
+    good = (p, p + 128, p + 256, p + 384)
+    for k, off in ((0, 8), (1, 4), (2, 4), (3, 4)):
+        args = list(good)
+        args[k] += off
+        assert lib.hx_apply_stiffness_noalloc(2, 2, 2, 1.0, 1.0, 1.0, 0.3, *args, None) == 6
+    # 3 x nodes per z-plane at 2^31 and beyond: in-plane offsets would overflow
+    assert lib.hx_apply_stiffness_noalloc(30000, 30000, 1, 1.0, 1.0, 1.0, 0.3, *good, None) == 6
+    assert lib.hx_apply_stiffness_noalloc(1 << 20, 1, 1, 1.0, 1.0, 1.0, 0.3, *good, None) == 6
+    assert lib.hx_apply_stiffness_noalloc(0, 1, 1, 1.0, 1.0, 1.0, 0.3, *good, None) == 6
+    assert lib.hx_apply_stiffness_noalloc(2, 2, 2, 1.0, 1.0, 1.0, 0.5, *good, None) == 6
+    # valid arguments get as far as the device query, which fails without a GPU
+    assert lib.hx_apply_stiffness_noalloc(2, 2, 2, 1.0, 1.0, 1.0, 0.3, *good, None) in (7, 8)

@@ -62,4 +62,14 @@ def test_noalloc_rejects_oversized_grid(hx):
     st = L.hx_apply_stiffness_noalloc(100000, 10000, 1, 1.0, 1.0, 1.0, 0.3, buf.data_ptr(),
                                       buf.data_ptr(), buf.data_ptr(), buf.data_ptr(), None)
     assert st == 6  # HX_BAD_ARG
+    # a misaligned array is refused before any launch (it would otherwise be a
+    # misaligned-address fault in the caller's context): x needs 16 bytes,
+    # the others 8
+    p = buf.data_ptr()
+    assert p % 16 == 0
+    for k, off in ((0, 8), (1, 4), (2, 4), (3, 4)):
+        args = [p, p + 32, p + 64, p + 96]
+        args[k] += off
+        st = L.hx_apply_stiffness_noalloc(1, 1, 1, 1.0, 1.0, 1.0, 0.3, *args, None)
+        assert st == 6, k
     del x, fac
