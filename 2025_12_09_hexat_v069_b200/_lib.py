@@ -18,7 +18,7 @@ HX_F32, HX_F64 = 0, 1
 HX_PREC_FP64, HX_PREC_MIXED32 = 0, 1
 HX_PC_JACOBI, HX_PC_LEARNED, HX_PC_NONE = 0, 1, 2
 (HX_KERNEL_PCG_STEP_FP64, HX_KERNEL_PCG_UPDATE_FP64, HX_KERNEL_APPLY_FP64, HX_KERNEL_PCG_STEP_FP32,
- HX_KERNEL_FILTER_MATVEC, HX_KERNEL_CONV3, HX_KERNEL_NET_APPLY) = range(7)
+ HX_KERNEL_FILTER_MATVEC, HX_KERNEL_CONV3, HX_KERNEL_NET_APPLY, HX_KERNEL_FCG_STEP_FP32) = range(8)
 
 
 class SolveOpts(C.Structure):

@@ -511,6 +511,34 @@ hx_status solve_grid(hx_ctx* c, const double* f, const double* fac, double* u,
       total_iters += inner;
       R.refinements = c->h_state[0].iter;
     }
+    // The FP64 forms stop on the recursive residual, which over thousands of
+    // iterations can drift below the true one.  Outside the reference's
+    // retry semantics (which stop on the recursive residual, as
+    // GPUSolver.jl:508 does), convergence is confirmed on the FP64 true
+    // residual: while it is still above tol, the same method restarts from
+    // the current iterate (at most twice, within max_iter).  The mixed forms
+    // already judge convergence on the true residual.
+    for (int restart = 0; restart < 2 && !o.ref_retry && o.precision == HX_PREC_FP64 &&
+                          st.status == HX_ST_CONVERGED && !timed_out;
+         ++restart) {
+      if (true_residual(c, fac, b, u, shift) < o.tol) break;
+      hx_solve_opts oc = o;
+      oc.max_iter = o.max_iter - total_iters;
+      if (oc.max_iter <= 0) {
+        st.status = HX_ST_MAXITER;
+        break;
+      }
+      if (o.preconditioner == HX_PC_LEARNED) {
+        int fb = 0, its = 0;
+        st = solve_learned(c, fac, b, u, true, shift, oc, t0, &timed_out, &fb, &its);
+        total_iters += its;
+        R.fallback_used |= fb;
+      } else {
+        st = pcg_fp64(c, fac, b, u, true, shift, oc, t0, &timed_out);
+        total_iters += st.iter;
+      }
+      R.refinements += 1;
+    }
     last = st;
     R.attempts = attempt;
     if (st.status == HX_ST_CONVERGED || st.status == HX_ST_ZERO_RHS) {
@@ -686,8 +714,9 @@ hx_status time_kernel(hx_ctx* c, int kernel, int reps, double* avg_ms) {
         launch_matvec<double>(c->stream, 0, c->d_p.p, c->d_q.p, c->d_fac.p, c->d_nmask.p, g, c->K,
                               0.0, st, c->d_partials.p, nullptr);
       };
-  } else if (kernel == HX_KERNEL_PCG_STEP_FP32) {
-    HX_REQUIRE(ready(c->d_fac.n, ne) && ready(c->d_nmask.n, g.nodes()) && ready(c->d_minv.n, n),
+  } else if (kernel == HX_KERNEL_PCG_STEP_FP32 || kernel == HX_KERNEL_FCG_STEP_FP32) {
+    HX_REQUIRE(ready(c->d_fac.n, ne) && ready(c->d_nmask.n, g.nodes()) && ready(c->d_minv.n, n) &&
+                   ready(c->d_r.n, n),
                "run a solve first");
     float* f32 = c->d_fac32.ensure(ne);
     float* p32 = c->d_p32.ensure(n);
@@ -702,10 +731,22 @@ hx_status time_kernel(hx_ctx* c, int kernel, int reps, double* avg_ms) {
     launch_convert<float, double>(c->stream, r32, c->d_r.p, n);
     HX_CUDA(cudaMemsetAsync(x32, 0, n * sizeof(float), c->stream));
     const ElemCoef<float> K32 = to_float(c->K);
-    body = [&, f32, p32, p32b, q32, r32, m32, x32, K32] {
-      launch_pcg_step<float>(c->stream, p32, p32b, r32, m32, x32, q32, f32, c->d_nmask.p, g, K32,
-                             0.0f, st, c->d_partials.p);
-    };
+    if (kernel == HX_KERNEL_PCG_STEP_FP32) {
+      body = [&, f32, p32, p32b, q32, r32, m32, x32, K32] {
+        launch_pcg_step<float>(c->stream, p32, p32b, r32, m32, x32, q32, f32, c->d_nmask.p, g,
+                               K32, 0.0f, st, c->d_partials.p);
+      };
+    } else {
+      // the flexible-CG step with z = the converted residual: beta = 0 gives
+      // p = z != 0, so p.q > 0 and the state stays running; alpha_old = 0
+      // leaves x unchanged; z.r (aux[3]) only scales the new alpha
+      ts.aux[3] = 1.0;
+      put_state(c, 3, ts);
+      body = [&, f32, p32, p32b, q32, r32, x32, K32] {
+        launch_fcg_step<float>(c->stream, p32, p32b, r32, x32, q32, f32, c->d_nmask.p, g, K32,
+                               0.0f, st, c->d_partials.p);
+      };
+    }
   } else if (kernel == HX_KERNEL_FILTER_MATVEC) {
     HX_REQUIRE(c->f_used, "run a filter before timing its kernel");
     const FilterCoef F = make_filter_coef(c->fh[0], c->fh[1], c->fh[2], c->f_radius_last,

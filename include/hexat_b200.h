@@ -83,7 +83,10 @@ typedef struct hx_solve_opts {
 typedef struct hx_solve_report {
   int32_t status;       /* hx_status of the solve */
   int32_t iterations;   /* CG iterations (all inner iterations when mixed) */
-  int32_t refinements;  /* FP64 residual replacements (mixed) */
+  int32_t refinements;  /* mixed: FP64 residual replacements; FP64 forms:
+                           restarts from the iterate because the true
+                           residual was still above tol when the recursive
+                           one converged (ref_retry = 0 only) */
   int32_t attempts;     /* retry attempts used (ref_retry) */
   int32_t fallback_used;/* learned -> Jacobi fallback taken */
   int32_t zero_rhs;     /* 1: ||f_free|| == 0, u = 0 returned */
@@ -379,7 +382,9 @@ enum {
   HX_KERNEL_PCG_STEP_FP32 = 3,
   HX_KERNEL_FILTER_MATVEC = 4,
   HX_KERNEL_CONV3 = 5,           /* one 16 -> 16 BF16 conv3d layer on the node grid */
-  HX_KERNEL_NET_APPLY = 6        /* one learned-preconditioner application */
+  HX_KERNEL_NET_APPLY = 6,       /* one learned-preconditioner application */
+  HX_KERNEL_FCG_STEP_FP32 = 7    /* flexible-CG step of the mixed learned solve:
+                                    p = z + beta p_old, x update, K.p, p.q */
 };
 HX_API hx_status hx_time_kernel(hx_ctx *ctx, int32_t kernel, int32_t reps,
                                 double *avg_ms);

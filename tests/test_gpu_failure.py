@@ -1,0 +1,154 @@
+"""The reference solver's failure handling, src/Solvers/GPUSolver.jl:536-606,
+as the library runs it (hx_solve with ref_retry = 1, keep_best = 1): attempt
+retries with the shift escalated x10 after a hard failure and x5 after a
+stagnation in (5e-2, 0.1], "acceptable stagnation" below 5e-2 returning the
+best iterate, the divergence tests, and the global-best return when every
+attempt fails.
+
+Each case is driven from host-side inputs only (iteration limits, a NaN load,
+a huge initial guess, elements with negative stiffness factors that make K
+indefinite) and compared with tests.helpers.gpu_solver_reference, a numpy
+restatement of the same branch logic on the assembled matrix.  The inputs
+are chosen so that every decision lies far from its threshold (the margins
+are asserted on the numpy side), so rounding differences cannot flip one.
+Nothing here faults or hangs the GPU: every failure is a value the solver
+reads and reports.
+"""
+import numpy as np
+import pytest
+
+from tests.helpers import assemble, free_dofs, gpu_solver_reference, haar_ke
+
+pytestmark = pytest.mark.gpu
+
+DIMS = (10, 4, 4)
+OK, NOT_CONVERGED, STALLED, BREAKDOWN, NONFINITE, DIVERGED = 0, 1, 2, 3, 4, 9
+ANY = (OK, NOT_CONVERGED, STALLED, BREAKDOWN, NONFINITE, DIVERGED)
+
+
+def _problem(hx, seed=3, negative=0.0):
+    nodes, el, bc, f = hx.workloads.cantilever(*DIMS)
+    c0 = hx.mesh.connectivity0(el)
+    rng = np.random.default_rng(seed)
+    fac = hx.workloads.simp(rng.uniform(0.2, 1.0, c0.shape[0]))
+    if negative:
+        fac[rng.uniform(size=fac.shape) < 0.15] = -negative
+    K = assemble(c0, nodes.shape[0], haar_ke((1.0, 1.0, 1.0), 0.3), fac)
+    free = free_dofs(c0, nodes.shape[0], fac, bc)
+    return bc, f, fac, K, free
+
+
+def _solve(ctx, bc, f, fac, **kw):
+    ctx.set_grid(*DIMS)
+    ctx.set_material(1.0, 0.3)
+    ctx.set_bc(bc)
+    return ctx.solve(f, fac, ref_retry=1, keep_best=1, ok=ANY, **kw)
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def test_stagnation_below_1e2_returns_the_best_iterate(ctx, hx):
+    """max_iter = 135 leaves the best residual at 4.4e-3 (< 5e-2, < 1e-2):
+    accepted as stagnation on attempt 1 with the snapshot of the best
+    iterate; status HX_STALLED."""
+    bc, f, fac, K, free = _problem(hx)
+    want = gpu_solver_reference(K, free, f, 1e-12, 135, 1e-9)
+    assert want["status"] == "stalled" and want["attempts"] == 1
+    assert 2e-3 < want["best"] < 8e-3
+    u, rep = _solve(ctx, bc, f, fac, tol=1e-12, max_iter=135, shift_factor=1e-9)
+    assert rep.status == STALLED and rep.attempts == 1
+    assert np.any(u != 0) and _rel(u, want["u"]) < 1e-8
+
+
+def test_stagnation_between_1e2_and_5e2_returns_the_initial_guess(ctx, hx):
+    """max_iter = 127 leaves the best residual at 3.1e-2: accepted, but the
+    reference snapshots iterates only below 1e-2, so the iterate returned is
+    the attempt's initial guess -- zeros from a cold start, the (masked)
+    guess from a warm one."""
+    bc, f, fac, K, free = _problem(hx)
+    want = gpu_solver_reference(K, free, f, 1e-12, 127, 1e-9)
+    assert want["status"] == "stalled" and 1.5e-2 < want["best"] < 4.5e-2
+    u, rep = _solve(ctx, bc, f, fac, tol=1e-12, max_iter=127, shift_factor=1e-9)
+    assert rep.status == STALLED and rep.attempts == 1
+    assert np.all(u == 0)
+    u0 = np.random.default_rng(1).standard_normal(f.shape[0]) * 1e-9
+    want = gpu_solver_reference(K, free, f, 1e-12, 127, 1e-9, u0=u0)
+    assert want["status"] == "stalled" and 1.5e-2 < want["best"] < 4.5e-2
+    u, rep = _solve(ctx, bc, f, fac, u0=u0, tol=1e-12, max_iter=127, shift_factor=1e-9)
+    assert rep.status == STALLED and _rel(u, u0 * free) < 1e-12
+
+
+def test_stagnation_band_escalates_x5_and_returns_the_global_best(ctx, hx):
+    """max_iter = 110 leaves every attempt's best in (5e-2, 0.1]: the shift
+    factor grows x5 twice, all three attempts fail, and the global best (the
+    zero start: no iterate ever fell below 1e-2) is returned."""
+    bc, f, fac, K, free = _problem(hx)
+    want = gpu_solver_reference(K, free, f, 1e-12, 110, 1e-9)
+    assert want["status"] == "failed" and want["attempts"] == 3
+    assert 5.5e-2 < want["best"] < 9e-2
+    u, rep = _solve(ctx, bc, f, fac, tol=1e-12, max_iter=110, shift_factor=1e-9)
+    assert rep.status == NOT_CONVERGED and rep.attempts == 3
+    assert rep.shift == pytest.approx(want["shift"], rel=1e-12)
+    assert np.all(u == 0)
+
+
+def test_nonfinite_load_escalates_x10_and_returns_zeros(ctx, hx):
+    bc, f, fac, K, free = _problem(hx)
+    fn = f.copy()
+    fn[np.nonzero(free)[0][7]] = np.nan
+    u, rep = _solve(ctx, bc, fn, fac, tol=1e-8, max_iter=500, shift_factor=1e-6)
+    maxd = K.diagonal()[free > 0].max()
+    assert rep.status == NONFINITE and rep.attempts == 3
+    assert rep.shift == pytest.approx(1e-6 * 100.0 * maxd, rel=1e-12)
+    assert np.all(u == 0)
+
+
+@pytest.mark.parametrize("sf,attempts", [(0.05, 2), (0.01, 3)])
+def test_indefinite_breakdown_escalates_x10_until_it_converges(ctx, hx, sf, attempts):
+    """Elements with factor -0.3 make K indefinite (lowest eigenvalue -0.235
+    on the free DOFs, largest diagonal 0.896).  Attempts whose shift stays
+    below 0.235 break down (p.Ap <= 0); the x10 escalation reaches a shift
+    that makes K + sI definite and that attempt converges from zero."""
+    bc, f, fac, K, free = _problem(hx, seed=1, negative=0.3)
+    want = gpu_solver_reference(K, free, f, 1e-8, 2000, sf)
+    assert want["status"] == "converged" and want["attempts"] == attempts
+    u, rep = _solve(ctx, bc, f, fac, tol=1e-8, max_iter=2000, shift_factor=sf)
+    assert rep.status == OK and rep.attempts == attempts
+    assert rep.shift == pytest.approx(want["shift"], rel=1e-12)
+    assert _rel(u, want["u"]) < 1e-6
+
+
+def test_indefinite_every_attempt_fails(ctx, hx):
+    """Shift factor 1e-3: even x100 (shift 0.09) leaves K + sI indefinite;
+    all three attempts fail hard and zeros come back."""
+    bc, f, fac, K, free = _problem(hx, seed=1, negative=0.3)
+    want = gpu_solver_reference(K, free, f, 1e-8, 2000, 1e-3)
+    assert want["status"] == "failed" and want["attempts"] == 3
+    assert want["reason"] in ("breakdown", "diverged")
+    u, rep = _solve(ctx, bc, f, fac, tol=1e-8, max_iter=2000, shift_factor=1e-3)
+    assert rep.status in (BREAKDOWN, DIVERGED) and rep.attempts == 3
+    assert rep.shift == pytest.approx(want["shift"], rel=1e-12)
+    assert np.all(u == 0)
+
+
+def test_explosion_check_then_cold_retry(ctx, hx):
+    """A warm start 1e6 times too large puts the first residual far above
+    1000 ||b||: with divergence checks the attempt is abandoned as diverged
+    (explosion), the shift grows x10 and the cold-started attempt 2
+    converges.  Without the checks attempt 1 simply converges."""
+    bc, f, fac, K, free = _problem(hx)
+    u0 = np.random.default_rng(2).standard_normal(f.shape[0]) * 1e6
+    want = gpu_solver_reference(K, free, f, 1e-8, 3000, 1e-9, u0=u0)
+    assert want["status"] == "converged" and want["attempts"] == 2
+    u, rep = _solve(ctx, bc, f, fac, u0=u0, tol=1e-8, max_iter=3000, shift_factor=1e-9,
+                    divergence_checks=1)
+    assert rep.status == OK and rep.attempts == 2
+    assert rep.shift == pytest.approx(want["shift"], rel=1e-12)
+    assert _rel(u, want["u"]) < 1e-6
+    want = gpu_solver_reference(K, free, f, 1e-8, 3000, 1e-9, u0=u0, divergence_checks=False)
+    assert want["status"] == "converged" and want["attempts"] == 1
+    u, rep = _solve(ctx, bc, f, fac, u0=u0, tol=1e-8, max_iter=3000, shift_factor=1e-9,
+                    divergence_checks=0)
+    assert rep.status == OK and rep.attempts == 1
