@@ -46,6 +46,28 @@ class SolveReport(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
 
 
+class UpdateParams(C.Structure):
+    _fields_ = [
+        ("nelem", C.c_int64 * 3), ("h", C.c_double * 3), ("max_domain_dim", C.c_double),
+        ("filter_tolerance", C.c_double), ("stress_regularization_ratio", C.c_double),
+        ("filter_R_init_perc", C.c_double), ("filter_R_interm_perc", C.c_double),
+        ("filter_R_final_perc", C.c_double), ("filter_R_interm_iter_perc", C.c_double),
+        ("final_density_threshold", C.c_double), ("max_culling_ratio", C.c_double),
+        ("mode", C.c_int32), ("reserved0", C.c_int32), ("oc_volfrac", C.c_double),
+        ("oc_move", C.c_double), ("reserved", C.c_double * 4),
+    ]
+
+
+class UpdateResult(C.Structure):
+    _fields_ = [
+        ("max_change", C.c_double), ("R_length", C.c_double), ("current_threshold", C.c_double),
+        ("filter_time", C.c_double), ("filter_res", C.c_double), ("filter_iters", C.c_int32),
+        ("culled", C.c_int32), ("reserved", C.c_double * 2),
+    ]
+
+
+HX_UPDATE_STRESS_RATIO, HX_UPDATE_OC = 0, 1
+
 _vp, _i32, _i64, _dbl, _f32p, _i64p = C.c_void_p, C.c_int32, C.c_int64, C.c_double, C.c_void_p, C.c_void_p
 
 # name -> (restype, argtypes); the full exported surface of include/hexat_b200.h
@@ -72,6 +94,9 @@ PROTOTYPES = {
     "hx_solve_system_gpu": (_i32, [_vp, _f32p, _i64, _i64p, _i64, C.c_float, C.c_float, _f32p,
                                    _f32p, _f32p, _i32, _dbl, C.c_float, C.c_float, _f32p, _f32p,
                                    C.POINTER(_dbl), C.c_char_p, _i32]),
+    "hx_solve_system_grid": (_i32, [_vp, _i64, _i64, _i64, _dbl, _dbl, _dbl, C.c_float,
+                                    C.c_float, _f32p, _f32p, _f32p, _i32, _dbl, C.c_float,
+                                    C.c_float, _f32p, _f32p, C.POINTER(_dbl), C.c_char_p, _i32]),
     "hx_filter": (_i32, [_vp, _i32, _vp, _vp, _dbl, _i32, _dbl, _i32, C.POINTER(SolveReport)]),
     "hx_filter_device": (_i32, [_vp, _vp, _vp, _dbl, _i32, _dbl, _i32, C.POINTER(SolveReport)]),
     "hx_apply_gpu_filter": (_i32, [_vp, _f32p, _i64, _i64, _i64, _dbl, _dbl, _dbl, _dbl, _dbl,
@@ -102,6 +127,10 @@ PROTOTYPES = {
     "hx_element_energy": (_i32, [_vp, _i32, _vp, _vp]),
     "hx_oc_update": (_i32, [_vp, _i32, _vp, _vp, _vp, _dbl, _dbl, _vp, C.POINTER(_dbl),
                             C.POINTER(_i32)]),
+    "hx_default_update_params": (None, [C.POINTER(UpdateParams)]),
+    "hx_update_density": (_i32, [_vp, _vp, _vp, _vp, C.c_float, C.c_float, _i32, _i32, _vp,
+                                 C.c_float, C.c_float, C.POINTER(UpdateParams), _vp, _vp,
+                                 C.POINTER(UpdateResult)]),
 }
 
 _lib = None

@@ -4,6 +4,7 @@ error behaviour of the reference routines this library replaces.
   solve_system_gpu       src/Solvers/GPUSolver.jl:611-627
   apply_gpu_filter       src/Optimization/GPUHelmholtz.jl:344-376
   compute_stress_field   src/Core/Stress.jl:57-100
+  update_density         src/Optimization/TopOpt.jl:139-405
 
 Arrays follow the Julia layout (see mesh.py); each call runs on the GPU
 through libhexat_b200.so.
@@ -63,6 +64,35 @@ def solve_system_gpu(nodes, elements, E, nu, bc_indicator, f, density, *, max_it
     return x, rel.value, name.value.decode()
 
 
+def solve_system_grid(nelem, h, E, nu, bc_indicator, f, density, *, max_iter=40000, tol=1e-6,
+                      shift_factor=1.0e-6, min_stiffness_threshold=1.0e-3, u_guess=None,
+                      ctx=None):
+    """solve_system_gpu on the unpruned generate_mesh grid (nelem = (nx, ny,
+    nz), h = (dx, dy, dz)) with the pruning of src/Solvers/Solver.jl:60-91
+    done on the device -> (x_full::float32[3nN], final_rel_res, prec_name).
+    The result equals the reference's prune / solve / reconstruct path."""
+    ctx = ctx or default_context()
+    bc_cm = np.asfortranarray(bc_indicator, dtype=np.float32)
+    f32 = np.ascontiguousarray(f, dtype=np.float32)
+    d32 = np.ascontiguousarray(density, dtype=np.float32)
+    ug = None if u_guess is None else np.ascontiguousarray(u_guess, dtype=np.float32)
+    x = np.zeros(f32.shape[0], np.float32)
+    rel = C.c_double()
+    name = C.create_string_buffer(32)
+    st = ctx.lib.hx_solve_system_grid(ctx.h, int(nelem[0]), int(nelem[1]), int(nelem[2]),
+                                      float(h[0]), float(h[1]), float(h[2]), float(E), float(nu),
+                                      _p(bc_cm), _p(f32), _p(d32), int(max_iter), float(tol),
+                                      float(shift_factor), float(min_stiffness_threshold),
+                                      _p(ug), _p(x), C.byref(rel), name, 32)
+    if st not in (HX_OK, HX_STALLED, HX_NOT_CONVERGED, _lib.HX_BREAKDOWN, _lib.HX_DIVERGED,
+                  _lib.HX_NONFINITE):
+        ctx.check(st, "solve_system_grid")
+    if st not in (HX_OK, HX_STALLED):
+        import warnings
+        warnings.warn("All solver attempts failed. Returning best stagnated result.")
+    return x, rel.value, name.value.decode()
+
+
 def apply_gpu_filter(density, nelem_x, nelem_y, nelem_z, dx, dy, dz, radius, elements=None,
                      tol=1.0e-5, ref_compat=1, ctx=None):
     """GPUHelmholtz.apply_gpu_filter! -> (filtered, time_s, iters, res).
@@ -105,3 +135,66 @@ def compute_stress_field(nodes, elements, U, E, nu, density, ctx=None):
                                          _p(l1), _p(dr))
     ctx.check(st, "compute_stress_field")
     return pr.T, vm, vo.T, l1, dr.T
+
+
+def update_params(config, mode=None):
+    """hx_update_params from the reference's config Dict (the keys
+    update_density! reads, src/Optimization/TopOpt.jl:156-169,216-222,351-352,
+    with its defaults); mode "stress_ratio" (the reference, default) or "oc"
+    (config["optimization_parameters"]["update"], or the argument)."""
+    o = config.get("optimization_parameters", {})
+    g = config["geometry"]
+    sp = config.get("solver_parameters", {})
+    p = _lib.UpdateParams()
+    _lib.load().hx_default_update_params(C.byref(p))
+    p.nelem[:] = [int(g["nElem_x_computed"]), int(g["nElem_y_computed"]),
+                  int(g["nElem_z_computed"])]
+    p.h[:] = [float(g["dx_computed"]), float(g["dy_computed"]), float(g["dz_computed"])]
+    p.max_domain_dim = float(g["max_domain_dim"])
+    p.filter_tolerance = float(sp.get("filter_tolerance", 1.0e-5))
+    p.stress_regularization_ratio = float(o.get("stress_regularization_ratio", 0.0))
+    p.filter_R_init_perc = float(o.get("filter_R_init_perc", 0.0))
+    p.filter_R_interm_perc = float(o.get("filter_R_interm_perc", 0.0))
+    p.filter_R_final_perc = float(o.get("filter_R_final_perc", 0.0))
+    p.filter_R_interm_iter_perc = float(o.get("filter_R_interm_iter_perc", 50.0))
+    p.final_density_threshold = float(o.get("final_density_threshold", 0.95))
+    p.max_culling_ratio = float(o.get("max_culling_ratio", 0.1))
+    mode = mode or o.get("update", "stress_ratio")
+    if mode not in ("stress_ratio", "oc"):
+        raise ValueError(f"unknown update mode {mode!r}")
+    p.mode = _lib.HX_UPDATE_OC if mode == "oc" else _lib.HX_UPDATE_STRESS_RATIO
+    p.oc_volfrac = float(o.get("volume_fraction", 0.3))
+    p.oc_move = float(o.get("move_limit", 0.2))
+    return p
+
+
+def update_density(density, l1_stress_norm_field, protected_elements_mask, E,
+                   l1_stress_allowable, iter, number_of_iterations, original_density,
+                   min_density, max_density, config, elements=None, is_annealing=False, *,
+                   dc=None, filtered_out=None, ctx=None):
+    """TopologyOptimization.update_density! -> (max_change, R_length,
+    current_threshold, filter_time, filter_iters, filter_res).
+
+    `density` (and `l1_stress_norm_field`, when stress regularisation is on)
+    are float32 arrays updated in place, as the Julia vectors are; `elements`
+    and `is_annealing` are accepted for signature parity (the update runs on
+    the structured grid the config names, as the reference's filter does).
+    With config["optimization_parameters"]["update"] == "oc" the OC step
+    runs instead, on the sensitivities `dc`."""
+    ctx = ctx or default_context()
+    for name, a in (("density", density), ("l1_stress_norm_field", l1_stress_norm_field)):
+        if not (isinstance(a, np.ndarray) and a.dtype == np.float32 and a.flags.c_contiguous):
+            raise TypeError(f"{name} must be a contiguous float32 array (updated in place)")
+    prot = np.ascontiguousarray(np.asarray(protected_elements_mask, dtype=bool), dtype=np.uint8)
+    orig = np.ascontiguousarray(original_density, dtype=np.float32)
+    dcv = None if dc is None else np.ascontiguousarray(dc, dtype=np.float32)
+    p = update_params(config)
+    res = _lib.UpdateResult()
+    st = ctx.lib.hx_update_density(ctx.h, _p(density), _p(l1_stress_norm_field), _p(prot),
+                                   float(E), float(l1_stress_allowable), int(iter),
+                                   int(number_of_iterations), _p(orig), float(min_density),
+                                   float(max_density), C.byref(p), _p(dcv), _p(filtered_out),
+                                   C.byref(res))
+    ctx.check(st, "update_density")
+    return (res.max_change, res.R_length, res.current_threshold, res.filter_time,
+            res.filter_iters, res.filter_res)

@@ -492,7 +492,8 @@ HX_API hx_status hx_solve_device(hx_ctx* c, const double* f, const double* fac, 
   return guard(c, [&] {
     need_mesh(c);
     HX_REQUIRE(f && fac && u, "null argument");
-    // the vector kernels access u two doubles at a time
+    // the vector kernels access u two doubles at a time, the operator stages
+    // it in 16-byte chunks
     HX_REQUIRE(((uintptr_t)u & 15u) == 0, "u_dev must be 16-byte aligned");
     hx_solve_opts o = sanitize(opts);
     const int64_t l0 = hx::launch_counter();
@@ -578,6 +579,65 @@ HX_API hx_status hx_solve_system_gpu(hx_ctx* c, const float* nodes, int64_t nN,
     }
     // The reference warns and returns its best iterate when every attempt
     // fails; the status carries that outcome here.
+    return s;
+  });
+}
+
+HX_API hx_status hx_solve_system_grid(hx_ctx* c, int64_t nx, int64_t ny, int64_t nz, double dx,
+                                      double dy, double dz, float E, float nu,
+                                      const float* bc_indicator, const float* f,
+                                      const float* density, int32_t max_iter, double tol,
+                                      float shift_factor, float min_stiffness_threshold,
+                                      const float* u_guess, float* x_full,
+                                      double* final_rel_res, char* prec_name,
+                                      int32_t prec_name_cap) {
+  return guard(c, [&] {
+    HX_REQUIRE(bc_indicator && f && density && x_full, "null argument");
+    HX_REQUIRE(E > 0 && nu > -1 && nu < 0.5, "bad material");
+    set_grid_impl(c, nx, ny, nz, dx, dy, dz);
+    c->E = E;
+    c->nu = nu;
+    c->K = hx::make_elem_coef(c->h[0], c->h[1], c->h[2], nu);
+    hx::ensure_workspace(c);
+    const int64_t nn = c->g.nodes(), ne = c->g.elems(), n = c->g.dofs();
+    // every per-element and per-node step on the device: the host only copies
+    float* st = (float*)c->d_stage.ensure(std::max<int64_t>(3 * nn, ne) * sizeof(float));
+    HX_CUDA(cudaMemcpyAsync(st, bc_indicator, 3 * nn * sizeof(float), cudaMemcpyHostToDevice,
+                            c->stream));
+    hx::launch_bc_bits(c->stream, st, c->d_bcfree.ensure(nn), nn);
+    c->bc_dirty = false;  // the device mask is current; the host copy is not used
+    double* dfac = c->d_fac.ensure(ne);
+    HX_CUDA(cudaMemcpyAsync(st, density, ne * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    hx::launch_threshold_factor(c->stream, st, min_stiffness_threshold, E, dfac, ne);
+    double* df = c->d_f.ensure(n);
+    double* du = c->d_x.ensure(n);
+    HX_CUDA(cudaMemcpyAsync(st, f, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    hx::launch_convert<double, float>(c->stream, df, st, n);
+    if (u_guess) {
+      HX_CUDA(cudaMemcpyAsync(st, u_guess, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+      hx::launch_convert<double, float>(c->stream, du, st, n);
+    }
+    hx_solve_opts o;
+    hx_default_opts(&o);
+    o.tol = tol;
+    o.max_iter = max_iter;
+    o.shift_factor = shift_factor;
+    o.warm_start = u_guess != nullptr;
+    o.ref_retry = 1;
+    o.keep_best = 1;
+    o.divergence_checks = 1;
+    hx_solve_report R{};
+    hx_status s = hx::solve_grid(c, df, dfac, du, o, &R);
+    float* so = (float*)c->d_stage.ensure(n * sizeof(float));
+    hx::launch_convert<float, double>(c->stream, so, du, n);
+    HX_CUDA(cudaMemcpyAsync(x_full, so, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    HX_CUDA(cudaStreamSynchronize(c->stream));
+    if (final_rel_res) *final_rel_res = R.rel_res;
+    if (prec_name && prec_name_cap > 0) {
+      const char* nm = R.zero_rhs ? "None" : "Jacobi";
+      std::strncpy(prec_name, nm, (size_t)prec_name_cap - 1);
+      prec_name[prec_name_cap - 1] = '\0';
+    }
     return s;
   });
 }
@@ -795,6 +855,31 @@ HX_API hx_status hx_oc_update(hx_ctx* c, int32_t dt, const void* x, const void* 
   });
 }
 
+HX_API void hx_default_update_params(hx_update_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->h[0] = p->h[1] = p->h[2] = 1.0;
+  p->filter_tolerance = 1e-5;             // src/Optimization/TopOpt.jl:169
+  p->filter_R_interm_iter_perc = 50.0;    // :220
+  p->final_density_threshold = 0.95;      // :351
+  p->max_culling_ratio = 0.1;             // :352
+  p->mode = HX_UPDATE_STRESS_RATIO;
+  p->oc_volfrac = 0.3;
+  p->oc_move = 0.2;
+}
+
+HX_API hx_status hx_update_density(hx_ctx* c, float* density, float* l1,
+                                   const uint8_t* prot, float E, float allow, int32_t iter,
+                                   int32_t n_iter, const float* orig, float min_d, float max_d,
+                                   const hx_update_params* params, const float* dc,
+                                   float* filtered_out, hx_update_result* result) {
+  return guard(c, [&] {
+    HX_REQUIRE(params != nullptr, "params is null");
+    return hx::update_density(c, density, l1, prot, E, allow, iter, n_iter, orig, min_d, max_d,
+                              *params, dc, filtered_out, result);
+  });
+}
+
 // ---- device-resident pieces of the optimisation loop (grid numbering) ----
 static void need_grid_numbering(hx_ctx* c) {
   need_mesh(c);
@@ -967,6 +1052,8 @@ HX_API hx_status hx_residual_device(hx_ctx* c, const double* f, const double* fa
   return guard(c, [&] {
     need_mesh(c);
     HX_REQUIRE(f && fac && x && r, "null argument");
+    // the operator stages x in 16-byte chunks
+    HX_REQUIRE(((uintptr_t)x & 15u) == 0, "x_dev must be 16-byte aligned");
     hx::ensure_workspace(c);
     if (c->bc_dirty) hx::upload_bc(c);
     const int64_t n = c->g.dofs();

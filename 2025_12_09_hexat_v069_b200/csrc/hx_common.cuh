@@ -354,12 +354,13 @@ class PerDeviceOnce {
 };
 
 // Largest grids the structured kernels index: nodes per axis below 2^20, a
-// node plane's DOFs (3 * nxn * nyn) below 2^31 (in-plane offsets are 32-bit)
-// and all DOFs below 2^40.  True when nx x ny x nz elements fit.
+// node plane's DOFs plus a margin of 16 node rows (3 * nxn * (nyn + 16),
+// the staged halo rows of a CTA) below 2^31, since in-plane offsets are
+// 32-bit, and all DOFs below 2^40.  True when nx x ny x nz elements fit.
 inline bool grid_extent_ok(int64_t nx, int64_t ny, int64_t nz) {
   if (nx < 1 || ny < 1 || nz < 1) return false;
   if (nx >= (1 << 20) || ny >= (1 << 20) || nz >= (1 << 20)) return false;
-  if (3 * (nx + 1) * (ny + 1) >= (int64_t(1) << 31)) return false;
+  if (3 * (nx + 1) * (ny + 1 + 16) >= (int64_t(1) << 31)) return false;
   return 3 * (nx + 1) * (ny + 1) * (nz + 1) < (int64_t(1) << 40);
 }
 

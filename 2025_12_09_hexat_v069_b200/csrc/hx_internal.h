@@ -116,6 +116,11 @@ void launch_ir_correct(cudaStream_t s, double* x, const float* d32, int64_t n, c
 template <typename TD, typename TS>
 void launch_convert(cudaStream_t s, TD* dst, const TS* src, int64_t n);
 void launch_fill_zero(cudaStream_t s, void* p, size_t bytes);
+// fac = density >= thr ? E * density : 0 (Float32 product, as the reference)
+void launch_threshold_factor(cudaStream_t s, const float* dens, float thr, float E, double* fac,
+                             int64_t n);
+// free-DOF bits per node from a column-major nN x 3 bc_indicator
+void launch_bc_bits(cudaStream_t s, const float* bc, uint8_t* free_bits, int64_t nn);
 // r = a - b
 void launch_axpby(cudaStream_t s, double* r, const double* a, const double* b, int64_t n);
 
@@ -203,6 +208,14 @@ struct hx_ctx {
   bool f_used = false;
 
   int64_t launches = 0;  // kernels launched on behalf of this context
+
+  // density update (hx_update.cu): Float32 fields, FP64 filter buffers
+  struct Update {
+    hx::DevBuf<float> dens, l1, orig, dc, fout;
+    hx::DevBuf<uint8_t> prot;
+    hx::DevBuf<double> a, b, c, d;
+    hx::DevBuf<unsigned int> hist;
+  } upd;
 
   // convolutional preconditioner networks (see hx_net.cu)
   struct Net {

@@ -58,6 +58,14 @@ hx_status solve_grid(hx_ctx* c, const double* f, const double* fac, double* u,
 hx_status filter_grid(hx_ctx* c, const Grid& g, const double h[3], const double* rho, double* out,
                       double radius, int ref_compat, double tol, int max_iter,
                       hx_solve_report* rep);
+// update_density! of the reference (or the OC step) on Float32 host arrays
+// (hx_update.cu); see hx_update_density.
+hx_status update_density(hx_ctx* c, float* density, float* l1, const uint8_t* prot, float E,
+                         float allow, int it, int n_iter, const float* orig, float min_d,
+                         float max_d, const hx_update_params& p, const float* dc,
+                         float* filtered_out, hx_update_result* res);
+void update_radius_schedule(const hx_update_params& p, int it, int n_iter, double* R_length,
+                            double* R_effective);
 // Average time of `reps` launches of one kernel on the last solve's buffers.
 hx_status time_kernel(hx_ctx* c, int kernel, int reps, double* avg_ms);
 }  // namespace hx

@@ -460,6 +460,43 @@ void launch_axpby(cudaStream_t s, double* r, const double* a, const double* b, i
   HX_CHECK_LAUNCH();
 }
 
+// Device-side pruning of the reference's solve entry (src/Solvers/Solver.jl:
+// 60-91 with src/Mesh/MeshPruner.jl:18-112): element factor E * density
+// where density >= thr (GPUSolver.jl:128,147), else 0; nodes left without
+// stiffness are then held at 0 by the node mask, which is what the
+// reference's prune-solve-reconstruct returns for them.
+__global__ void k_threshold_factor(const float* __restrict__ dens, float thr, float E,
+                                   double* __restrict__ fac, int64_t n) {
+  for (int64_t e = gtid(); e < n; e += gstride()) {
+    const float d = dens[e];
+    fac[e] = d >= thr ? (double)(E * d) : 0.0;
+  }
+}
+
+// Free-DOF bits per node from the reference's bc_indicator (nN x 3 Float32,
+// column-major, > 0 = fixed; src/Core/Boundary.jl:135-160).
+__global__ void k_bc_bits(const float* __restrict__ bc, uint8_t* __restrict__ free_bits,
+                          int64_t nn) {
+  for (int64_t i = gtid(); i < nn; i += gstride()) {
+    unsigned m = 0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      if (!(bc[d * nn + i] > 0.0f)) m |= 1u << d;
+    free_bits[i] = (uint8_t)m;
+  }
+}
+
+void launch_threshold_factor(cudaStream_t s, const float* dens, float thr, float E, double* fac,
+                             int64_t n) {
+  k_threshold_factor<<<vec_blocks(n), VEC_THREADS, 0, s>>>(dens, thr, E, fac, n);
+  HX_CHECK_LAUNCH();
+}
+
+void launch_bc_bits(cudaStream_t s, const float* bc, uint8_t* free_bits, int64_t nn) {
+  k_bc_bits<<<vec_blocks(nn), VEC_THREADS, 0, s>>>(bc, free_bits, nn);
+  HX_CHECK_LAUNCH();
+}
+
 void launch_fill_zero(cudaStream_t s, void* p, size_t bytes) {
   HX_CUDA(cudaMemsetAsync(p, 0, bytes, s));
 }

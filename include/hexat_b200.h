@@ -209,6 +209,22 @@ HX_API hx_status hx_solve_system_gpu(
     float *x_full, double *final_rel_res, char *prec_name,
     int32_t prec_name_cap);
 
+/* The same solve on the unpruned structured mesh of generate_mesh
+ * (nx*ny*nz elements of dx*dy*dz; src/Mesh/Mesh.jl:23-60), given by its
+ * dimensions instead of node and element arrays, with the reference's
+ * pruning done on the device: elements with density < min_stiffness_threshold
+ * get zero stiffness and nodes left without stiffness are held at 0 -- the
+ * x_full the reference's prune_system / solve / reconstruct_full_solution
+ * returns (src/Solvers/Solver.jl:60-91,158-160, src/Mesh/MeshPruner.jl).
+ * The host only copies: no per-element or per-node host work.  Arrays in the
+ * grid's numbering (generate_mesh's own). */
+HX_API hx_status hx_solve_system_grid(
+    hx_ctx *ctx, int64_t nx, int64_t ny, int64_t nz, double dx, double dy,
+    double dz, float E, float nu, const float *bc_indicator, const float *f,
+    const float *density, int32_t max_iter, double tol, float shift_factor,
+    float min_stiffness_threshold, const float *u_guess, float *x_full,
+    double *final_rel_res, char *prec_name, int32_t prec_name_cap);
+
 /* ---- Helmholtz PDE density filter ------------------------------------------
  * (r^2 K + M) x = T rho with T the lumped vol/8 scatter, Jacobi-CG (at most
  * max_iter iterations, residual tested every 10), element value = mean of
@@ -281,6 +297,66 @@ HX_API hx_status hx_oc_update(hx_ctx *ctx, int32_t dtype, const void *x,
                               const void *dc, const void *dv, double volfrac,
                               double move, void *xnew, double *lambda,
                               int32_t *steps);
+
+/* ---- density update -----------------------------------------------------------------
+ * Drop-in for TopologyOptimization.update_density!(density, l1_stress_norm_field,
+ * protected_elements_mask, E, l1_stress_allowable, iter, number_of_iterations,
+ * original_density, min_density, max_density, config, elements, is_annealing)
+ * -> (max_change, R_length, current_threshold, filter_time, filter_iters,
+ * filter_res), src/Optimization/TopOpt.jl:139-405, on the structured grid of
+ * params->nelem (elements in grid order, as the reference's density vector).
+ * Float32 host arrays of n = nx*ny*nz entries, updated in place like the
+ * Julia vectors: density (and l1_stress when stress regularisation is on);
+ * protected_mask is one byte per element (non-zero = protected).
+ * mode HX_UPDATE_STRESS_RATIO (the reference): optional stress
+ * regularisation filter, radius schedule with the 1.2 h guard and R/2.5,
+ * proposal clamp((l1/allowable)/E, min, max) (original density where
+ * protected), Helmholtz filter with the reference element, clamp, culling of
+ * at most floor(active * max_culling_ratio) of the weakest elements below
+ * threshold * iter / number_of_iterations (ties in element order), protected
+ * re-enforce; every per-element step in the reference's Float32 arithmetic,
+ * the filters in FP64 (radius, sizes and tolerance rounded to Float32 as the
+ * reference's filter workspace does, at most 200 iterations).
+ * mode HX_UPDATE_OC (no reference counterpart): dc (the compliance
+ * sensitivities, required) is Helmholtz-filtered with the same radius and
+ * the density takes one optimality-criteria step (bisection on the volume
+ * multiplier, unit volumes, oc_volfrac, oc_move), then the clamp and the
+ * protected re-enforce; no culling (current_threshold 0).
+ * filtered_out (optional, n floats) receives the filtered proposal (or the
+ * filtered dc), rounded to Float32. */
+typedef enum hx_update_mode { HX_UPDATE_STRESS_RATIO = 0, HX_UPDATE_OC = 1 } hx_update_mode;
+typedef struct hx_update_params {
+  int64_t nelem[3];     /* config geometry nElem_x/y/z_computed */
+  double h[3];          /* dx/dy/dz_computed (used as Float32) */
+  double max_domain_dim;
+  double filter_tolerance;            /* solver_parameters (default 1e-5) */
+  double stress_regularization_ratio; /* optimization_parameters (default 0) */
+  double filter_R_init_perc;          /* (default 0) */
+  double filter_R_interm_perc;        /* (default 0) */
+  double filter_R_final_perc;         /* (default 0) */
+  double filter_R_interm_iter_perc;   /* (default 50) */
+  double final_density_threshold;     /* (default 0.95) */
+  double max_culling_ratio;           /* (default 0.1) */
+  int32_t mode;                       /* hx_update_mode */
+  int32_t reserved0;
+  double oc_volfrac, oc_move;         /* HX_UPDATE_OC only */
+  double reserved[4];
+} hx_update_params;
+typedef struct hx_update_result {
+  double max_change, R_length, current_threshold, filter_time, filter_res;
+  int32_t filter_iters;
+  int32_t culled;       /* elements set to min_density by the culling */
+  double reserved[2];
+} hx_update_result;
+HX_API void hx_default_update_params(hx_update_params *params);
+HX_API hx_status hx_update_density(hx_ctx *ctx, float *density, float *l1_stress,
+                                   const uint8_t *protected_mask, float E,
+                                   float l1_stress_allowable, int32_t iter,
+                                   int32_t number_of_iterations,
+                                   const float *original_density, float min_density,
+                                   float max_density, const hx_update_params *params,
+                                   const float *dc, float *filtered_out,
+                                   hx_update_result *result);
 
 /* ---- device-resident optimisation loop pieces ---------------------------------------
  * No reference counterpart (the OC loop is the published method).  FP64

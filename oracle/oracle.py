@@ -199,3 +199,118 @@ def topopt_oc_loop(conn0, n_nodes, dims, bc_indicator, f, volfrac, radius, n_ite
                                      filter_tol, filter_max_iter)
         x, _, _ = oc_update(x, dcf, np.ones(ne), volfrac, move)
     return np.array(hist), x, rho
+
+
+def structured_conn0(nx, ny, nz):
+    """0-based Hex8 connectivity of generate_mesh (src/Mesh/Mesh.jl:44-55):
+    element e = i + nx*(j + ny*k), corners in NAT_COORDS order."""
+    nnx, nny = nx + 1, ny + 1
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    n0 = (i + nnx * (j + nny * k)).ravel()
+    off = [0, 1, 1 + nnx, nnx, nnx * nny, 1 + nnx * nny, 1 + nnx + nnx * nny, nnx + nnx * nny]
+    return (n0[:, None] + np.array(off)[None, :]).astype(np.int32)
+
+
+def radius_schedule(it, n_iter, h, max_domain_dim, R_init_perc=0.0, R_interm_perc=0.0,
+                    R_final_perc=0.0, R_interm_iter_perc=50.0):
+    """Filter radius of update_density!, src/Optimization/TopOpt.jl:216-255,
+    with Julia's types: the percentages and element sizes are Float32,
+    max_domain_dim is taken as Float64 (a YAML number), so the lengths are
+    Float64; t, the guard 1.2 * mean element size and the divisor 2.5 are
+    Float32.  Returns (R_length, R_effective) as Python floats."""
+    f32 = np.float32
+    dx, dy, dz = (f32(v) for v in h)
+    avg = (dx + dy + dz) / f32(3.0)
+    ri = f32(R_init_perc) / f32(100.0)
+    rm = f32(R_interm_perc) / f32(100.0)
+    rf = f32(R_final_perc) / f32(100.0)
+    rip = f32(R_interm_iter_perc) / f32(100.0)
+    Ri, Rm, Rf = (float(v) * float(max_domain_dim) for v in (ri, rm, rf))
+    iter_interm = max(1, int(np.rint(rip * f32(n_iter))))
+    calc = min(it, n_iter)
+    if calc <= iter_interm:
+        t = f32(calc - 1) / f32(iter_interm - 1) if iter_interm > 1 else f32(0.0)
+        R = Ri * float(f32(1.0) - t) + Rm * float(t)
+    else:
+        t = (f32(calc - iter_interm) / f32(n_iter - iter_interm)) if n_iter > iter_interm \
+            else f32(0.0)
+        R = Rm * float(f32(1.0) - t) + Rf * float(t)
+    safe = f32(1.2) * avg
+    if R < float(safe):
+        return float(safe), float(safe / f32(2.5))
+    return R, R / 2.5
+
+
+def update_density(density, l1, protected, E, allowable, it, n_iter, original, min_d, max_d,
+                   dims, h, max_domain_dim, filter_tol=1e-5, stress_regularization_ratio=0.0,
+                   R_init_perc=0.0, R_interm_perc=0.0, R_final_perc=0.0,
+                   R_interm_iter_perc=50.0, final_density_threshold=0.95,
+                   max_culling_ratio=0.1, filtered=None):
+    """Restatement of TopologyOptimization.update_density!
+    (src/Optimization/TopOpt.jl:139-405) in float32 numpy on the structured
+    grid `dims` (elements in grid order):
+      * optional stress regularisation: the L1 stress field filtered with
+        radius ratio * mean element size (:176-211);
+      * radius schedule and guard (:216-255, radius_schedule);
+      * stress-ratio proposal clamp((l1 / allowable) / E, min, max), the
+        original density on protected elements (:260-271);
+      * Helmholtz filter of the proposal with the reference element
+        (ref_compat, GPUHelmholtz.apply_gpu_filter! at :286), radius rounded
+        to Float32 as the filter workspace does, at most 200 iterations;
+      * clamp and the largest change over unprotected elements (:327-343);
+      * culling below threshold * iter / n_iter (the final threshold once iter
+        exceeds n_iter), at most floor(active * max_culling_ratio) elements,
+        the weakest first, ties in element order (:350-395; Julia's default
+        sort is stable);
+      * protected elements re-enforced (:398-402).
+    `filtered` (float32), when given, replaces the filter's output, so the
+    rest can be compared bit for bit with a device run that reports its
+    filtered field.  Returns (density, l1, (max_change, R_length,
+    threshold, filter_iters, filter_res), filtered)."""
+    f32 = np.float32
+    nx, ny, nz = dims
+    dens = np.array(density, dtype=f32)
+    l1 = np.array(l1, dtype=f32)
+    orig = np.asarray(original, dtype=f32)
+    prot = np.asarray(protected, dtype=bool)
+    min_d, max_d, E, allowable = f32(min_d), f32(max_d), f32(E), f32(allowable)
+    conn0 = None
+    dxf, dyf, dzf = (f32(v) for v in h)
+    avg = (dxf + dyf + dzf) / f32(3.0)
+    nn = (nx + 1) * (ny + 1) * (nz + 1)
+    ratio = f32(stress_regularization_ratio)
+    if ratio > 1e-6:
+        conn0 = structured_conn0(nx, ny, nz)
+        r = float(f32(ratio * avg))
+        s, _, _ = helmholtz_filter(conn0, nn, l1.astype(np.float64), float(dxf), float(dyf),
+                                   float(dzf), r, 1, float(f32(filter_tol)), 200)
+        l1 = s.astype(f32)
+    R_length, R_eff = radius_schedule(it, n_iter, h, max_domain_dim, R_init_perc, R_interm_perc,
+                                      R_final_perc, R_interm_iter_perc)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        val = (l1 / allowable) / E
+    prop = np.where(prot, orig, np.clip(val, min_d, max_d)).astype(f32)
+    iters, res = 0, 0.0
+    if filtered is None:
+        if conn0 is None:
+            conn0 = structured_conn0(nx, ny, nz)
+        fo, iters, res = helmholtz_filter(conn0, nn, prop.astype(np.float64), float(dxf),
+                                          float(dyf), float(dzf), float(f32(R_eff)), 1,
+                                          float(f32(filter_tol)), 200)
+        filtered = fo.astype(f32)
+    filtered = np.asarray(filtered, dtype=f32)
+    new = np.clip(filtered, min_d, max_d).astype(f32)
+    change = np.abs(new - dens)
+    max_change = float(change[~prot].max()) if np.any(~prot) else 0.0
+    dens = np.where(prot, dens, new)
+    thr = f32(final_density_threshold) if it > n_iter else \
+        f32(final_density_threshold) * (f32(it) / f32(n_iter))
+    active = int(np.count_nonzero(~prot & (dens > min_d)) + np.count_nonzero(prot & (orig > min_d)))
+    cand = np.nonzero(~prot & (dens > min_d) & (dens < thr))[0]
+    max_allowed = int(np.floor(f32(active) * f32(max_culling_ratio)))
+    if cand.size > max_allowed:
+        order = np.argsort(dens[cand], kind="stable")
+        cand = cand[order[:max_allowed]]
+    dens[cand] = min_d
+    dens[prot] = orig[prot]
+    return dens, l1, (max_change, R_length, float(thr), iters, res), filtered

@@ -321,3 +321,42 @@ def test_solve_system_gpu_pruned_mesh(ctx, hx, orc):
     uo_full = reconstruct_full_solution(uo, n2o, nodes.shape[0])
     assert rel < 1e-7
     assert np.abs(u_full - uo_full).max() <= 2e-5 * np.abs(uo_full).max()
+
+
+def test_solve_system_grid_device_pruning_matches_pruned_path(ctx, hx, orc):
+    """The unpruned grid plus min_stiffness_threshold, pruned on the device
+    (hx_solve_system_grid), against the reference's host path: prune_system
+    (src/Mesh/MeshPruner.jl:18-112), the solve on the pruned, renumbered mesh
+    (hx_solve_system_gpu, lattice embedding) and reconstruct_full_solution;
+    and both against the oracle's solve of the pruned mesh."""
+    from importlib import import_module
+    api = import_module("2025_12_09_hexat_v069_b200.api")
+    dims = (14, 6, 5)
+    nodes, el, bc, f = hx.workloads.cantilever(*dims)
+    rng = np.random.default_rng(17)
+    dens = rng.uniform(0.3, 1.0, el.shape[0]).astype(np.float32)
+    i = np.arange(el.shape[0]) % dims[0]
+    hole = (i > 4) & (i < 9) & (rng.uniform(size=el.shape[0]) < 0.7)
+    dens[hole] = 1e-3
+    thr = np.float32(1e-3) * np.float32(1.01)
+    f32 = f.astype(np.float32)
+    xg, relg, name = api.solve_system_grid(dims, (1.0, 1.0, 1.0), 1.0, 0.3, bc, f32, dens,
+                                           tol=1e-7, shift_factor=0.0,
+                                           min_stiffness_threshold=thr, ctx=ctx)
+    assert name == "Jacobi" and relg < 1e-7
+    pn, pe, pbc, pf, pd, n2o = prune_system(nodes, el, dens, thr, bc, f32)
+    xp, relp, _ = api.solve_system_gpu(pn, pe, 1.0, 0.3, pbc, pf, pd, tol=1e-7,
+                                       shift_factor=0.0, min_stiffness_threshold=thr, ctx=ctx)
+    up = reconstruct_full_solution(xp, n2o, nodes.shape[0])
+    assert np.abs(xg - up).max() <= 1e-5 * np.abs(up).max()
+    # nodes outside the pruned mesh are exactly zero, as reconstruct returns
+    gone = np.ones(nodes.shape[0], bool)
+    gone[n2o] = False
+    assert np.all(xg.reshape(-1, 3)[gone] == 0)
+    c0 = hx.mesh.connectivity0(pe)
+    fac = pd.astype(np.float64)
+    free = orc.free_mask_from(pbc, orc.diagonal(c0, pn.shape[0], orc.canonical_ke(), fac))
+    uo, _, _, _ = orc.cg_solve(c0, pn.shape[0], orc.canonical_ke(), fac, free, pf * free,
+                               tol=1e-10)
+    uo_full = reconstruct_full_solution(uo, n2o, nodes.shape[0])
+    assert np.abs(xg - uo_full).max() <= 2e-5 * np.abs(uo_full).max()

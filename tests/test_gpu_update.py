@@ -1,0 +1,149 @@
+"""The reference's density update on the GPU (hx_update_density, the drop-in
+for TopologyOptimization.update_density!, src/Optimization/TopOpt.jl:139-405)
+against the oracle's float32 restatement (oracle.update_density).
+
+Every per-element step runs in the reference's Float32 arithmetic on both
+sides, so given the same filtered field the updated densities, the largest
+change, the radius and the threshold are compared bit for bit (the device
+reports its filtered field through filtered_out).  The filters themselves
+(FP64 CG on both sides, summed in different orders) agree to 1e-9 before the
+Float32 rounding, so the filtered fields are compared to 2 ulp.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+DIMS = (24, 10, 8)
+
+
+def _config(dims=DIMS, h=(1.0, 1.0, 1.0), **opt):
+    o = {"filter_R_init_perc": 8.0, "filter_R_interm_perc": 5.0, "filter_R_final_perc": 3.0}
+    o.update(opt)
+    return {"geometry": {"nElem_x_computed": dims[0], "nElem_y_computed": dims[1],
+                         "nElem_z_computed": dims[2], "dx_computed": h[0], "dy_computed": h[1],
+                         "dz_computed": h[2], "max_domain_dim": float(max(dims) * max(h))},
+            "optimization_parameters": o, "solver_parameters": {"filter_tolerance": 1e-5}}
+
+
+def _inputs(seed, n, protect=0.05):
+    rng = np.random.default_rng(seed)
+    dens = rng.uniform(0.05, 1.0, n).astype(np.float32)
+    l1 = rng.gamma(2.0, 0.4, n).astype(np.float32)
+    prot = rng.uniform(size=n) < protect
+    orig = rng.uniform(0.5, 1.0, n).astype(np.float32)
+    return dens, l1, prot, orig
+
+
+def _run(hx, ctx, cfg, dens, l1, prot, orig, it, n_iter, E=1.0, allow=1.0, min_d=1e-3,
+         max_d=1.0, dc=None):
+    from importlib import import_module
+    api = import_module(hx.__name__ + ".api")
+    d = dens.copy()
+    s = l1.copy()
+    filt = np.empty_like(d)
+    out = api.update_density(d, s, prot, E, allow, it, n_iter, orig, min_d, max_d, cfg, None,
+                             False, dc=dc, filtered_out=filt, ctx=ctx)
+    return d, s, filt, out
+
+
+def _oracle(orc, cfg, dens, l1, prot, orig, it, n_iter, filtered=None, E=1.0, allow=1.0,
+            min_d=1e-3, max_d=1.0):
+    g = cfg["geometry"]
+    o = cfg["optimization_parameters"]
+    return orc.update_density(
+        dens, l1, prot, E, allow, it, n_iter, orig, min_d, max_d,
+        (g["nElem_x_computed"], g["nElem_y_computed"], g["nElem_z_computed"]),
+        (g["dx_computed"], g["dy_computed"], g["dz_computed"]), g["max_domain_dim"],
+        filter_tol=cfg["solver_parameters"]["filter_tolerance"],
+        stress_regularization_ratio=o.get("stress_regularization_ratio", 0.0),
+        R_init_perc=o.get("filter_R_init_perc", 0.0),
+        R_interm_perc=o.get("filter_R_interm_perc", 0.0),
+        R_final_perc=o.get("filter_R_final_perc", 0.0),
+        R_interm_iter_perc=o.get("filter_R_interm_iter_perc", 50.0),
+        final_density_threshold=o.get("final_density_threshold", 0.95),
+        max_culling_ratio=o.get("max_culling_ratio", 0.1), filtered=filtered)
+
+
+def _ulp_close(a, b, ulps=2):
+    a = np.asarray(a, np.float32)
+    b = np.asarray(b, np.float32)
+    tol = ulps * np.spacing(np.maximum(np.abs(a), np.abs(b)))
+    return bool(np.all(np.abs(a.astype(np.float64) - b) <= tol))
+
+
+@pytest.mark.parametrize("it,n_iter", [(1, 40), (7, 40), (25, 40), (45, 40)])
+def test_stress_ratio_update_matches_oracle(ctx, hx, orc, it, n_iter):
+    n = int(np.prod(DIMS))
+    dens, l1, prot, orig = _inputs(it, n)
+    cfg = _config()
+    d, s, filt, out = _run(hx, ctx, cfg, dens, l1, prot, orig, it, n_iter)
+    # the filter against the oracle's (FP64 on both sides, then Float32)
+    _, _, _, fo = _oracle(orc, cfg, dens, l1, prot, orig, it, n_iter)
+    assert _ulp_close(filt, fo)
+    # everything after the filter, bit for bit, on the device's filtered field
+    do, so, (mc, R, thr, _, _), _ = _oracle(orc, cfg, dens, l1, prot, orig, it, n_iter,
+                                            filtered=filt)
+    assert np.array_equal(d, do)
+    assert np.array_equal(s, l1)  # no stress regularisation: untouched
+    assert out[0] == mc and out[1] == R and out[2] == thr
+    assert out[4] > 0 and out[4] % 10 == 0 and out[5] < 1e-5
+    assert np.array_equal(d[prot], orig[prot])
+
+
+def test_culling_cap_ties_in_element_order(ctx, hx, orc):
+    """A uniform stress field makes the filtered proposal (nearly) constant:
+    thousands of candidates share a few density values, more than the cap
+    allows, so the cut falls inside runs of equal values; the reference's
+    stable sort culls those ties in element order, and so must the device's
+    radix select."""
+    n = int(np.prod(DIMS))
+    dens = np.full(n, 0.6, np.float32)
+    l1 = np.full(n, 0.2, np.float32)
+    prot = np.zeros(n, bool)
+    prot[::97] = True
+    orig = np.full(n, 0.8, np.float32)
+    cfg = _config(max_culling_ratio=0.03)
+    d, _, filt, out = _run(hx, ctx, cfg, dens, l1, prot, orig, 40, 40)
+    vals, counts = np.unique(filt[~prot], return_counts=True)
+    assert counts.max() > 100  # ties, as intended
+    do, _, (mc, R, thr, _, _), _ = _oracle(orc, cfg, dens, l1, prot, orig, 40, 40, filtered=filt)
+    assert np.array_equal(d, do)
+    culled = np.count_nonzero((d == np.float32(1e-3)) & ~prot)
+    active = np.count_nonzero(~prot) + np.count_nonzero(prot)
+    assert culled == int(np.floor(np.float32(active) * np.float32(0.03)))
+
+
+def test_stress_regularisation_filters_the_l1_field_in_place(ctx, hx, orc):
+    n = int(np.prod(DIMS))
+    dens, l1, prot, orig = _inputs(3, n)
+    cfg = _config(stress_regularization_ratio=1.5)
+    d, s, filt, out = _run(hx, ctx, cfg, dens, l1, prot, orig, 10, 40)
+    _, so, _, _ = _oracle(orc, cfg, dens, l1, prot, orig, 10, 40)
+    assert not np.array_equal(s, l1) and _ulp_close(s, so)
+    # the rest of the update from the device's filtered field
+    cfg0 = _config(stress_regularization_ratio=0.0)
+    do, _, (mc, R, thr, _, _), _ = _oracle(orc, cfg0, dens, s, prot, orig, 10, 40, filtered=filt)
+    assert np.array_equal(d, do) and out[0] == mc and out[1] == R and out[2] == thr
+
+
+def test_oc_mode_matches_oracle(ctx, hx, orc):
+    n = int(np.prod(DIMS))
+    dens, _, prot, orig = _inputs(5, n)
+    rng = np.random.default_rng(6)
+    dc = (-rng.uniform(0.1, 2.0, n)).astype(np.float32)
+    cfg = _config(update="oc", volume_fraction=0.4, move_limit=0.2)
+    d, s, filt, out = _run(hx, ctx, cfg, dens, np.zeros(n, np.float32), prot, orig, 3, 40, dc=dc)
+    g = cfg["geometry"]
+    conn0 = orc.structured_conn0(*DIMS)
+    R, Reff = orc.radius_schedule(3, 40, (1.0, 1.0, 1.0), g["max_domain_dim"], 8.0, 5.0, 3.0)
+    fo, _, _ = orc.helmholtz_filter(conn0, (DIMS[0] + 1) * (DIMS[1] + 1) * (DIMS[2] + 1),
+                                    dc.astype(np.float64), 1.0, 1.0, 1.0,
+                                    float(np.float32(Reff)), 1, float(np.float32(1e-5)), 200)
+    assert _ulp_close(filt, fo.astype(np.float32))
+    # the OC bisection runs on the FP64 filtered sensitivities on both sides
+    xo, _, _ = orc.oc_update(dens.astype(np.float64), fo, np.ones(n), 0.4, 0.2)
+    want = np.clip(xo.astype(np.float32), np.float32(1e-3), np.float32(1.0))
+    want[prot] = orig[prot]
+    assert _ulp_close(d, want, ulps=1)
+    assert out[1] == R and out[2] == 0.0

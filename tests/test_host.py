@@ -21,6 +21,8 @@ def test_abi_struct_sizes(hx):
     # natural x86-64 alignment, identical for the C compiler and ctypes
     assert ctypes.sizeof(L.SolveOpts) == 96
     assert ctypes.sizeof(L.SolveReport) == 6 * 4 + 10 * 8
+    assert ctypes.sizeof(L.UpdateParams) == 176
+    assert ctypes.sizeof(L.UpdateResult) == 64
 
 
 def test_no_device_fails_loudly(hx):
@@ -126,3 +128,23 @@ def test_noalloc_rejects_bad_arguments_before_the_device(hx):
     assert lib.hx_apply_stiffness_noalloc(2, 2, 2, 1.0, 1.0, 1.0, 0.5, *good, None) == 6
     # valid arguments get as far as the device query, which fails without a GPU
     assert lib.hx_apply_stiffness_noalloc(2, 2, 2, 1.0, 1.0, 1.0, 0.3, *good, None) in (7, 8)
+
+
+def test_update_params_from_reference_config(hx):
+    """The config Dict keys update_density! reads (TopOpt.jl:156-169, 216-222,
+    351-352) and its defaults, packed for hx_update_density."""
+    api = importlib.import_module("2025_12_09_hexat_v069_b200.api")
+    cfg = {"geometry": {"nElem_x_computed": 60, "nElem_y_computed": 20, "nElem_z_computed": 20,
+                        "dx_computed": 1.0, "dy_computed": 1.0, "dz_computed": 1.0,
+                        "max_domain_dim": 60.0},
+           "optimization_parameters": {"filter_R_init_perc": 4.0, "max_culling_ratio": 0.05}}
+    p = api.update_params(cfg)
+    assert list(p.nelem) == [60, 20, 20] and p.max_domain_dim == 60.0
+    assert p.filter_R_init_perc == 4.0 and p.filter_R_interm_iter_perc == 50.0
+    assert p.final_density_threshold == 0.95 and p.max_culling_ratio == 0.05
+    assert p.filter_tolerance == 1e-5 and p.mode == 0
+    cfg["optimization_parameters"]["update"] = "oc"
+    assert api.update_params(cfg).mode == 1
+    cfg["optimization_parameters"]["update"] = "bogus"
+    with pytest.raises(ValueError):
+        api.update_params(cfg)
