@@ -97,6 +97,10 @@ PROTOTYPES = {
     "hx_solve_system_grid": (_i32, [_vp, _i64, _i64, _i64, _dbl, _dbl, _dbl, C.c_float,
                                     C.c_float, _f32p, _f32p, _f32p, _i32, _dbl, C.c_float,
                                     C.c_float, _f32p, _f32p, C.POINTER(_dbl), C.c_char_p, _i32]),
+    "hx_export_webdata": (_i32, [_vp, C.c_char_p, _i32, _vp, _vp, _vp, C.c_float, _i32,
+                                 C.c_float, C.c_char_p, _i64, C.POINTER(_i64)]),
+    "hx_export_webdata_device": (_i32, [_vp, C.c_char_p, _vp, _vp, _vp, C.c_float, _i32,
+                                        C.c_float, C.c_char_p, _i64, C.POINTER(_i64)]),
     "hx_filter": (_i32, [_vp, _i32, _vp, _vp, _dbl, _i32, _dbl, _i32, C.POINTER(SolveReport)]),
     "hx_filter_device": (_i32, [_vp, _vp, _vp, _dbl, _i32, _dbl, _i32, C.POINTER(SolveReport)]),
     "hx_apply_gpu_filter": (_i32, [_vp, _f32p, _i64, _i64, _i64, _dbl, _dbl, _dbl, _dbl, _dbl,

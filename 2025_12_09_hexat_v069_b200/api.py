@@ -5,6 +5,8 @@ error behaviour of the reference routines this library replaces.
   apply_gpu_filter       src/Optimization/GPUHelmholtz.jl:344-376
   compute_stress_field   src/Core/Stress.jl:57-100
   update_density         src/Optimization/TopOpt.jl:139-405
+  export_binary_for_web  src/IO/Postprocessing.jl:159-262 (and load_checkpoint,
+                         src/IO/Configuration.jl:31-77, to read the file back)
 
 Arrays follow the Julia layout (see mesh.py); each call runs on the GPU
 through libhexat_b200.so.
@@ -198,3 +200,86 @@ def update_density(density, l1_stress_norm_field, protected_elements_mask, E,
     ctx.check(st, "update_density")
     return (res.max_change, res.R_length, res.current_threshold, res.filter_time,
             res.filter_iters, res.filter_res)
+
+
+def _webdata_meta(config, iter, current_radius, threshold):
+    """The JSON metadata export_binary_for_web writes (Postprocessing.jl:198-231):
+    the config plus iteration, radius and threshold, an 'action' synthesised
+    from 'stiffness_ratio' for geometry shapes, and the loads / bcs / settings
+    aliases the viewers read."""
+    import copy
+    meta = copy.deepcopy(config)
+    meta["iteration"] = int(iter)
+    meta["radius"] = float(current_radius)
+    meta["threshold"] = float(threshold)
+    geom = meta.get("geometry")
+    if isinstance(geom, dict):
+        for shape in geom.values():
+            if isinstance(shape, dict) and "type" in shape and "action" not in shape \
+                    and "stiffness_ratio" in shape:
+                shape["action"] = "add" if float(shape["stiffness_ratio"]) > 0 else "remove"
+    meta["loads"] = config.get("external_forces", [])
+    meta["bcs"] = config.get("boundary_conditions", [])
+    meta["settings"] = config.get("optimization_parameters", {})
+    return meta
+
+
+def export_binary_for_web(filename, nodes, elements, density, l1_stress, principal_field, geom,
+                          threshold, iter, current_radius, config, ctx=None):
+    """export_binary_for_web: writes the webdata/checkpoint file.  `nodes`
+    and `elements` must be generate_mesh's (grid numbering); `geom` is
+    accepted for signature parity (the element sizes come from the mesh);
+    principal_field is (3, nE) as in the reference.  Returns the number of
+    elements written (0: no file, as in the reference)."""
+    import json
+    ctx = ctx or default_context()
+    ctx.set_mesh(nodes, elements)
+    d = np.ascontiguousarray(density, dtype=np.float32)
+    l1 = np.ascontiguousarray(l1_stress, dtype=np.float32)
+    pr = np.ascontiguousarray(np.asarray(principal_field, dtype=np.float32).T)
+    text = json.dumps(_webdata_meta(config, iter, current_radius, threshold),
+                      separators=(",", ":")).encode()
+    cnt = C.c_int64()
+    st = ctx.lib.hx_export_webdata(ctx.h, str(filename).encode(), _lib.HX_F32, _p(d), _p(l1),
+                                   _p(pr), float(threshold), int(iter), float(current_radius),
+                                   text, len(text), C.byref(cnt))
+    ctx.check(st, "export_binary_for_web")
+    return cnt.value
+
+
+def read_webdata(filename):
+    """Every field of a webdata file, in the layout load_checkpoint
+    (src/IO/Configuration.jl:31-77) reads: a dict with magic, version, iter,
+    radius, threshold, count, h, centroids (count, 3), density, signed_l1 and
+    config (the parsed JSON)."""
+    import json
+    with open(filename, "rb") as fh:
+        buf = fh.read()
+    hdr = np.frombuffer(buf, "<u4", 2, 0)
+    it = int(np.frombuffer(buf, "<i4", 1, 8)[0])
+    rad, thr = (float(v) for v in np.frombuffer(buf, "<f4", 2, 12))
+    count = int(np.frombuffer(buf, "<u4", 1, 20)[0])
+    h = tuple(float(v) for v in np.frombuffer(buf, "<f4", 3, 24))
+    o = 36
+    cent = np.frombuffer(buf, "<f4", 3 * count, o).reshape(count, 3)
+    o += 12 * count
+    dens = np.frombuffer(buf, "<f4", count, o)
+    o += 4 * count
+    sl1 = np.frombuffer(buf, "<f4", count, o)
+    o += 4 * count
+    jl = int(np.frombuffer(buf, "<u4", 1, o)[0])
+    o += 4
+    cfg = json.loads(buf[o:o + jl].decode()) if jl else None
+    assert o + jl == len(buf), "trailing bytes in webdata file"
+    return {"magic": int(hdr[0]), "version": int(hdr[1]), "iter": it, "radius": rad,
+            "threshold": thr, "count": count, "h": h, "centroids": cent, "density": dens,
+            "signed_l1": sl1, "config": cfg}
+
+
+def load_checkpoint(filename):
+    """load_checkpoint (src/IO/Configuration.jl:31-77) -> (config, density,
+    restart_iter, restart_radius, restart_threshold)."""
+    w = read_webdata(filename)
+    if w["magic"] != 0x48455841:
+        raise ValueError("Invalid file format. Not a HEXA checkpoint.")
+    return w["config"], w["density"].copy(), w["iter"], w["radius"], w["threshold"]

@@ -67,6 +67,7 @@ void set_grid_impl(hx_ctx* c, int64_t nx, int64_t ny, int64_t nz, double dx, dou
   c->h[2] = dz;
   c->K = hx::make_elem_coef(dx, dy, dz, c->nu);
   c->has_mesh = true;
+  c->origin[0] = c->origin[1] = c->origin[2] = 0.0;
   c->node_map.clear();
   c->elem_map.clear();
   c->present.clear();
@@ -160,6 +161,7 @@ void set_mesh_impl(hx_ctx* c, const float* nodes, int64_t nN, const int64_t* el,
     if (ge != e) ident = false;
   }
   set_grid_impl(c, g.nxe, g.nye, g.nze, dx, dy, dz);
+  for (int d = 0; d < 3; ++d) c->origin[d] = mn[d];
   if (!ident) {
     c->node_map = std::move(nmap);
     c->elem_map = std::move(emap);
@@ -245,6 +247,11 @@ void down_elems(hx_ctx* c, int32_t dt, const double* d, void* h, int w = 1) {
 
 void need_mesh(const hx_ctx* c) {
   HX_REQUIRE(c->has_mesh, "no mesh: call hx_set_grid or hx_set_mesh first");
+}
+
+void need_grid_numbering(hx_ctx* c) {
+  need_mesh(c);
+  HX_REQUIRE(identity(c), "device-array entry points need a grid mesh (hx_set_grid)");
 }
 
 hx_solve_opts sanitize(const hx_solve_opts* o) {
@@ -642,6 +649,40 @@ HX_API hx_status hx_solve_system_grid(hx_ctx* c, int64_t nx, int64_t ny, int64_t
   });
 }
 
+HX_API hx_status hx_export_webdata(hx_ctx* c, const char* path, int32_t dt, const void* density,
+                                   const void* l1, const void* principal, float threshold,
+                                   int32_t iter, float radius, const char* json, int64_t json_len,
+                                   int64_t* count) {
+  return guard(c, [&] {
+    need_mesh(c);
+    check_dtype(dt);
+    HX_REQUIRE(density && l1 && principal, "null argument");
+    HX_REQUIRE(identity(c), "the export needs the mesh in grid numbering (generate_mesh order)");
+    hx::ensure_workspace(c);
+    const int64_t ne = c->g.elems();
+    double* dd = c->d_aux0.ensure(ne);
+    double* dl = c->d_aux1.ensure(ne);
+    double* dp = c->d_aux2.ensure(3 * ne);
+    up_elems(c, dt, density, dd);
+    up_elems(c, dt, l1, dl);
+    up_elems(c, dt, principal, dp, 3);
+    return hx::export_webdata<double>(c, path, dd, dl, dp, threshold, iter, radius, json,
+                                      json_len, count);
+  });
+}
+
+HX_API hx_status hx_export_webdata_device(hx_ctx* c, const char* path, const double* density,
+                                          const double* l1, const double* principal,
+                                          float threshold, int32_t iter, float radius,
+                                          const char* json, int64_t json_len, int64_t* count) {
+  return guard(c, [&] {
+    need_grid_numbering(c);
+    HX_REQUIRE(density && l1 && principal, "null argument");
+    return hx::export_webdata<double>(c, path, density, l1, principal, threshold, iter, radius,
+                                      json, json_len, count);
+  });
+}
+
 HX_API hx_status hx_filter(hx_ctx* c, int32_t dt, const void* rho, void* out, double radius,
                            int32_t ref_compat, double tol, int32_t max_iter,
                            hx_solve_report* rep) {
@@ -881,10 +922,6 @@ HX_API hx_status hx_update_density(hx_ctx* c, float* density, float* l1,
 }
 
 // ---- device-resident pieces of the optimisation loop (grid numbering) ----
-static void need_grid_numbering(hx_ctx* c) {
-  need_mesh(c);
-  HX_REQUIRE(identity(c), "device-array entry points need a grid mesh (hx_set_grid)");
-}
 
 HX_API hx_status hx_simp_device(hx_ctx* c, const double* rho, double p, double e0, double emin,
                                 double* fac) {

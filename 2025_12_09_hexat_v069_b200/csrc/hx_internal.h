@@ -209,6 +209,15 @@ struct hx_ctx {
 
   int64_t launches = 0;  // kernels launched on behalf of this context
 
+  // lattice origin of the mesh (the minimum node coordinates; 0 for hx_set_grid)
+  double origin[3] = {0, 0, 0};
+
+  // webdata export (hx_export.cu): per-block survivor counts and offsets, outputs
+  struct Export {
+    hx::DevBuf<unsigned long long> counts, offsets;
+    hx::DevBuf<float> cent, dens, sl1;
+  } exp;
+
   // density update (hx_update.cu): Float32 fields, FP64 filter buffers
   struct Update {
     hx::DevBuf<float> dens, l1, orig, dc, fout;

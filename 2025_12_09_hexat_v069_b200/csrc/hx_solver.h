@@ -66,6 +66,12 @@ hx_status update_density(hx_ctx* c, float* density, float* l1, const uint8_t* pr
                          float* filtered_out, hx_update_result* res);
 void update_radius_schedule(const hx_update_params& p, int it, int n_iter, double* R_length,
                             double* R_effective);
+// export_binary_for_web from element arrays in grid numbering on the device
+// (T = double or float; principal: 3 values per element) (hx_export.cu).
+template <typename T>
+hx_status export_webdata(hx_ctx* c, const char* path, const T* dens, const T* l1, const T* pr,
+                         float threshold, int iter, float radius, const char* json,
+                         int64_t json_len, int64_t* count_out);
 // Average time of `reps` launches of one kernel on the last solve's buffers.
 hx_status time_kernel(hx_ctx* c, int kernel, int reps, double* avg_ms);
 }  // namespace hx

@@ -279,6 +279,35 @@ HX_API hx_status hx_compute_stress_field(
     int64_t n_elem, const float *U, float E, float nu, const float *density,
     float *principal, float *vonmises, float *voigt, float *l1, float *dir);
 
+/* ---- result file ------------------------------------------------------------
+ * Drop-in for export_binary_for_web(filename, nodes, elements, density,
+ * l1_stress, principal_field, geom, threshold, iter, current_radius, config),
+ * src/IO/Postprocessing.jl:159-262: the "webdata" file the reference's
+ * viewers and its checkpoint restart (src/IO/Configuration.jl:31-77) read.
+ * Magic 0x48455841 ("HEXA"), version 2, iter, radius, threshold, count, dx,
+ * dy, dz, then for the elements with density >= threshold, in element order:
+ * centroids (3 Float32 each), densities, L1 stress signed by the principal
+ * stress of largest magnitude; then the JSON text's byte length and the text
+ * (the caller serialises its config, as the reference's JSON.json does).
+ * The selection and the per-element values are computed on the device; no
+ * file is written when no element passes (*count = 0).  Needs the mesh in
+ * grid numbering (hx_set_grid, or generate_mesh order through hx_set_mesh).
+ * hx_export_webdata: host arrays of dtype (principal: 3 values per element,
+ * element-major); _device: FP64 device arrays. */
+HX_API hx_status hx_export_webdata(hx_ctx *ctx, const char *path, int32_t dtype,
+                                   const void *density, const void *l1_stress,
+                                   const void *principal, float threshold,
+                                   int32_t iter, float current_radius,
+                                   const char *json, int64_t json_len,
+                                   int64_t *count);
+HX_API hx_status hx_export_webdata_device(hx_ctx *ctx, const char *path,
+                                          const double *density_dev,
+                                          const double *l1_dev,
+                                          const double *principal_dev,
+                                          float threshold, int32_t iter,
+                                          float current_radius, const char *json,
+                                          int64_t json_len, int64_t *count);
+
 /* ---- compliance, sensitivities, OC update ------------------------------------
  * hx_compliance: c = f.u in FP64 (src/Main.jl:428 computes it on the host).
  * hx_element_energy: ce_e = u_e^T Ke u_e with unit modulus (no reference

@@ -314,3 +314,37 @@ def update_density(density, l1, protected, E, allowable, it, n_iter, original, m
     dens[cand] = min_d
     dens[prot] = orig[prot]
     return dens, l1, (max_change, R_length, float(thr), iters, res), filtered
+
+
+def webdata_arrays(dims, h, density, l1, principal, threshold):
+    """Restatement of export_binary_for_web's arrays
+    (src/IO/Postprocessing.jl:172-193) on generate_mesh's grid, in float32:
+    findall(density .>= threshold) in element order; centroid = Float32 sum
+    of the 8 corner coordinates (Int * Float32 products) in NAT_COORDS order
+    times 0.125f0 (MeshUtilities.element_centroid); L1 stress times the sign
+    of the principal stress of largest magnitude.  Returns (centroids (n, 3),
+    densities, signed L1)."""
+    f32 = np.float32
+    nx, ny, nz = dims
+    d = np.asarray(density, f32)
+    idx = np.nonzero(d >= f32(threshold))[0]
+    i = idx % nx
+    j = (idx // nx) % ny
+    k = idx // (nx * ny)
+    cent = np.zeros((idx.size, 3), f32)
+    corner = [(0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0), (0, 0, 1), (1, 0, 1), (1, 1, 1),
+              (0, 1, 1)]
+    for a, (ijk, hh) in enumerate(zip((i, j, k), h)):
+        acc = np.zeros(idx.size, f32)
+        for c in corner:
+            acc = (acc + (ijk + c[a]).astype(f32) * f32(hh)).astype(f32)
+        cent[:, a] = acc * f32(0.125)
+    pr = np.asarray(principal, f32).reshape(-1, 3)[idx]
+    sgn = np.sign(pr[:, 0])
+    amax = np.abs(pr[:, 0])
+    for c in (1, 2):
+        big = np.abs(pr[:, c]) > amax
+        amax = np.where(big, np.abs(pr[:, c]), amax)
+        sgn = np.where(big, np.sign(pr[:, c]), sgn)
+    sl1 = (np.asarray(l1, f32)[idx] * sgn.astype(f32)).astype(f32)
+    return cent, d[idx], sl1

@@ -147,3 +147,41 @@ def test_oc_mode_matches_oracle(ctx, hx, orc):
     want[prot] = orig[prot]
     assert _ulp_close(d, want, ulps=1)
     assert out[1] == R and out[2] == 0.0
+
+
+def test_webdata_file_matches_the_restatement(ctx, hx, orc, tmp_path):
+    """export_binary_for_web (src/IO/Postprocessing.jl:159-262) through
+    hx_export_webdata: the file parses as load_checkpoint reads it and every
+    array equals the oracle's float32 restatement bit for bit."""
+    from importlib import import_module
+    api = import_module(hx.__name__ + ".api")
+    dims = (13, 7, 5)
+    h = (1.0, 0.5, 2.0)
+    nodes, el, _ = hx.mesh.generate_mesh(*dims, *h)
+    n = el.shape[0]
+    rng = np.random.default_rng(9)
+    dens = rng.uniform(0.0, 1.0, n).astype(np.float32)
+    l1 = rng.gamma(2.0, 1.0, n).astype(np.float32)
+    pr = rng.standard_normal((3, n)).astype(np.float32)
+    pr[:, ::11] = 0.0  # sign(0) = 0
+    cfg = {"geometry": {"hole": {"type": "sphere", "stiffness_ratio": 0.0}},
+           "optimization_parameters": {"max_culling_ratio": 0.1}, "external_forces": [1]}
+    path = tmp_path / "it7.bin"
+    cnt = api.export_binary_for_web(path, nodes, el, dens, l1, pr, None, np.float32(0.3), 7,
+                                    np.float32(2.5), cfg, ctx=ctx)
+    w = api.read_webdata(path)
+    cent, d, s = orc.webdata_arrays(dims, h, dens, l1, pr.T, np.float32(0.3))
+    assert cnt == w["count"] == d.size > 0
+    assert w["magic"] == 0x48455841 and w["version"] == 2 and w["iter"] == 7
+    assert w["radius"] == 2.5 and w["threshold"] == float(np.float32(0.3))
+    assert w["h"] == h
+    assert np.array_equal(w["centroids"], cent)
+    assert np.array_equal(w["density"], d) and np.array_equal(w["signed_l1"], s)
+    assert w["config"]["iteration"] == 7 and w["config"]["loads"] == [1]
+    assert w["config"]["geometry"]["hole"]["action"] == "remove"
+    c2, d2, it2, r2, t2 = api.load_checkpoint(path)
+    assert it2 == 7 and np.array_equal(d2, d)
+    # nothing passes the threshold: no file, as in the reference
+    assert api.export_binary_for_web(tmp_path / "none.bin", nodes, el, dens * 0, l1, pr, None,
+                                     np.float32(0.3), 7, np.float32(2.5), cfg, ctx=ctx) == 0
+    assert not (tmp_path / "none.bin").exists()
