@@ -564,6 +564,9 @@ HX_API hx_status hx_solve_system_gpu(hx_ctx* c, const float* nodes, int64_t nN,
     o.ref_retry = 1;
     o.keep_best = 1;
     o.divergence_checks = 1;
+    // the reference's default "jacobi_amg" (configs/default.yaml:191):
+    // multigrid takes over from a failed Jacobi attempt
+    o.multigrid_fallback = 1;
     std::vector<float> u(3 * nN, 0.0f);
     if (u_guess) std::memcpy(u.data(), u_guess, u.size() * sizeof(float));
     hx_solve_report R{};
@@ -580,7 +583,7 @@ HX_API hx_status hx_solve_system_gpu(hx_ctx* c, const float* nodes, int64_t nN,
     down_nodes3(c, HX_F32, du, x_full);
     if (final_rel_res) *final_rel_res = R.rel_res;
     if (prec_name && prec_name_cap > 0) {
-      const char* nm = R.zero_rhs ? "None" : "Jacobi";
+      const char* nm = R.zero_rhs ? "None" : (R.fallback_used ? "GMG" : "Jacobi");
       std::strncpy(prec_name, nm, (size_t)prec_name_cap - 1);
       prec_name[prec_name_cap - 1] = '\0';
     }
@@ -633,6 +636,9 @@ HX_API hx_status hx_solve_system_grid(hx_ctx* c, int64_t nx, int64_t ny, int64_t
     o.ref_retry = 1;
     o.keep_best = 1;
     o.divergence_checks = 1;
+    // the reference's default "jacobi_amg" (configs/default.yaml:191):
+    // multigrid takes over from a failed Jacobi attempt
+    o.multigrid_fallback = 1;
     hx_solve_report R{};
     hx_status s = hx::solve_grid(c, df, dfac, du, o, &R);
     float* so = (float*)c->d_stage.ensure(n * sizeof(float));
@@ -641,7 +647,7 @@ HX_API hx_status hx_solve_system_grid(hx_ctx* c, int64_t nx, int64_t ny, int64_t
     HX_CUDA(cudaStreamSynchronize(c->stream));
     if (final_rel_res) *final_rel_res = R.rel_res;
     if (prec_name && prec_name_cap > 0) {
-      const char* nm = R.zero_rhs ? "None" : "Jacobi";
+      const char* nm = R.zero_rhs ? "None" : (R.fallback_used ? "GMG" : "Jacobi");
       std::strncpy(prec_name, nm, (size_t)prec_name_cap - 1);
       prec_name[prec_name_cap - 1] = '\0';
     }
@@ -1089,11 +1095,17 @@ HX_API hx_status hx_residual_device(hx_ctx* c, const double* f, const double* fa
   return guard(c, [&] {
     need_mesh(c);
     HX_REQUIRE(f && fac && x && r, "null argument");
-    // the operator stages x in 16-byte chunks
-    HX_REQUIRE(((uintptr_t)x & 15u) == 0, "x_dev must be 16-byte aligned");
+    HX_REQUIRE(((uintptr_t)x & 7u) == 0, "x_dev must be 8-byte aligned");
     hx::ensure_workspace(c);
     if (c->bc_dirty) hx::upload_bc(c);
     const int64_t n = c->g.dofs();
+    // the operator stages x in 16-byte chunks: an x that is only 8-byte
+    // aligned (a row of a snapshot matrix with an odd row length) is copied
+    if (((uintptr_t)x & 15u) != 0) {
+      double* xa = c->d_aux3.ensure(n);
+      HX_CUDA(cudaMemcpyAsync(xa, x, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+      x = xa;
+    }
     double shift = 0;
     hx::jacobi_setup_public(c, fac, 0.0, &shift);
     double* q = c->d_q.ensure(n);

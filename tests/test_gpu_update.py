@@ -92,26 +92,45 @@ def test_stress_ratio_update_matches_oracle(ctx, hx, orc, it, n_iter):
 
 
 def test_culling_cap_ties_in_element_order(ctx, hx, orc):
-    """A uniform stress field makes the filtered proposal (nearly) constant:
-    thousands of candidates share a few density values, more than the cap
-    allows, so the cut falls inside runs of equal values; the reference's
-    stable sort culls those ties in element order, and so must the device's
-    radix select."""
+    """A uniform stress field makes the filtered proposal nearly constant, so
+    many candidates share a density value.  A first run gives the filtered
+    field; the cap of the second run (same inputs, same field) is chosen so
+    that the cut falls inside the longest run of equal candidate values.
+    The reference's stable sort culls such ties in element order, and so
+    must the device's radix select: the result equals the oracle's bit for
+    bit and splits the run."""
     n = int(np.prod(DIMS))
     dens = np.full(n, 0.6, np.float32)
     l1 = np.full(n, 0.2, np.float32)
     prot = np.zeros(n, bool)
     prot[::97] = True
     orig = np.full(n, 0.8, np.float32)
-    cfg = _config(max_culling_ratio=0.03)
-    d, _, filt, out = _run(hx, ctx, cfg, dens, l1, prot, orig, 40, 40)
-    vals, counts = np.unique(filt[~prot], return_counts=True)
-    assert counts.max() > 100  # ties, as intended
+    f32 = np.float32
+    _, _, filt, _ = _run(hx, ctx, _config(), dens, l1, prot, orig, 40, 40)
+    new = np.clip(filt, f32(1e-3), f32(1.0))
+    cand = np.nonzero(~prot & (new > f32(1e-3)) & (new < f32(0.95)))[0]
+    order = cand[np.argsort(new[cand], kind="stable")]
+    vals = new[order]
+    # the longest run of equal values among the sorted candidates
+    starts = np.r_[0, np.nonzero(vals[1:] != vals[:-1])[0] + 1]
+    ends = np.r_[starts[1:], vals.size]
+    a, b = max(zip(starts, ends), key=lambda t: t[1] - t[0])
+    assert b - a >= 3, "no run of tied candidates to split"
+    active = np.count_nonzero(~prot & (new > f32(1e-3))) + np.count_nonzero(prot)
+    k = a + (b - a) // 2  # cull the first k: the cut splits the run
+    ratio = f32((k + 0.5) / active)
+    assert int(np.floor(f32(active) * ratio)) == k
+    cfg = _config(max_culling_ratio=float(ratio))
+    d, _, filt2, out = _run(hx, ctx, cfg, dens, l1, prot, orig, 40, 40)
+    assert np.array_equal(filt2, filt)  # deterministic
     do, _, (mc, R, thr, _, _), _ = _oracle(orc, cfg, dens, l1, prot, orig, 40, 40, filtered=filt)
     assert np.array_equal(d, do)
-    culled = np.count_nonzero((d == np.float32(1e-3)) & ~prot)
-    active = np.count_nonzero(~prot) + np.count_nonzero(prot)
-    assert culled == int(np.floor(np.float32(active) * np.float32(0.03)))
+    culled = (d == f32(1e-3)) & ~prot
+    assert np.count_nonzero(culled) == k
+    run = order[a:b]
+    assert 0 < np.count_nonzero(culled[run]) < run.size  # the run is split
+    # ties go in element order: the culled members of the run come first
+    assert np.all(culled[run][:k - a]) and not np.any(culled[run][k - a:])
 
 
 def test_stress_regularisation_filters_the_l1_field_in_place(ctx, hx, orc):
