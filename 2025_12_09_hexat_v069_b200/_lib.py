@@ -16,7 +16,7 @@ HX_OK, HX_NOT_CONVERGED, HX_STALLED, HX_BREAKDOWN, HX_NONFINITE = 0, 1, 2, 3, 4
 HX_OOM, HX_BAD_ARG, HX_CUDA_ERROR, HX_NO_DEVICE, HX_DIVERGED = 5, 6, 7, 8, 9
 HX_F32, HX_F64 = 0, 1
 HX_PREC_FP64, HX_PREC_MIXED32 = 0, 1
-HX_PC_JACOBI, HX_PC_LEARNED, HX_PC_NONE = 0, 1, 2
+HX_PC_JACOBI, HX_PC_LEARNED, HX_PC_NONE, HX_PC_MULTIGRID = 0, 1, 2, 3
 (HX_KERNEL_PCG_STEP_FP64, HX_KERNEL_PCG_UPDATE_FP64, HX_KERNEL_APPLY_FP64, HX_KERNEL_PCG_STEP_FP32,
  HX_KERNEL_FILTER_MATVEC, HX_KERNEL_CONV3, HX_KERNEL_NET_APPLY, HX_KERNEL_FCG_STEP_FP32) = range(8)
 
@@ -28,7 +28,8 @@ class SolveOpts(C.Structure):
         ("wall_limit_ms", C.c_double), ("check_every", C.c_int32), ("keep_best", C.c_int32),
         ("inner_tol", C.c_double), ("max_refine", C.c_int32), ("ref_retry", C.c_int32),
         ("divergence_checks", C.c_int32), ("verify_true_residual", C.c_int32),
-        ("learned_no_fallback", C.c_int32), ("reserved", C.c_int32 * 5),
+        ("learned_no_fallback", C.c_int32), ("multigrid_fallback", C.c_int32),
+        ("reserved", C.c_int32 * 4),
     ]
 
 

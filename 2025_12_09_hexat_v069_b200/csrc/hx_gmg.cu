@@ -1,0 +1,477 @@
+// hx_gmg.cu -- geometric multigrid on the voxel grid: the robust
+// preconditioner that replaces the reference's CPU algebraic multigrid
+// (src/Solvers/GPUSolver.jl:168-268 assembles the matrix on the host and
+// builds AlgebraicMultigrid's smoothed aggregation; every PCG iteration then
+// copies r to the host and z back, :513-516).  Here nothing leaves the GPU
+// and no matrix is assembled.
+//
+// Hierarchy: level l+1 halves every element count of level l (built while
+// all three are even); its element factor is the mean of its 8 children and
+// its element size doubles, so the coarse operator is the same matrix-free
+// structured operator (hx_operator.cu) on the coarse grid.  A coarse node is
+// the fine node at twice its index; it is fixed where that fine node's BC
+// bit is set, and nodes without stiffness are held at 0 as on level 0.
+// Transfers: trilinear prolongation P and its exact transpose R = P^T
+// (full weighting), the kernels of the learned preconditioner's levels.
+//
+// V-cycle (FP32): on each level Chebyshev smoothing of degree GMG_DEGREE
+// with Jacobi scaling on [0.05, 1.1] x lambda_max(D^-1 A) (estimated by
+// power iteration at set-up), from zero before the restriction and from the
+// prolonged correction after it; on the coarsest level GMG_COARSE_ITERS
+// iterations of FP32 Jacobi-PCG on the fused kernels.  The cycle is
+// symmetric positive definite up to the coarse solve's early stop and FP32
+// rounding, which the flexible CG around it absorbs (Notay's FCG, the same
+// step kernels as the learned preconditioner).
+#include <cmath>
+#include <limits>
+
+#include "hx_cnn.h"
+#include "hx_solver.h"
+
+namespace hx {
+
+namespace {
+
+constexpr int GMG_DEGREE = 2;          // Chebyshev degree per smoothing
+constexpr int GMG_COARSE_ITERS = 64;   // PCG iterations on the coarsest level
+constexpr int64_t GMG_COARSE_NODES = 4096;
+constexpr float GMG_LO = 0.05f, GMG_HI = 1.1f;  // Chebyshev range / lambda_max
+
+__device__ __forceinline__ int64_t gt() { return blockIdx.x * (int64_t)blockDim.x + threadIdx.x; }
+__device__ __forceinline__ int64_t gs() { return (int64_t)gridDim.x * blockDim.x; }
+
+// coarse element factor = mean of its 8 children
+__global__ void k_coarse_fac(const float* __restrict__ ff, float* __restrict__ fc, Grid gf,
+                             Grid gc) {
+  const int64_t ne = gc.elems();
+  for (int64_t e = gt(); e < ne; e += gs()) {
+    const int i = (int)(e % gc.nxe);
+    const int64_t t = e / gc.nxe;
+    const int j = (int)(t % gc.nye), k = (int)(t / gc.nye);
+    float s = 0.f;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const int fi = 2 * i + (c & 1), fj = 2 * j + ((c >> 1) & 1), fk = 2 * k + (c >> 2);
+      s += ff[((int64_t)fk * gf.nye + fj) * gf.nxe + fi];
+    }
+    fc[e] = 0.125f * s;
+  }
+}
+
+// coarse node BC bits = those of the fine node at twice its index
+__global__ void k_coarse_bc(const uint8_t* __restrict__ bf, uint8_t* __restrict__ bc, Grid gf,
+                            Grid gc) {
+  const int64_t nn = gc.nodes();
+  for (int64_t n = gt(); n < nn; n += gs()) {
+    const int i = (int)(n % gc.nxn);
+    const int64_t t = n / gc.nxn;
+    const int j = (int)(t % gc.nyn), k = (int)(t / gc.nyn);
+    bc[n] = bf[((int64_t)(2 * k) * gf.nyn + 2 * j) * gf.nxn + 2 * i];
+  }
+}
+
+// v[3n + c] = 0 where bit c of nmask[n] is clear (fixed DOF)
+__global__ void k_mask3(float* __restrict__ v, const uint8_t* __restrict__ nmask, int64_t nn) {
+  for (int64_t i = gt(); i < 3 * nn; i += gs())
+    if (!((nmask[i / 3] >> (i % 3)) & 1u)) v[i] = 0.f;
+}
+
+// Chebyshev start: r = b - q (q may be null: x = 0), d = minv r / theta,
+// x = (x0 or 0) + d
+__global__ void k_cheb_start(const float* __restrict__ b, const float* __restrict__ q,
+                             const float* __restrict__ minv, float* __restrict__ r,
+                             float* __restrict__ d, float* __restrict__ x, int xzero,
+                             float inv_theta, int64_t n) {
+  for (int64_t i = gt(); i < n; i += gs()) {
+    const float ri = q ? b[i] - q[i] : b[i];
+    const float di = minv[i] * ri * inv_theta;
+    r[i] = ri;
+    d[i] = di;
+    x[i] = xzero ? di : x[i] + di;
+  }
+}
+
+// Chebyshev step: r -= q (q = A d), d = a d + c minv r, x += d
+__global__ void k_cheb_step(const float* __restrict__ q, const float* __restrict__ minv,
+                            float* __restrict__ r, float* __restrict__ d, float* __restrict__ x,
+                            float a, float cc, int64_t n) {
+  for (int64_t i = gt(); i < n; i += gs()) {
+    const float ri = r[i] - q[i];
+    const float di = a * d[i] + cc * minv[i] * ri;
+    r[i] = ri;
+    d[i] = di;
+    x[i] += di;
+  }
+}
+
+// r -= q
+__global__ void k_sub(float* __restrict__ r, const float* __restrict__ q, int64_t n) {
+  for (int64_t i = gt(); i < n; i += gs()) r[i] -= q[i];
+}
+
+template <typename TD, typename TS>
+__global__ void k_copy_cvt(TD* __restrict__ d, const TS* __restrict__ s, int64_t n) {
+  for (int64_t i = gt(); i < n; i += gs()) d[i] = (TD)s[i];
+}
+
+// d = a * s
+__global__ void k_scale_copy(float* __restrict__ d, const float* __restrict__ s, float a,
+                             int64_t n) {
+  for (int64_t i = gt(); i < n; i += gs()) d[i] = a * s[i];
+}
+
+// power-iteration start: a pseudo-random vector (hash of the index), zero on
+// fixed DOFs
+__global__ void k_rand_vec(float* __restrict__ v, const uint8_t* __restrict__ nmask, int64_t nn) {
+  for (int64_t i = gt(); i < 3 * nn; i += gs()) {
+    uint32_t h = (uint32_t)i * 2654435761u + 0x9E3779B9u;
+    h ^= h >> 16;
+    h *= 0x85EBCA6Bu;
+    h ^= h >> 13;
+    const float u = (float)(h & 0xFFFFFF) / 16777216.f - 0.5f;
+    v[i] = ((nmask[i / 3] >> (i % 3)) & 1u) ? u : 0.f;
+  }
+}
+
+// w = minv * w (in place); out[0] = |w|^2, out[1] = |v|^2 (FP64 sums)
+__global__ void k_power_norms(float* __restrict__ w, const float* __restrict__ minv,
+                              const float* __restrict__ v, int64_t n, double* partials,
+                              CgState* st, double* out) {
+  double a = 0.0, b = 0.0;
+  for (int64_t i = gt(); i < n; i += gs()) {
+    const float wi = minv[i] * w[i];
+    w[i] = wi;
+    a += (double)wi * wi;
+    b += (double)v[i] * v[i];
+  }
+  double vv[2] = {a, b};
+  if (grid_reduce<2>(vv, partials, &st->ticket[TK_AUX]) && threadIdx.x == 0) {
+    out[0] = vv[0];
+    out[1] = vv[1];
+  }
+}
+
+// fresh coarse-solve state (inside a captured cycle: no host round trip)
+__global__ void k_coarse_reset(CgState* st, int max_iter, double tol) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    st->iter = 0;
+    st->max_iter = max_iter;
+    st->tol = tol;
+    st->status = HX_RUNNING;
+    st->check_every = 1;
+    st->explode = 0.0;
+    st->div_ratio = 0.0;
+    st->keep_best = 0;
+    st->alpha = 0.0;
+    st->beta = 0.0;
+    st->aux[1] = 0.0;
+    st->best_rel = INFINITY;
+  }
+}
+
+// the pending x += alpha p_k of the last coarse PCG iteration, p_k picked
+// by the iteration count's parity (iteration k writes p into P[k % 2])
+__global__ void k_coarse_finish(float* __restrict__ x, const float* __restrict__ p0,
+                                const float* __restrict__ p1, const CgState* st, int64_t n) {
+  const int it = st->iter;
+  if (st->status == HX_ST_BREAKDOWN || it <= 0) return;
+  const float* pk = ((it - 1) % 2 == 0) ? p0 : p1;
+  const float a = (float)st->alpha;
+  for (int64_t i = gt(); i < n; i += gs()) x[i] += a * pk[i];
+}
+
+// flexible-CG coefficients for a preconditioned residual z: beta =
+// -(z.q_old) / (p_old.q_old) (st->pq), st->aux[3] = z.r (the step length's
+// numerator, used by the flexible-CG step)
+template <typename T>
+__global__ void k_fcg_coeffs(const T* __restrict__ z, const T* __restrict__ q_old,
+                             const T* __restrict__ r, int64_t n, double* partials, CgState* st) {
+  if (st->status != HX_RUNNING) return;
+  double zq = 0.0, zr = 0.0;
+  for (int64_t i = gt(); i < n; i += gs()) {
+    zq += (double)z[i] * (double)q_old[i];
+    zr += (double)z[i] * (double)r[i];
+  }
+  double v[2] = {zq, zr};
+  if (grid_reduce<2>(v, partials, &st->ticket[TK_AUX2]) && threadIdx.x == 0) {
+    const double pq = st->pq;
+    st->beta = (pq > 0.0 && isfinite(v[0])) ? -v[0] / pq : 0.0;
+    st->aux[3] = v[1];
+  }
+}
+
+unsigned gblocks(int64_t n) {
+  return (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv(n, 256), 16LL * sm_count()));
+}
+
+GridN node_grid(const Grid& g) { return GridN{g.nxn, g.nyn, g.nzn}; }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Hierarchy set-up for the factors `fac` (FP64, level 0) with the solve's
+// node mask and M^-1 (c->d_nmask, c->d_minv, already set up with `shift`).
+// ---------------------------------------------------------------------------
+void gmg_setup(hx_ctx* c, const double* fac, double shift) {
+  auto& G = c->gmg;
+  cudaStream_t s = c->stream;
+  G.nl = 0;
+  Grid g = c->g;
+  double h[3] = {c->h[0], c->h[1], c->h[2]};
+  for (int l = 0; l < HX_GMG_MAX_LEVELS; ++l) {
+    auto& L = G.lv[l];
+    L.g = g;
+    for (int a = 0; a < 3; ++a) L.h[a] = h[a];
+    const int64_t nn = g.nodes(), n = g.dofs(), ne = g.elems();
+    L.K = to_float(make_elem_coef(h[0], h[1], h[2], c->nu));
+    float* fl = L.fac.ensure(ne);
+    uint8_t* bc = L.bc.ensure(nn);
+    uint8_t* nm = L.nmask.ensure(nn);
+    float* minv = L.minv.ensure(n);
+    L.b.ensure(n);
+    L.x.ensure(n);
+    L.r.ensure(n);
+    L.d.ensure(n);
+    L.q.ensure(n);
+    if (l == 0) {
+      k_copy_cvt<float, double><<<gblocks(ne), 256, 0, s>>>(fl, fac, ne);
+      HX_CHECK_LAUNCH();
+      HX_CUDA(cudaMemcpyAsync(bc, c->d_bcfree.p, nn, cudaMemcpyDeviceToDevice, s));
+      HX_CUDA(cudaMemcpyAsync(nm, c->d_nmask.p, nn, cudaMemcpyDeviceToDevice, s));
+      k_copy_cvt<float, double><<<gblocks(n), 256, 0, s>>>(minv, c->d_minv.p, n);
+      HX_CHECK_LAUNCH();
+      L.shift = (float)shift;
+    } else {
+      const auto& F = G.lv[l - 1];
+      k_coarse_fac<<<gblocks(ne), 256, 0, s>>>(F.fac.p, fl, F.g, g);
+      HX_CHECK_LAUNCH();
+      k_coarse_bc<<<gblocks(nn), 256, 0, s>>>(F.bc.p, bc, F.g, g);
+      HX_CHECK_LAUNCH();
+      put_state(c, 3, CgState{});
+      launch_node_diag<float>(s, fl, bc, nm, minv, g, make_elem_coef(h[0], h[1], h[2], c->nu),
+                              c->d_partials.p, c->d_state.p + 3, c->d_scalars.p);
+      launch_minv<float>(s, nm, minv, minv, nn, 0.0);
+      HX_CUDA(cudaStreamSynchronize(s));  // the pinned state mirror is reused below
+      L.shift = 0.f;
+    }
+    G.nl = l + 1;
+    const bool even = g.nxe % 2 == 0 && g.nye % 2 == 0 && g.nze % 2 == 0;
+    if (!even || nn <= GMG_COARSE_NODES || g.nxe < 4 || g.nye < 4 || g.nze < 4) break;
+    Grid gc{};
+    gc.nxe = g.nxe / 2;
+    gc.nye = g.nye / 2;
+    gc.nze = g.nze / 2;
+    gc.nxn = gc.nxe + 1;
+    gc.nyn = gc.nye + 1;
+    gc.nzn = gc.nze + 1;
+    g = gc;
+    for (int a = 0; a < 3; ++a) h[a] *= 2.0;
+  }
+  // lambda_max(D^-1 A) of every smoothed level (all but the coarsest):
+  // 12 power iterations each
+  for (int l = 0; l + 1 < G.nl; ++l) {
+    auto& L = G.lv[l];
+    const int64_t nn = L.g.nodes(), n = L.g.dofs();
+    k_rand_vec<<<gblocks(n), 256, 0, s>>>(L.x.p, L.nmask.p, nn);
+    HX_CHECK_LAUNCH();
+    double lam = 1.0;
+    for (int it = 0; it < 12; ++it) {
+      launch_matvec<float>(s, 0, L.x.p, L.q.p, L.fac.p, L.nmask.p, L.g, L.K, L.shift,
+                           c->d_state.p + 3, c->d_partials.p, nullptr);
+      put_state(c, 3, CgState{});
+      k_power_norms<<<gblocks(n), 256, 0, s>>>(L.q.p, L.minv.p, L.x.p, n, c->d_partials.p,
+                                                c->d_state.p + 3, c->d_scalars.p);
+      HX_CHECK_LAUNCH();
+      double nv[2];
+      HX_CUDA(cudaMemcpyAsync(nv, c->d_scalars.p, sizeof(nv), cudaMemcpyDeviceToHost, s));
+      HX_CUDA(cudaStreamSynchronize(s));
+      if (!(nv[1] > 0.0) || !(nv[0] > 0.0)) break;
+      lam = std::sqrt(nv[0] / nv[1]);
+      // next iterate: w / |w|
+      k_scale_copy<<<gblocks(n), 256, 0, s>>>(L.x.p, L.q.p, (float)(1.0 / std::sqrt(nv[0])), n);
+      HX_CHECK_LAUNCH();
+    }
+    L.lmax = (float)lam;
+  }
+  G.coarse_st.ensure(1);
+  G.p0.ensure(G.lv[G.nl - 1].g.dofs());
+  G.p1.ensure(G.lv[G.nl - 1].g.dofs());
+  G.ready = true;
+  HX_CUDA(cudaStreamSynchronize(s));
+}
+
+// Chebyshev smoothing of A x = b on level L (GMG_DEGREE steps): from x = 0
+// when xzero, else from x; leaves r = b - A x when want_residual.
+static void cheb_smooth(hx_ctx* c, hx_ctx::GmgLevel& L, bool xzero, bool want_residual) {
+  cudaStream_t s = c->stream;
+  const int64_t n = L.g.dofs();
+  const unsigned nb = gblocks(n);
+  const float lmax = L.lmax;
+  const float lo = GMG_LO * lmax, hi = GMG_HI * lmax;
+  const float theta = 0.5f * (hi + lo), delta = 0.5f * (hi - lo);
+  const float sigma = theta / delta;
+  auto A = [&](const float* v, float* out) {
+    launch_matvec<float>(s, 0, v, out, L.fac.p, L.nmask.p, L.g, L.K, L.shift, c->d_state.p + 3,
+                         c->d_partials.p, nullptr);
+  };
+  if (!xzero) A(L.x.p, L.q.p);
+  k_cheb_start<<<nb, 256, 0, s>>>(L.b.p, xzero ? nullptr : L.q.p, L.minv.p, L.r.p, L.d.p, L.x.p,
+                                  xzero ? 1 : 0, 1.0f / theta, n);
+  HX_CHECK_LAUNCH();
+  float rho = 1.0f / sigma;
+  for (int k = 1; k < GMG_DEGREE; ++k) {
+    A(L.d.p, L.q.p);
+    const float rho_n = 1.0f / (2.0f * sigma - rho);
+    k_cheb_step<<<nb, 256, 0, s>>>(L.q.p, L.minv.p, L.r.p, L.d.p, L.x.p, rho_n * rho,
+                                   2.0f * rho_n / delta, n);
+    HX_CHECK_LAUNCH();
+    rho = rho_n;
+  }
+  if (want_residual) {
+    A(L.d.p, L.q.p);  // r tracks b - A x: subtract A of the last increment
+    k_sub<<<nb, 256, 0, s>>>(L.r.p, L.q.p, n);
+    HX_CHECK_LAUNCH();
+  }
+}
+
+// z = V(r): one V-cycle on r (FP64 or FP32 DOF vector of level 0).
+// Every launch is on c->stream and needs no host round trip, so the cycle
+// can be captured in a CUDA graph.
+template <typename T>
+void gmg_vcycle(hx_ctx* c, const T* r, T* z) {
+  auto& G = c->gmg;
+  HX_REQUIRE(G.ready, "multigrid hierarchy not set up");
+  cudaStream_t s = c->stream;
+  const int nl = G.nl;
+  {
+    auto& L0 = G.lv[0];
+    const int64_t n = L0.g.dofs();
+    k_copy_cvt<float, T><<<gblocks(n), 256, 0, s>>>(L0.b.p, r, n);
+    HX_CHECK_LAUNCH();
+  }
+  for (int l = 0; l + 1 < nl; ++l) {
+    auto& L = G.lv[l];
+    auto& C = G.lv[l + 1];
+    cheb_smooth(c, L, true, true);
+    launch_restrict(s, 3, L.r.p, C.b.p, node_grid(L.g), node_grid(C.g), false);
+    k_mask3<<<gblocks(3 * C.g.nodes()), 256, 0, s>>>(C.b.p, C.nmask.p, C.g.nodes());
+    HX_CHECK_LAUNCH();
+  }
+  {
+    // coarsest level (the only one for small grids): fixed-count FP32
+    // Jacobi-PCG from zero
+    auto& L = G.lv[nl - 1];
+    const int64_t n = L.g.dofs();
+    CgState* st = G.coarse_st.p;
+    k_coarse_reset<<<1, 32, 0, s>>>(st, GMG_COARSE_ITERS, 1e-4);
+    HX_CHECK_LAUNCH();
+    launch_fill_zero(s, L.x.p, n * sizeof(float));
+    launch_cg_init<float>(s, L.b.p, nullptr, L.minv.p, L.r.p, G.p1.p, n, st, c->d_partials.p);
+    for (int it = 0; it < GMG_COARSE_ITERS; it += 2) {
+      launch_pcg_step<float>(s, G.p1.p, G.p0.p, L.r.p, L.minv.p, L.x.p, L.q.p, L.fac.p,
+                             L.nmask.p, L.g, L.K, L.shift, st, c->d_partials.p);
+      launch_cg_update2<float>(s, L.r.p, L.q.p, L.minv.p, n, st, c->d_partials.p);
+      launch_pcg_step<float>(s, G.p0.p, G.p1.p, L.r.p, L.minv.p, L.x.p, L.q.p, L.fac.p,
+                             L.nmask.p, L.g, L.K, L.shift, st, c->d_partials.p);
+      launch_cg_update2<float>(s, L.r.p, L.q.p, L.minv.p, n, st, c->d_partials.p);
+    }
+    k_coarse_finish<<<gblocks(n), 256, 0, s>>>(L.x.p, G.p0.p, G.p1.p, st, n);
+    HX_CHECK_LAUNCH();
+  }
+  for (int l = nl - 2; l >= 0; --l) {
+    auto& L = G.lv[l];
+    auto& C = G.lv[l + 1];
+    // x_l += P x_{l+1}, masked; then post-smoothing from it
+    launch_prolong(s, C.x.p, L.x.p, node_grid(L.g), node_grid(C.g), true);
+    k_mask3<<<gblocks(3 * L.g.nodes()), 256, 0, s>>>(L.x.p, L.nmask.p, L.g.nodes());
+    HX_CHECK_LAUNCH();
+    cheb_smooth(c, L, false, false);
+  }
+  {
+    auto& L0 = G.lv[0];
+    const int64_t n = L0.g.dofs();
+    k_copy_cvt<T, float><<<gblocks(n), 256, 0, s>>>(z, L0.x.p, n);
+    HX_CHECK_LAUNCH();
+  }
+}
+template void gmg_vcycle<double>(hx_ctx*, const double*, double*);
+template void gmg_vcycle<float>(hx_ctx*, const float*, float*);
+
+template <typename T>
+void launch_fcg_coeffs(cudaStream_t s, const T* z, const T* q_old, const T* r, int64_t n,
+                       double* partials, CgState* st) {
+  k_fcg_coeffs<T><<<gblocks(n), 256, 0, s>>>(z, q_old, r, n, partials, st);
+  HX_CHECK_LAUNCH();
+}
+template void launch_fcg_coeffs<double>(cudaStream_t, const double*, const double*,
+                                        const double*, int64_t, double*, CgState*);
+template void launch_fcg_coeffs<float>(cudaStream_t, const float*, const float*, const float*,
+                                       int64_t, double*, CgState*);
+
+// ---------------------------------------------------------------------------
+// FP64 flexible CG preconditioned by the V-cycle (Notay's FCG, one stored
+// direction, the step kernels of the learned solve).  Convergence on the
+// recursive residual, confirmed on the true one by solve_grid.  With
+// keep_best the best iterate is kept, as the reference's failure handling
+// needs it.
+// ---------------------------------------------------------------------------
+CgState solve_gmg(hx_ctx* c, const double* fac, const double* b, double* x, bool warm,
+                  double shift, const hx_solve_opts& o, double t0, bool* timed_out,
+                  int* iters_out) {
+  const Grid& g = c->g;
+  const int64_t n = g.dofs();
+  gmg_setup(c, fac, shift);
+  double* r = c->d_r.ensure(n);
+  double* P0 = c->d_p.ensure(n);
+  double* P1 = c->d_p2.ensure(n);
+  double* q = c->d_q.ensure(n);
+  double* z = c->gmg.z.ensure(n);
+  double* s64 = c->gmg.s.ensure(n);
+  double* xbest = o.keep_best ? c->d_xbest.ensure(n) : nullptr;
+  const double* minv = c->d_minv.p;
+  CgState* st = c->d_state.p;
+  put_state(c, 0, fresh_state(o.tol, o.max_iter, 1, o.divergence_checks != 0, o.keep_best != 0));
+  if (warm) {
+    launch_matvec<double>(c->stream, 0, x, q, fac, c->d_nmask.p, g, c->K, shift,
+                          c->d_state.p + 3, c->d_partials.p, nullptr);
+    launch_cg_init<double>(c->stream, b, q, minv, r, s64, n, st, c->d_partials.p);
+  } else {
+    launch_fill_zero(c->stream, x, n * sizeof(double));
+    launch_cg_init<double>(c->stream, b, nullptr, minv, r, s64, n, st, c->d_partials.p);
+  }
+  // no previous direction: p_old = q_old = 0 and pq = 0 give beta = 0
+  launch_fill_zero(c->stream, q, n * sizeof(double));
+  launch_fill_zero(c->stream, P1, n * sizeof(double));
+  if (xbest)
+    HX_CUDA(cudaMemcpyAsync(xbest, x, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  CgState s0 = get_state(c, 0);
+  *iters_out = 0;
+  if (s0.status != HX_RUNNING || o.max_iter <= 0) return s0;
+  s0.pq = 0.0;
+  s0.alpha = 0.0;
+  s0.beta = 0.0;
+  put_state(c, 0, s0);
+  auto one = [&](double* pin, double* pout) {
+    gmg_vcycle<double>(c, r, z);
+    launch_fcg_coeffs<double>(c->stream, z, q, r, n, c->d_partials.p, st);
+    launch_fcg_step<double>(c->stream, pin, pout, z, x, q, fac, c->d_nmask.p, g, c->K, shift, st,
+                            c->d_partials.p);
+    launch_cg_update2<double>(c->stream, r, q, minv, n, st, c->d_partials.p);
+    // best-iterate snapshot (the reference's failure handling returns it)
+    if (xbest) launch_axpy_state<double>(c->stream, xbest, x, pout, n, st, 1);
+  };
+  auto body = [&]() {
+    one(P1, P0);
+    one(P0, P1);
+  };
+  const int reps = std::max(1, std::min(8, auto_batch(g, o.check_every) / 2));
+  CgState sf = run_batched(c, 0, reps, body, o.wall_limit_ms, t0, timed_out, 0);
+  if (sf.status != HX_ST_BREAKDOWN && sf.iter > 0) {
+    double* pk = ((sf.iter - 1) % 2 == 0) ? P0 : P1;
+    launch_axpy_state<double>(c->stream, x, x, pk, n, st, 0);
+  }
+  *iters_out = sf.iter;
+  return sf;
+}
+
+}  // namespace hx

@@ -10,6 +10,8 @@
 
 #include "hx_common.cuh"
 
+#define HX_GMG_MAX_LEVELS 10
+
 namespace hx {
 
 struct Grid {
@@ -208,6 +210,24 @@ struct hx_ctx {
   bool f_used = false;
 
   int64_t launches = 0;  // kernels launched on behalf of this context
+
+  // geometric multigrid hierarchy (hx_gmg.cu): FP32 levels, level 0 = the mesh's grid
+  struct GmgLevel {
+    hx::Grid g{};
+    double h[3] = {1, 1, 1};
+    hx::ElemCoef<float> K{};
+    float shift = 0.f, lmax = 1.f;  // operator shift; lambda_max(D^-1 A)
+    hx::DevBuf<float> fac, minv, b, x, r, d, q;
+    hx::DevBuf<uint8_t> bc, nmask;  // BC bits; free-DOF mask (BC and stiffness)
+  };
+  struct Gmg {
+    bool ready = false;
+    int nl = 0;
+    GmgLevel lv[HX_GMG_MAX_LEVELS];
+    hx::DevBuf<hx::CgState> coarse_st;
+    hx::DevBuf<float> p0, p1;   // coarse PCG directions
+    hx::DevBuf<double> z, s;    // FCG: preconditioned residual, scratch
+  } gmg;
 
   // lattice origin of the mesh (the minimum node coordinates; 0 for hx_set_grid)
   double origin[3] = {0, 0, 0};

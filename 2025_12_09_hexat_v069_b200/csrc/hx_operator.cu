@@ -29,6 +29,8 @@
 //    buffers so neighbouring CTAs never read a value another CTA rewrote.
 //    The epilogue applies the free-DOF mask and the shift and reduces p.q
 //    deterministically into the CG state (alpha = rz / pq).
+#include <type_traits>
+
 #include "hx_internal.h"
 
 namespace hx {
@@ -56,21 +58,38 @@ __device__ __forceinline__ unsigned smem_u32(const void* p) {
   return (unsigned)__cvta_generic_to_shared(p);
 }
 
-template <int BYTES>
-__device__ __forceinline__ void cp_async_zfill(unsigned sdst, const void* gsrc, bool valid) {
-  const unsigned n = valid ? BYTES : 0;
-  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(sdst), "l"(gsrc),
-               "n"(BYTES), "r"(n));
+// 16-byte asynchronous copy global -> shared; only the first `bytes`
+// (0..16) are read, the rest of the 16 are zero-filled.
+__device__ __forceinline__ void cp_async16(unsigned sdst, const void* gsrc, unsigned bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sdst), "l"(gsrc),
+               "r"(bytes));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
-// Shared-memory layout (dynamic).  Planes are component-major
-// ([c][row][node]) so the lanes of a warp touch consecutive words.
+// Staging geometry.  A staged row is the 33 nodes i0-1 .. i0+31 of one
+// node row, 99 contiguous values of an interleaved vector.  It is copied in
+// 16-byte chunks (V values) starting at the 16-byte boundary at or below its
+// first value, so a row takes CPR chunks and sits in shared memory with a
+// lead of (first value's index) mod V values, which depends on the row and
+// the plane.  Lanes then read node a, component c of row b at
+// b*RS + lead_b + 3a + c: a stride of 3 words (FP32) or 3 doublewords
+// (FP64) across a warp, free of bank conflicts.
+template <typename T>
+struct Stage {
+  static constexpr int V = 16 / (int)sizeof(T);                // values per chunk
+  static constexpr int ROWV = 3 * (MV_BX + 1);                 // 99 values per row
+  static constexpr int CPR = (ROWV + V - 1 + V - 1) / V;       // chunks per row
+  static constexpr int RS = CPR * V;                           // row stride (values)
+  static_assert(RS >= ROWV + V - 1, "a row with any lead fits its staged chunks");
+};
+
+// Shared-memory layout (dynamic): rows of interleaved values (see Stage).
 template <typename T, int BY, bool FUSED>
 struct OpSmem {
-  static constexpr int PLANE = 3 * (BY + 1) * (MV_BX + 1);
+  static constexpr int PLANE = (BY + 1) * Stage<T>::RS;
+  static_assert((PLANE * sizeof(T)) % 16 == 0, "planes keep 16-byte chunk alignment");
   static constexpr int PF = mv_prefetch<T>();
   static constexpr int NP = PF + 1;             // slots: k, k+1, k+2, k+3 .. k+PF
   static constexpr int NR = FUSED ? PF - 1 : 1;  // slots: k+2 .. k+PF
@@ -149,13 +168,15 @@ template <typename T, int BY, int MODE, int MINB>
 __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
   constexpr bool FUSED = MODE >= 3;
   constexpr int NT = MV_BX * BY;
-  constexpr int PLANE = OpSmem<T, BY, FUSED>::PLANE;
-  constexpr int RW = MV_BX + 1;          // nodes per staged row
-  constexpr int CPL = (BY + 1) * RW;      // staged nodes per component
-  constexpr int NCP = (PLANE + NT - 1) / NT;
+  constexpr int V = Stage<T>::V;
+  constexpr int CPR = Stage<T>::CPR;
+  constexpr int RS = Stage<T>::RS;
+  constexpr int NCH = (BY + 1) * CPR;          // chunks per staged plane
+  constexpr int NCT = (NCH + NT - 1) / NT;     // chunks per thread
   constexpr int PF = OpSmem<T, BY, FUSED>::PF;
   constexpr int NP = OpSmem<T, BY, FUSED>::NP;
   constexpr int NR = OpSmem<T, BY, FUSED>::NR;
+  using VecT = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
   if (MODE >= 2 && A.st->status != HX_RUNNING) return;
   extern __shared__ __align__(16) unsigned char smraw[];
   OpSmem<T, BY, FUSED>& sm = *reinterpret_cast<OpSmem<T, BY, FUSED>*>(smraw);
@@ -170,31 +191,47 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
   const bool out_ok = lx >= 1 && ly >= 1 && in < g.nxn && jn < g.nyn;
   const int64_t nplane = (int64_t)g.nxn * g.nyn;
   const int64_t eplane = (int64_t)g.nxe * g.nye;
+  const int64_t ndof = 3 * nplane * g.nzn;
   T alpha_old = T(0), beta_old = T(0);
   if (FUSED) {
     alpha_old = (T)A.st->alpha;
     beta_old = (T)A.st->beta;
   }
 
-  // Copy assignment, the same for every plane: staged value idx is the
-  // shared index itself, (component c, row b, node a) with a fastest.
-  int goff[NCP];       // offset within a plane (3 * node-in-plane + c)
-  unsigned flags = 0;  // bit q: in grid, bit 8+q: owned node
+  // Chunk assignment, the same for every plane: this thread copies (and, in
+  // the fused modes, transforms) chunks tid, tid + NT, ... of the plane.
+  // row_off = first staged value of the chunk's row, relative to the plane's
+  // first value 3 * kp * nplane (32-bit: the grid extent check bounds it);
+  // a row's owned nodes i0 .. i0+30 (inside the grid) are the own_len values
+  // from row_off + 3; halo rows own none (bit q of own_rows clear).
+  int row_off[NCT];
+  int cbase[NCT];  // shared-memory offset of the chunk: its row's start + ccv
+  int ccv[NCT];    // offset of the chunk within its row (values)
+  unsigned own_rows = 0;
+  const int own_len = 3 * (min(i0 + MV_BX - 1, g.nxn) - i0);
 #pragma unroll
-  for (int q = 0; q < NCP; ++q) {
-    const int idx = tid + q * NT;
-    const int c = idx / CPL, rem = idx - c * CPL;
-    const int b = rem / RW, a = rem - b * RW;
-    const int ii = i0 - 1 + a, jj = j0 - 1 + b;
-    const bool ok = idx < PLANE && ii >= 0 && ii < g.nxn && jj >= 0 && jj < g.nyn;
-    const bool own = ok && a >= 1 && a <= MV_BX - 1 && b >= 1 && b <= BY - 1;
-    goff[q] = ok ? 3 * (jj * g.nxn + ii) + c : 0;
-    flags |= (ok ? 1u : 0u) << q;
-    flags |= (own ? 1u : 0u) << (8 + q);
+  for (int q = 0; q < NCT; ++q) {
+    const int ch = min(tid + q * NT, NCH - 1);
+    const int b = ch / CPR, cc = ch - b * CPR;
+    const int jj = j0 - 1 + b;
+    row_off[q] = 3 * (jj * g.nxn + i0 - 1);
+    if (b >= 1 && b <= BY - 1 && jj < g.nyn) own_rows |= 1u << q;
+    ccv[q] = cc * V;
+    cbase[q] = b * RS + ccv[q];
   }
+  // global index of a chunk's first value in plane kp (a multiple of V)
+  auto chunk_start = [&](int q, int64_t base) -> int64_t {
+    const int64_t o = base + row_off[q];
+    return o - (o & (V - 1)) + ccv[q];
+  };
 
   // One commit group per call, empty for planes past k1, so that the
-  // wait counts below hold to the end of the chunk.
+  // wait counts below hold to the end of the chunk.  Chunks outside the
+  // vectors (planes k0-1 < 0 or nzn, rows before the first value) are
+  // zero-filled; a chunk reaching past the last value copies only its part
+  // inside.  Other values outside the grid (halo nodes beyond a row's end,
+  // halo rows beyond the plane) are copied as they lie in memory: they only
+  // feed element columns with factor 0, whose products are zero.
   auto issue = [&](int kp) {
     if (kp > k1) {
       cp_async_commit();
@@ -207,24 +244,28 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
     const unsigned smv = smem_u32(&sm.m[FUSED ? ring<NR>(kp) : 0][0]);
     const unsigned sx = smem_u32(&sm.x[FUSED ? ring<NR>(kp) : 0][0]);
 #pragma unroll
-    for (int q = 0; q < NCP; ++q) {
-      const int idx = tid + q * NT;
-      if (q == NCP - 1 && idx >= PLANE) continue;
-      const bool ok = kin && ((flags >> q) & 1u);
-      const int64_t gi = ok ? base + goff[q] : 0;
-      const unsigned so = (unsigned)idx * (unsigned)sizeof(T);
-      cp_async_zfill<sizeof(T)>(sp + so, A.pin + gi, ok);
+    for (int q = 0; q < NCT; ++q) {
+      if (q == NCT - 1 && tid + q * NT >= NCH) continue;
+      const int64_t s = chunk_start(q, base);
+      const int64_t left = ndof - s;
+      const unsigned bytes =
+          (kin && s >= 0 && left > 0) ? (unsigned)((left < V ? left : (int64_t)V) * sizeof(T)) : 0u;
+      const int64_t gi = bytes ? s : 0;
+      const unsigned so = (unsigned)cbase[q] * (unsigned)sizeof(T);
+      cp_async16(sp + so, A.pin + gi, bytes);
       if (FUSED) {
-        if (MODE == 3) cp_async_zfill<sizeof(T)>(sr + so, A.r + gi, ok);
-        cp_async_zfill<sizeof(T)>(smv + so, A.minv + gi, ok);
-        cp_async_zfill<sizeof(T)>(sx + so, A.x + gi, ok);
+        if (MODE == 3) cp_async16(sr + so, A.r + gi, bytes);
+        cp_async16(smv + so, A.minv + gi, bytes);
+        cp_async16(sx + so, A.x + gi, bytes);
       }
     }
     cp_async_commit();
   };
 
-  // FUSED: p = M^-1 r + beta p_old (MODE 4: z + beta p_old) in place; owned
-  // nodes of owned planes store p and advance x with the old direction.
+  // FUSED: p = M^-1 r + beta p_old (MODE 4: z + beta p_old) in place, chunk
+  // by chunk; the values of owned nodes of owned planes are stored to p and
+  // advance x with the old direction (16-byte stores where a whole chunk is
+  // owned).
   auto transform = [&](int kp) {
     if (!FUSED) return;
     const bool kown = kp >= k0 && kp < k1;
@@ -234,26 +275,59 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
     const T* ms = &sm.m[ring<NR>(kp)][0];
     const T* xs = &sm.x[ring<NR>(kp)][0];
 #pragma unroll
-    for (int q = 0; q < NCP; ++q) {
-      const int idx = tid + q * NT;
-      if (q == NCP - 1 && idx >= PLANE) continue;
-      const T pold = ps[idx];
-      const T pnew = (MODE == 4 ? ms[idx] : ms[idx] * rs[idx]) + beta_old * pold;
-      ps[idx] = pnew;
-      if (kown && ((flags >> (8 + q)) & 1u)) {
-        const int64_t gi = base + goff[q];
-        A.pout[gi] = pnew;
-        A.x[gi] = xs[idx] + alpha_old * pold;
+    for (int q = 0; q < NCT; ++q) {
+      if (q == NCT - 1 && tid + q * NT >= NCH) continue;
+      const int o = cbase[q];
+      T pnew[V], xv[V];
+      {
+        const VecT pv = *reinterpret_cast<const VecT*>(ps + o);
+        const VecT mv = *reinterpret_cast<const VecT*>(ms + o);
+        const VecT xw = *reinterpret_cast<const VecT*>(xs + o);
+        const T* pa = reinterpret_cast<const T*>(&pv);
+        const T* ma = reinterpret_cast<const T*>(&mv);
+        const T* xa = reinterpret_cast<const T*>(&xw);
+        VecT rv{};
+        if (MODE == 3) rv = *reinterpret_cast<const VecT*>(rs + o);
+        const T* ra = reinterpret_cast<const T*>(&rv);
+#pragma unroll
+        for (int t = 0; t < V; ++t) {
+          pnew[t] = (MODE == 4 ? ma[t] : ma[t] * ra[t]) + beta_old * pa[t];
+          xv[t] = xa[t] + alpha_old * pa[t];
+        }
+      }
+      *reinterpret_cast<VecT*>(ps + o) = *reinterpret_cast<const VecT*>(pnew);
+      if (!kown || !((own_rows >> q) & 1u)) continue;
+      const int64_t s = chunk_start(q, base);
+      const int64_t lo = base + row_off[q] + 3, hi = lo + own_len;
+      if (s >= lo && s + V <= hi) {
+        *reinterpret_cast<VecT*>(A.pout + s) = *reinterpret_cast<const VecT*>(pnew);
+        *reinterpret_cast<VecT*>(A.x + s) = *reinterpret_cast<const VecT*>(xv);
+      } else if (s + V > lo && s < hi) {
+#pragma unroll
+        for (int t = 0; t < V; ++t)
+          if (s + t >= lo && s + t < hi) {
+            A.pout[s + t] = pnew[t];
+            A.x[s + t] = xv[t];
+          }
       }
     }
   };
 
-  auto face = [&](int kp, int c, T (&v)[4]) {
-    const T* ps = &sm.p[ring<NP>(kp)][(c * (BY + 1) + ly) * RW + lx];
-    v[0] = ps[0];
-    v[1] = ps[1];
-    v[2] = ps[RW];
-    v[3] = ps[RW + 1];
+  // Shared-memory offsets of this thread's nodes (lx, ly) and (lx, ly + 1)
+  // in plane kp: row start + the row's lead in that plane (see Stage) + 3 lx.
+  const int rowA = 3 * (jn * g.nxn + i0 - 1), rowB = rowA + 3 * g.nxn;
+  auto offA = [&](int kp) -> int {
+    return ly * RS + (int)(((int64_t)kp * nplane * 3 + rowA) & (V - 1)) + 3 * lx;
+  };
+  auto offB = [&](int kp) -> int {
+    return (ly + 1) * RS + (int)(((int64_t)kp * nplane * 3 + rowB) & (V - 1)) + 3 * lx;
+  };
+  // the four corners (bx + 2 by) of component c of the element face
+  auto face = [&](const T* ps, int a, int b, int c, T (&v)[4]) {
+    v[0] = ps[a + c];
+    v[1] = ps[a + 3 + c];
+    v[2] = ps[b + c];
+    v[3] = ps[b + 3 + c];
   };
 
   // prologue: planes k0-1 .. k0+PF-3 requested (one group each); k0-1 and
@@ -314,6 +388,9 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
     if (ke + 2 <= k1) transform(ke + 2);
     issue(ke + PF);  // into the slot of plane ke-1
 
+    const T* pl0 = &sm.p[ring<NP>(ke)][0];
+    const T* pl1 = &sm.p[ring<NP>(ke + 1)][0];
+    const int a0 = offA(ke), a1 = offA(ke + 1), b1 = offB(ke + 1);
     T U[3][8];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -322,10 +399,10 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
 #pragma unroll
         for (int q = 0; q < 4; ++q) Pb[q] = Pcarry[c][q];
       } else {
-        face(ke, c, v);
+        face(pl0, a0, offB(ke), c, v);
         face_fwd(v, Pb);
       }
-      face(ke + 1, c, v);
+      face(pl1, a1, b1, c, v);
       face_fwd(v, Pt);
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
@@ -334,7 +411,7 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
         U[c][q + 4] = Pt[q] - Pb[q];
       }
     }
-    T rowA[3];
+    T rowS[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       T Y[8];
@@ -344,31 +421,43 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
       T F[4];
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        const T ys = Y[q] * f, yd = Y[q + 4] * f;
-        F[q] = (ys - yd) + Ytp[c][q];
-        Ytp[c][q] = ys + yd;
+        // bottom face: f (Y_s - Y_d) plus the layer below's top face; top
+        // face: f (Y_s + Y_d), carried to the layer above.  (FP32 forms the
+        // sum and difference first, one instruction less; in FP64 that
+        // order needs more live registers than the 128-register bound.)
+        if (sizeof(T) == 4) {
+          F[q] = fma(f, Y[q] - Y[q + 4], Ytp[c][q]);
+          Ytp[c][q] = f * (Y[q] + Y[q + 4]);
+        } else {
+          const T ys = Y[q] * f, yd = Y[q + 4] * f;
+          F[q] = (ys - yd) + Ytp[c][q];
+          Ytp[c][q] = ys + yd;
+        }
       }
       const T as = F[0] - F[2], ad = F[1] - F[3], bs = F[0] + F[2], bd = F[1] + F[3];
       const T c0 = as - ad, c1 = as + ad, c2 = bs - bd, c3 = bs + bd;
       // element lx-1 contributes its +x corners to this thread's nodes
       const T l1 = __shfl_up_sync(0xffffffffu, c1, 1);
       const T l3 = __shfl_up_sync(0xffffffffu, c3, 1);
-      rowA[c] = c0 + l1;
+      rowS[c] = c0 + l1;
       sm.red[ly][c][lx] = c2 + l3;
     }
     __syncthreads();  // B: red of this layer visible
     if (ke >= k0 && out_ok) {
+      // this node's p.q in T (3 terms), accumulated in FP64 across planes
+      T pdot = T(0);
       const int64_t node = (int64_t)ke * nplane + (int64_t)jn * g.nxn + in;
       const unsigned m = PREFETCH ? m_pre : (A.nmask ? A.nmask[node] : 7u);
-      const T* own = &sm.p[ring<NP>(ke)][ly * RW + lx];
+      const T* own = pl0 + a0;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        T v = rowA[c] + sm.red[ly - 1][c][lx];
-        const T xv = own[c * (BY + 1) * RW];
+        T v = rowS[c] + sm.red[ly - 1][c][lx];
+        const T xv = own[c];
         v = ((m >> c) & 1u) ? v + A.shift * xv : T(0);
         A.q[3 * node + c] = v;
-        if (MODE != 0) dsum += (double)xv * (double)v;
+        if (MODE != 0) pdot = fma(xv, v, pdot);
       }
+      if (MODE != 0) dsum += (double)pdot;
     }
   }
 

@@ -454,8 +454,11 @@ hx_status solve_grid(hx_ctx* c, const double* f, const double* fac, double* u,
   const double t0 = now_ms();
   HX_REQUIRE(c->has_mesh, "no mesh: call hx_set_grid or hx_set_mesh first");
   HX_REQUIRE(o.tol > 0, "tol must be > 0");
-  HX_REQUIRE(o.preconditioner == HX_PC_JACOBI || o.preconditioner == HX_PC_LEARNED,
+  HX_REQUIRE(o.preconditioner == HX_PC_JACOBI || o.preconditioner == HX_PC_LEARNED ||
+                 o.preconditioner == HX_PC_MULTIGRID,
              "unknown preconditioner");
+  HX_REQUIRE(o.preconditioner != HX_PC_MULTIGRID || o.precision == HX_PREC_FP64,
+             "the multigrid preconditioner runs with FP64 vectors");
   HX_REQUIRE(o.preconditioner != HX_PC_LEARNED || o.precision == HX_PREC_FP64 ||
                  o.precision == HX_PREC_MIXED32,
              "the learned preconditioner runs with FP64 or FP32 (mixed) vectors");
@@ -476,6 +479,10 @@ hx_status solve_grid(hx_ctx* c, const double* f, const double* fac, double* u,
   bool timed_out = false;
   int total_iters = 0;
   double t_setup = 0;
+  // the reference's Jacobi -> AMG switch (GPUSolver.jl:540-579), with the
+  // multigrid preconditioner in place of the CPU AMG
+  bool use_mg = o.preconditioner == HX_PC_MULTIGRID;
+  bool can_switch = o.ref_retry && o.multigrid_fallback && o.preconditioner == HX_PC_JACOBI;
   for (int attempt = 1; attempt <= attempts; ++attempt) {
     const double ts = now_ms();
     if (attempt == 1) {
@@ -502,6 +509,11 @@ hx_status solve_grid(hx_ctx* c, const double* f, const double* fac, double* u,
       }
       total_iters += its;
       R.fallback_used = fb;
+    } else if (use_mg) {
+      int its = 0;
+      st = solve_gmg(c, fac, b, u, warm, shift, o, t0, &timed_out, &its);
+      total_iters += its;
+      if (o.preconditioner != HX_PC_MULTIGRID) R.fallback_used = 1;
     } else if (o.precision == HX_PREC_FP64) {
       st = pcg_fp64(c, fac, b, u, warm, shift, o, t0, &timed_out);
       total_iters += st.iter;
@@ -533,6 +545,10 @@ hx_status solve_grid(hx_ctx* c, const double* f, const double* fac, double* u,
         st = solve_learned(c, fac, b, u, true, shift, oc, t0, &timed_out, &fb, &its);
         total_iters += its;
         R.fallback_used |= fb;
+      } else if (use_mg) {
+        int its = 0;
+        st = solve_gmg(c, fac, b, u, true, shift, oc, t0, &timed_out, &its);
+        total_iters += its;
       } else {
         st = pcg_fp64(c, fac, b, u, true, shift, oc, t0, &timed_out);
         total_iters += st.iter;
@@ -550,7 +566,8 @@ hx_status solve_grid(hx_ctx* c, const double* f, const double* fac, double* u,
     const bool diverged = st.status == HX_ST_BREAKDOWN || st.status == HX_ST_NONFINITE ||
                           st.status == HX_ST_DIVERGED;
     const bool failed_badly = diverged || st.best_rel > 0.1;
-    if (!failed_badly && st.best_rel < 5e-2) {
+    // with a stronger preconditioner to switch to, stagnation is not accepted
+    if (!failed_badly && !can_switch && st.best_rel < 5e-2) {
       if (o.keep_best)
         HX_CUDA(cudaMemcpyAsync(u, c->d_xbest.p, n * sizeof(double), cudaMemcpyDeviceToDevice,
                                 c->stream));
@@ -559,7 +576,13 @@ hx_status solve_grid(hx_ctx* c, const double* f, const double* fac, double* u,
       R.status = HX_STALLED;
       break;
     }
-    if (failed_badly) {
+    if (failed_badly || (can_switch && st.best_rel > o.tol)) {
+      if (can_switch) {
+        use_mg = true;  // the next attempt runs multigrid-preconditioned
+        can_switch = false;
+      } else if (use_mg && o.preconditioner != HX_PC_MULTIGRID) {
+        use_mg = false;  // multigrid failed too: back to Jacobi, no more switching
+      }
       factor *= 10.0;
     } else {
       if (st.best_rel < global_lowest && o.keep_best) {

@@ -72,6 +72,18 @@ template <typename T>
 hx_status export_webdata(hx_ctx* c, const char* path, const T* dens, const T* l1, const T* pr,
                          float threshold, int iter, float radius, const char* json,
                          int64_t json_len, int64_t* count_out);
+// geometric multigrid (hx_gmg.cu): hierarchy for `fac` (after the Jacobi
+// set-up of the solve), one V-cycle z = V(r), the flexible-CG coefficients
+// of a preconditioned residual, and the FP64 FCG solve it preconditions
+void gmg_setup(hx_ctx* c, const double* fac, double shift);
+template <typename T>
+void gmg_vcycle(hx_ctx* c, const T* r, T* z);
+template <typename T>
+void launch_fcg_coeffs(cudaStream_t s, const T* z, const T* q_old, const T* r, int64_t n,
+                       double* partials, CgState* st);
+CgState solve_gmg(hx_ctx* c, const double* fac, const double* b, double* x, bool warm,
+                  double shift, const hx_solve_opts& o, double t0, bool* timed_out,
+                  int* iters_out);
 // Average time of `reps` launches of one kernel on the last solve's buffers.
 hx_status time_kernel(hx_ctx* c, int kernel, int reps, double* avg_ms);
 }  // namespace hx

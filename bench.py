@@ -504,6 +504,68 @@ def run_c4_loop(args):
     ctx.close()
 
 
+def run_slab(args):
+    """The C1 solve split into z-slabs across the ranks (slab.py): one
+    process per GPU, NCCL for the shared-plane exchange and the scalar
+    all-reduces, the library's operator on each slab, FP64 Jacobi-PCG to
+    rtol 1e-6.  Strong scaling: the whole job solves one system.  Timed as
+    the max over ranks of the device time; not the headline metric."""
+    import importlib
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    ws, rank, local = dist_info()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if ws > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+    else:
+        dist.init_process_group("nccl", store=dist.HashStore(), rank=0, world_size=1,
+                                device_id=dev)
+    hx = importlib.import_module("2025_12_09_hexat_v069_b200")
+    slab_mod = importlib.import_module("2025_12_09_hexat_v069_b200.slab")
+    dims = tuple(args.dims)
+    ctx = hx.Context(local)
+    f, fac, _ = c1_inputs(hx, ctx, dims)
+    _, _, bc, _ = hx.workloads.cantilever(*dims, with_elements=False)
+    S = slab_mod.Slab(dims, rank, ws)
+    fac_l = torch.from_numpy(fac[S.elem_slice()].copy()).to(dev)
+    op = slab_mod.DeviceSlabOperator(S, fac_l)
+    # the slab's partial diagonal from the library (hx_diagonal on the slab grid)
+    ctx.set_grid(dims[0], dims[1], S.nzl)
+    ctx.set_material(1.0, 0.3)
+    diag_l = torch.from_numpy(ctx.diagonal(fac[S.elem_slice()], S.n)).to(dev)
+    free = torch.from_numpy((~(np.asarray(bc) > 0)).reshape(-1)[S.node_slice()]
+                            .astype(np.float64)).to(dev)
+    b = torch.from_numpy(f[S.node_slice()].copy()).to(dev)
+    for _ in range(args.warmup):
+        slab_mod.pcg(S, dist, op, diag_l, free, b, tol=1e-6, max_iter=5)
+    torch.cuda.synchronize()
+    dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    its, rel = [], 0.0
+    for _ in range(args.steps):
+        u, it, rel, _ = slab_mod.pcg(S, dist, op, diag_l, free, b, tol=1e-6, max_iter=100000)
+        its.append(it)
+    e1.record()
+    e1.synchronize()
+    dist.barrier()
+    t = max_over_ranks(e0.elapsed_time(e1) / 1e3, ws, dev) / args.steps
+    if rank == 0:
+        print(json.dumps({"metric": "s per C1 FP64 Jacobi-PCG solve, z-slab split", "value": t,
+                          "unit": "s/solve", "n_gpus": ws, "steps": args.steps,
+                          "warmup": args.warmup, "ms_per_step": t * 1e3,
+                          "higher_is_better": False, "scaling": "strong", "vs_baseline": None,
+                          "dtype": "f64", "data": "synthetic (C1 density construction)",
+                          "config": {"workload": f"C1 cantilever {dims}, z-slabs of "
+                                                 f"{S.nzl}+ element planes per rank",
+                                     "iterations": its[-1], "rel_res": rel}}), flush=True)
+    ctx.close()
+    dist.destroy_process_group()
+
+
 def run_reference(args):
     ws, rank, local = dist_info()
     if rank != 0:
@@ -553,8 +615,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-variants", action="store_true",
                     help="skip the mixed / learned solver forms")
-    ap.add_argument("--workload", choices=["c1-solve", "c4-loop"], default="c1-solve",
-                    help="c4-loop: the MBB optimisation loop comparison (not the headline)")
+    ap.add_argument("--workload", choices=["c1-solve", "c4-loop", "c1-slab"],
+                    default="c1-solve",
+                    help="c4-loop: the MBB optimisation loop comparison; c1-slab: one C1 "
+                         "solve split into z-slabs across the ranks (neither is the headline)")
     ap.add_argument("--oc-iters", type=int, default=200)
     ap.add_argument("--dims", type=int, nargs=3, default=list(DIMS),
                     help="grid size; other than 320 160 160 only for profiling")
@@ -563,6 +627,8 @@ def main():
         run_reference(args)
     elif args.workload == "c4-loop":
         run_c4_loop(args)
+    elif args.workload == "c1-slab":
+        run_slab(args)
     else:
         run_ours(args)
 

@@ -56,7 +56,10 @@ typedef enum hx_precision {
 typedef enum hx_preconditioner {
   HX_PC_JACOBI = 0,
   HX_PC_LEARNED = 1, /* CNN preconditioner inside flexible CG (needs weights) */
-  HX_PC_NONE = 2
+  HX_PC_NONE = 2,
+  HX_PC_MULTIGRID = 3 /* geometric multigrid V-cycle (FP32) inside flexible CG
+                         (FP64 vectors): the GPU replacement of the reference's
+                         CPU algebraic multigrid (GPUSolver.jl:168-268) */
 } hx_preconditioner;
 
 typedef struct hx_solve_opts {
@@ -77,7 +80,11 @@ typedef struct hx_solve_opts {
   int32_t divergence_checks; /* 1: explosion and 100x-over-best checks */
   int32_t verify_true_residual; /* 1: recompute ||b-Au|| in FP64 at the end */
   int32_t learned_no_fallback; /* 1: learned FCG without the Jacobi fallback */
-  int32_t reserved[5];
+  int32_t multigrid_fallback;  /* 1 (with ref_retry): after a failed or stagnated
+                                  Jacobi attempt switch to HX_PC_MULTIGRID, as the
+                                  reference's "jacobi_amg" switches to AMG
+                                  (GPUSolver.jl:540-579) */
+  int32_t reserved[4];
 } hx_solve_opts;
 
 typedef struct hx_solve_report {
@@ -88,7 +95,8 @@ typedef struct hx_solve_report {
                            residual was still above tol when the recursive
                            one converged (ref_retry = 0 only) */
   int32_t attempts;     /* retry attempts used (ref_retry) */
-  int32_t fallback_used;/* learned -> Jacobi fallback taken */
+  int32_t fallback_used;/* a fallback preconditioner finished the solve:
+                           learned -> Jacobi, or Jacobi -> multigrid */
   int32_t zero_rhs;     /* 1: ||f_free|| == 0, u = 0 returned */
   double rel_res;       /* recursive residual at stop (reference final_rel_res) */
   double true_rel_res;  /* ||b - (K+sI)u|| / ||b|| recomputed in FP64 */
@@ -200,7 +208,11 @@ HX_API hx_status hx_solve_device(hx_ctx *ctx, const double *f_dev,
  * src/Solvers/IterativeSolver.jl:27-39).  Elements with density <
  * min_stiffness_threshold are inactive (GPUSolver.jl:128); factor =
  * E*density (:147).  u_guess may be NULL (cold start).  Writes x_full
- * (3*n_nodes), *final_rel_res and the preconditioner name. */
+ * (3*n_nodes), *final_rel_res and the preconditioner name.  Failure
+ * handling as the reference's with its default preconditioner "jacobi_amg"
+ * (configs/default.yaml:191): three attempts with shift escalation, and
+ * after a failed or stagnated Jacobi attempt the geometric multigrid
+ * preconditioner in place of the CPU AMG (prec_name "GMG"). */
 HX_API hx_status hx_solve_system_gpu(
     hx_ctx *ctx, const float *nodes, int64_t n_nodes, const int64_t *elements,
     int64_t n_elem, float E, float nu, const float *bc_indicator,
