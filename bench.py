@@ -130,10 +130,11 @@ def c1_inputs(hx, ctx, dims=DIMS):
 
 
 FORMS = {"fp64_jacobi": (0, 0), "mixed32_jacobi": (1, 0), "fp64_learned_fcg": (0, 1),
-         "mixed32_learned_fcg": (1, 1)}
+         "mixed32_learned_fcg": (1, 1), "fp64_multigrid_fcg": (0, 3)}
 DTYPES = {"fp64_jacobi": "f64", "mixed32_jacobi": "f32 in f64 reliable updates",
           "fp64_learned_fcg": "f64 vectors, bf16 network",
-          "mixed32_learned_fcg": "f32 vectors in f64 reliable updates, bf16 network"}
+          "mixed32_learned_fcg": "f32 vectors in f64 reliable updates, bf16 network",
+          "fp64_multigrid_fcg": "f64 vectors, f32 V-cycle"}
 
 
 def run_ours(args):
@@ -352,8 +353,8 @@ class OracleResidual:
 def variants(hx, ctx, f, fac, f_d, fac_d, lib_stream, dims=DIMS):
     """The solver forms on the same workload, each timed once on the device
     after one untimed run: FP64 and mixed (FP32 in FP64 reliable updates)
-    Jacobi-PCG, and flexible CG with the shipped learned preconditioner in
-    FP64 and mixed.  Errors of u, compliance f.u and max von Mises stress
+    Jacobi-PCG, flexible CG with the shipped learned preconditioner in FP64
+    and mixed, and flexible CG with the geometric multigrid V-cycle.  Errors of u, compliance f.u and max von Mises stress
     against the FP64 Jacobi-PCG solution, and each solution's relative
     residual recomputed on the host by the oracle (oracle_true_rel_res)."""
     import importlib
