@@ -341,6 +341,7 @@ HX_API void hx_destroy(hx_ctx* c) {
   for (int i = 0; i < 2; ++i) {
     if (c->net.side[i]) cudaStreamDestroy(c->net.side[i]);
     if (c->net.ev_join[i]) cudaEventDestroy(c->net.ev_join[i]);
+    if (c->net.ev_x[i]) cudaEventDestroy(c->net.ev_x[i]);
   }
   if (c->net.ev_fork) cudaEventDestroy(c->net.ev_fork);
   if (c->stream) cudaStreamDestroy(c->stream);

@@ -258,9 +258,10 @@ struct hx_ctx {
       hx::DevBuf<__nv_bfloat16> x0, y, act[7];  // network input, output, training activations
       hx::DevBuf<__nv_bfloat16> pp[2];          // application ping-pong (levels >= 2)
     } lv[8];
-    // side streams and events: the coarser levels' networks run beside level 1
+    // side streams and events: the coarser networks run beside the finest;
+    // ev_x[i]: side i's level restricted, ev_join[i]: its correction summed
     cudaStream_t side[2] = {nullptr, nullptr};
-    cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
+    cudaEvent_t ev_fork = nullptr, ev_x[2] = {nullptr, nullptr}, ev_join[2] = {nullptr, nullptr};
     hx::DevBuf<double> z, scal, facbuf;
     hx::DevBuf<float> z32, s32;  // mixed-precision FCG: preconditioned vector, scratch
     hx::DevBuf<__nv_bfloat16> ys;  // FCG: BF16(D^-1/2 r), n + 8 entries

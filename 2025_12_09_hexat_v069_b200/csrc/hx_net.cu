@@ -145,6 +145,7 @@ void net_buffers(hx_ctx* c, bool train) {
     for (int i = 0; i < 2; ++i) {
       HX_CUDA(cudaStreamCreateWithFlags(&N.side[i], cudaStreamNonBlocking));
       HX_CUDA(cudaEventCreateWithFlags(&N.ev_join[i], cudaEventDisableTiming));
+      HX_CUDA(cudaEventCreateWithFlags(&N.ev_x[i], cudaEventDisableTiming));
     }
   }
   if (train) {
@@ -235,45 +236,66 @@ void precond_z(hx_ctx* c, const T* r, const T* minv, CgState* st, double scale_m
     ys = y;
   }
   launch_restrict_ys(c->stream, ys, st, scale_mul, N.lv[1].x.p, gl[0], gl[1]);
-  for (int l = 2; l <= NET_TOP; ++l)
-    launch_restrict(c->stream, 3, N.lv[l - 1].x.p, N.lv[l].x.p, gl[l - 1], gl[l], false);
   if (train) {
+    for (int l = 2; l <= NET_TOP; ++l)
+      launch_restrict(c->stream, 3, N.lv[l - 1].x.p, N.lv[l].x.p, gl[l - 1], gl[l], false);
     for (int l = NET_TOP; l >= NET_L0; --l) {
       auto& L = N.lv[l];
       launch_lift(c->stream, L.x.p, L.feat.p, L.x0.p, nodes_of(gl[l]));
       stack_forward_train(c, l - NET_L0, gl[l], L.x0.p, L.act, L.y.p);
     }
+    // acc_l = E_l^T y_l (network levels) + R^T acc_{l+1}, coarsest first
+    for (int l = NET_TOP; l >= NET_L0; --l) {
+      auto& L = N.lv[l];
+      launch_unlift(c->stream, L.y.p, L.feat.p, L.acc.p, false, nodes_of(gl[l]));
+      if (l < NET_TOP)
+        launch_prolong(c->stream, N.lv[l + 1].acc.p, L.acc.p, gl[l], gl[l + 1], true);
+    }
   } else {
-    // the coarser networks on side streams, the finest on the main one
-    // (fork/join by events; inside a stream capture these become parallel
-    // branches of the graph)
+    for (int l = 2; l <= NET_L0; ++l)
+      launch_restrict(c->stream, 3, N.lv[l - 1].x.p, N.lv[l].x.p, gl[l - 1], gl[l], false);
+    // Each coarser network on its own side stream, the finest on the main
+    // one; a side stream also restricts its level's input (after its finer
+    // neighbour's, event ev_x) and sums its coarser neighbour's correction
+    // into its own (after ev_join of that neighbour), so that only the
+    // finest level's transfers stay on the main stream.  Inside a stream
+    // capture the events become edges between parallel graph branches.
     HX_CUDA(cudaEventRecord(N.ev_fork, c->stream));
     for (int l = NET_L0 + 1; l <= NET_TOP; ++l) {
       const int side = l - NET_L0 - 1;
       cudaStream_t ss = N.side[side];
       auto& L = N.lv[l];
-      HX_CUDA(cudaStreamWaitEvent(ss, N.ev_fork, 0));
+      HX_CUDA(cudaStreamWaitEvent(ss, side == 0 ? N.ev_fork : N.ev_x[side - 1], 0));
+      launch_restrict(ss, 3, N.lv[l - 1].x.p, L.x.p, gl[l - 1], gl[l], false);
+      if (l < NET_TOP) HX_CUDA(cudaEventRecord(N.ev_x[side], ss));
       launch_lift(ss, L.x.p, L.feat.p, L.x0.p, nodes_of(gl[l]));
       stack_apply(c, ss, l - NET_L0, gl[l], L.x0.p, L.y.p, L.pp[0].p, L.pp[1].p);
+    }
+    // corrections, coarsest first: acc_l = E_l^T y_l + R^T acc_{l+1}
+    for (int l = NET_TOP; l > NET_L0; --l) {
+      const int side = l - NET_L0 - 1;
+      cudaStream_t ss = N.side[side];
+      auto& L = N.lv[l];
+      launch_unlift(ss, L.y.p, L.feat.p, L.acc.p, false, nodes_of(gl[l]));
+      if (l < NET_TOP) {
+        HX_CUDA(cudaStreamWaitEvent(ss, N.ev_join[side + 1], 0));
+        launch_prolong(ss, N.lv[l + 1].acc.p, L.acc.p, gl[l], gl[l + 1], true);
+      }
       HX_CUDA(cudaEventRecord(N.ev_join[side], ss));
     }
     auto& L1 = N.lv[NET_L0];
     launch_lift(c->stream, L1.x.p, L1.feat.p, L1.x0.p, nodes_of(gl[NET_L0]));
     stack_apply(c, c->stream, 0, gl[NET_L0], L1.x0.p, L1.y.p, N.tmp[0].p, N.tmp[1].p);
-    for (int l = NET_L0 + 1; l <= NET_TOP; ++l)
-      HX_CUDA(cudaStreamWaitEvent(c->stream, N.ev_join[l - NET_L0 - 1], 0));
-  }
-  // acc_l = E_l^T y_l (network levels) + R^T acc_{l+1}, coarsest first
-  for (int l = NET_TOP; l >= 1; --l) {
-    auto& L = N.lv[l];
-    if (l >= NET_L0) {
-      launch_unlift(c->stream, L.y.p, L.feat.p, L.acc.p, false, nodes_of(gl[l]));
-      if (l < NET_TOP)
-        launch_prolong(c->stream, N.lv[l + 1].acc.p, L.acc.p, gl[l], gl[l + 1], true);
-    } else {
-      launch_prolong(c->stream, N.lv[l + 1].acc.p, L.acc.p, gl[l], gl[l + 1], false);
+    launch_unlift(c->stream, L1.y.p, L1.feat.p, L1.acc.p, false, nodes_of(gl[NET_L0]));
+    if (NET_TOP > NET_L0) {
+      HX_CUDA(cudaStreamWaitEvent(c->stream, N.ev_join[0], 0));
+      launch_prolong(c->stream, N.lv[NET_L0 + 1].acc.p, L1.acc.p, gl[NET_L0], gl[NET_L0 + 1],
+                     true);
     }
   }
+  // levels below the networks: acc_l = R^T acc_{l+1}
+  for (int l = NET_L0 - 1; l >= 1; --l)
+    launch_prolong(c->stream, N.lv[l + 1].acc.p, N.lv[l].acc.p, gl[l], gl[l + 1], false);
   launch_net_output<T>(c->stream, r, minv, N.lv[1].acc.p, gl[0], gl[1], st, scale_mul, z, q_old,
                        c->d_partials.p);
 }
