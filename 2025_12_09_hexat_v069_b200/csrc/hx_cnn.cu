@@ -13,6 +13,8 @@
 // one tap per warp at a time; partials summed across CTAs in a fixed order.
 #include <cuda_bf16.h>
 
+#include <type_traits>
+
 #include "hx_cnn.h"
 
 namespace hx {
@@ -365,93 +367,137 @@ __global__ void __launch_bounds__(256)
 
 // The same level-1 field from ys = BF16(D^-1/2 v) (k_cg_update2 writes it
 // with the residual): out = k R ys.  One CTA per (x-chunk of <= RES_CX
-// cells, block of YS_JB coarse y-rows j0.., coarse plane k): the fine rows
-// 2j0-1 .. 2(j0+YS_JB-1)+1 of planes 2k-1 .. 2k+1 (clamped to the grid) are
-// staged with 16-byte cp.async chunks, each row from the chunk holding its
+// cells, block of YS_JB coarse y-rows j0.., segment of kseg coarse planes)
+// marches up the fine planes of its segment, so that each fine row is read
+// once per segment (the y-rows shared with the neighbouring blocks and the
+// plane below the segment are read twice).  Per fine plane p the rows
+// 2j0-1 .. 2(j0+YS_JB-1)+1 (clamped to the grid) are staged with 16-byte
+// cp.async chunks into a ring of YS_RING slots, planes p+1 .. p+YS_RING-1
+// in flight while p is used; each row is copied from the chunk holding its
 // first entry (a shift of 0-7 entries; the last chunk may reach 7 entries
-// past n, so ys holds n + 8 entries); each coarse row is then collapsed in
-// y and z per fine DOF and weighted in x.
+// past n, so ys holds n + 8 entries).  Plane p is collapsed in y per fine
+// DOF of each coarse row (S_p) and added into the z-sums of its coarse
+// planes: A_k = 0.5 S_{2k-1} + S_{2k} + 0.5 S_{2k+1} (two buffers, k even
+// and odd); a finished A_k is weighted in x and stored.
 constexpr int YS_JB = 4;
 constexpr int YS_NY = 2 * YS_JB + 1;  // staged fine y-rows per plane
+constexpr int YS_RING = 4;            // staged planes: the one in use and 3 ahead
+
+__device__ __forceinline__ int ys_chunks(int cxw) { return 3 * (2 * cxw + 1) / 8 + 3; }
 
 __global__ void __launch_bounds__(256)
     k_restrict_ys(const __nv_bfloat16* __restrict__ ys, const CgState* sst, double scale_mul,
-                  float* __restrict__ out, GridN gf, GridN gc, int cxw) {
+                  float* __restrict__ out, GridN gf, GridN gc, int cxw, int kseg) {
   extern __shared__ __align__(16) unsigned char rsm[];
   const int seg = 3 * (2 * cxw + 1);
-  const int segc = seg / 8 + 3;  // 16-byte chunks per staged row
-  uint4* sc = reinterpret_cast<uint4*>(rsm);                   // [3][YS_NY][segc]
-  float* srow = reinterpret_cast<float*>(sc + 3 * YS_NY * segc);  // [YS_JB][seg]
+  const int segc = ys_chunks(cxw);  // 16-byte chunks per staged row
+  uint4* sc = reinterpret_cast<uint4*>(rsm);                          // [YS_RING][YS_NY][segc]
+  float* acc = reinterpret_cast<float*>(sc + YS_RING * YS_NY * segc);  // [2][YS_JB][seg]
   const int cx0 = blockIdx.x * cxw, w = min(cxw, gc.nx - cx0);
-  const int j0 = blockIdx.y * YS_JB, k = blockIdx.z;
+  const int j0 = blockIdx.y * YS_JB;
   const int jn = min(YS_JB, gc.ny - j0);  // coarse rows of this block
+  const int k0 = blockIdx.z * kseg, k1 = min(k0 + kseg, gc.nz);
   const int fxa = max(2 * cx0 - 1, 0);
   const int fxb = min(2 * (cx0 + w - 1) + 1, gf.nx - 1);
   const int L = 3 * (fxb - fxa + 1);
   const int fy_lo = max(2 * j0 - 1, 0);
   const int fy_hi = min(2 * (j0 + jn - 1) + 1, gf.ny - 1);
   const int ny_r = fy_hi - fy_lo + 1;  // <= YS_NY
+  // fine planes of the segment: 2k0-1 .. 2k1-1, clipped to the grid
+  const int pa = max(2 * k0 - 1, 0), pb = min(2 * k1 - 1, gf.nz - 1);
+  const int np = pb - pa + 1;
   const uint4* yc = reinterpret_cast<const uint4*>(ys);
-  // one flat loop over (staged row, chunk) so that every thread copies
-  for (int u = threadIdx.x; u < 3 * ny_r * segc; u += blockDim.x) {
-    const int t = u / segc, cu = u - t * segc;
-    const int dz = t / ny_r - 1, yy = t - (dz + 1) * ny_r;
-    const int fz = min(max(2 * k + dz, 0), gf.nz - 1);
-    const int64_t e0 = 3 * (((int64_t)fz * gf.ny + fy_lo + yy) * gf.nx + fxa);
-    const int64_t c0 = e0 >> 3, c1 = (e0 + L + 7) >> 3;
-    if (cu < c1 - c0)
-      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(
-                       (unsigned)__cvta_generic_to_shared(sc + ((dz + 1) * YS_NY + yy) * segc + cu)),
-                   "l"(yc + c0 + cu));
-  }
-  asm volatile("cp.async.commit_group;\n" ::);
-  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-  __syncthreads();
-  const __nv_bfloat16* sy = reinterpret_cast<const __nv_bfloat16*>(sc);
-  for (int jj = 0; jj < jn; ++jj) {
-    const int j = j0 + jj;
-    // the 9 (dz, dy) rows of coarse row j: staged index and weight (0 outside the grid)
-    int off[9];
-    float rw[9];
+  auto stage = [&](int p, int slot) {
+    for (int u = threadIdx.x; u < ny_r * segc; u += blockDim.x) {
+      const int yy = u / segc, cu = u - yy * segc;
+      const int64_t e0 = 3 * (((int64_t)p * gf.ny + fy_lo + yy) * gf.nx + fxa);
+      const int64_t c0 = e0 >> 3, c1 = (e0 + L + 7) >> 3;
+      if (cu < c1 - c0)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(
+                         (unsigned)__cvta_generic_to_shared(sc + (slot * YS_NY + yy) * segc + cu)),
+                     "l"(yc + c0 + cu));
+    }
+  };
 #pragma unroll
-    for (int dz = -1; dz <= 1; ++dz)
+  for (int i = 0; i < YS_RING - 1; ++i) {
+    if (i < np) stage(pa + i, i);
+    asm volatile("cp.async.commit_group;\n" ::);
+  }
+  const float kc = (float)field_coef(sst, nullptr, 0, scale_mul);
+  const __nv_bfloat16* sy = reinterpret_cast<const __nv_bfloat16*>(sc);
+  // x-weights of finished coarse plane k (buffer k & 1), stored
+  auto finish = [&](int k) {
+    const float* A = acc + (k & 1) * YS_JB * seg;
+    for (int e = threadIdx.x; e < 3 * w * jn; e += blockDim.x) {
+      const int jj = e / (3 * w), ex = e - jj * 3 * w;
+      const int cl = ex / 3, c = ex - 3 * cl;
+      const int fx = 2 * (cx0 + cl);
+      const int l = fx - fxa;
+      const float* sr = A + jj * seg;
+      float a = sr[3 * l + c];
+      if (fx >= 1) a += 0.5f * sr[3 * (l - 1) + c];
+      if (fx + 1 < gf.nx) a += 0.5f * sr[3 * (l + 1) + c];
+      out[3 * (((int64_t)k * gc.ny + j0 + jj) * gc.nx + cx0) + ex] = kc * a;
+    }
+  };
+  for (int i = 0; i < np; ++i) {
+    const int p = pa + i, slot = i % YS_RING;
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(YS_RING - 2) : "memory");
+    __syncthreads();  // plane p landed for every thread; slot of plane p-1 free
+    if (i + YS_RING - 1 < np) stage(p + YS_RING - 1, (i + YS_RING - 1) % YS_RING);
+    asm volatile("cp.async.commit_group;\n" ::);
+    const int kp = p >> 1;     // p = 2 kp (+1)
+    const bool odd = p & 1;
+    // odd p: A_kp (if in the segment) += 0.5 S, A_{kp+1} (if in it) = 0.5 S;
+    // even p: A_kp += S, or = S on the grid's first plane
+    const bool add_lo = odd ? kp >= k0 : kp > 0;
+    const bool set_hi = odd && kp + 1 < k1;
+    const float wz = odd ? 0.5f : 1.f;
+    float* Alo = acc + (kp & 1) * YS_JB * seg;
+    float* Ahi = acc + ((kp + 1) & 1) * YS_JB * seg;
+    for (int jj = 0; jj < jn; ++jj) {
+      // the 3 fine rows of coarse row j: staged offset and weight
+      int off[3];
+      float rw[3];
 #pragma unroll
       for (int dy = -1; dy <= 1; ++dy) {
-        const int q = (dz + 1) * 3 + (dy + 1);
-        const int fz0 = 2 * k + dz, fy0 = 2 * j + dy;
-        const bool ok = fz0 >= 0 && fz0 < gf.nz && fy0 >= 0 && fy0 < gf.ny;
+        const int fy0 = 2 * (j0 + jj) + dy;
+        const bool ok = fy0 >= 0 && fy0 < gf.ny;
         const int yy = min(max(fy0, fy_lo), fy_hi) - fy_lo;
-        const int fz = min(max(fz0, 0), gf.nz - 1);
-        const int64_t e0 = 3 * (((int64_t)fz * gf.ny + fy_lo + yy) * gf.nx + fxa);
-        off[q] = 8 * ((dz + 1) * YS_NY + yy) * segc + (int)(e0 & 7);
-        rw[q] = ok ? fw(dz) * fw(dy) : 0.f;
+        const int64_t e0 = 3 * (((int64_t)p * gf.ny + fy_lo + yy) * gf.nx + fxa);
+        off[dy + 1] = 8 * (slot * YS_NY + yy) * segc + (int)(e0 & 7);
+        rw[dy + 1] = ok ? wz * fw(dy) : 0.f;
       }
-    float* sr = srow + jj * seg;
-    for (int dl = threadIdx.x; dl < L; dl += blockDim.x) {
-      float acc = 0.f;
+      for (int dl = threadIdx.x; dl < L; dl += blockDim.x) {
+        float v = 0.f;
 #pragma unroll
-      for (int q = 0; q < 9; ++q) acc += rw[q] * __bfloat162float(sy[off[q] + dl]);
-      sr[dl] = acc;
+        for (int q = 0; q < 3; ++q) v += rw[q] * __bfloat162float(sy[off[q] + dl]);
+        const int o = jj * seg + dl;
+        Alo[o] = add_lo ? Alo[o] + v : v;
+        if (set_hi) Ahi[o] = v;
+      }
+    }
+    // a coarse plane is complete after its top fine plane 2k+1, or after
+    // plane 2k when that is the grid's last
+    const int kdone = odd ? kp : (p == gf.nz - 1 ? kp : -1);
+    if (kdone >= k0) {
+      __syncthreads();
+      finish(kdone);
     }
   }
-  __syncthreads();
-  const float kc = (float)field_coef(sst, nullptr, 0, scale_mul);
-  for (int e = threadIdx.x; e < 3 * w * jn; e += blockDim.x) {
-    const int jj = e / (3 * w), ex = e - jj * 3 * w;
-    const int cl = ex / 3, c = ex - 3 * cl;
-    const int fx = 2 * (cx0 + cl);
-    const int l = fx - fxa;
-    const float* sr = srow + jj * seg;
-    float a = sr[3 * l + c];
-    if (fx >= 1) a += 0.5f * sr[3 * (l - 1) + c];
-    if (fx + 1 < gf.nx) a += 0.5f * sr[3 * (l + 1) + c];
-    out[3 * (((int64_t)k * gc.ny + j0 + jj) * gc.nx + cx0) + ex] = kc * a;
-  }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+static int ys_kseg(const GridN& gc, int cxw) {
+  const int64_t cols = cdiv(gc.nx, cxw) * cdiv(gc.ny, YS_JB);
+  const int64_t want = 4LL * sm_count();  // CTAs: 4 per SM
+  const int64_t segs = std::max<int64_t>(1, std::min<int64_t>(gc.nz, cdiv(want, cols)));
+  return (int)cdiv(gc.nz, segs);
 }
 
 static size_t restrict_ys_smem(int cxw) {
   const size_t seg = 3 * (2 * (size_t)cxw + 1);
-  return 3 * YS_NY * (seg / 8 + 3) * 16 + YS_JB * seg * sizeof(float);
+  return (size_t)YS_RING * YS_NY * (seg / 8 + 3) * 16 + 2 * YS_JB * seg * sizeof(float);
 }
 
 // Prolongation, the exact transpose of k_restrict (without normalisation):
@@ -578,40 +624,84 @@ __global__ void __launch_bounds__(256)
     }
   }
   __syncthreads();
-  // the (up to) 4 fine rows, each L DOFs: a thread takes the same DOF
-  // offset in every row (12 loads in flight); rows past the grid are read at
-  // row 0 and not stored
+  // the (up to) 4 fine rows, each L DOFs from DOF rowb[q]: a thread takes
+  // the same 16-byte chunk offset in every row (12 vector loads in flight).
+  // Chunks are aligned in the vectors, so a row's first and last chunks
+  // hold DOFs of the neighbouring rows: those are loaded but neither used
+  // nor stored.  The vectors' last chunk may reach past n: it is read per
+  // DOF.  Rows past the grid are read at row 0 and not stored.
+  constexpr int V = 16 / (int)sizeof(T);
+  using VecT = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
   const int fx0 = 2 * cx0;
   const int L = 3 * (min(2 * (cx0 + w), gf.nx) - fx0);
-  int64_t rowb[4];
+  const int64_t nv = 3 * ((int64_t)gf.nx * gf.ny * gf.nz);
+  int64_t rowb[4], cb[4];
   bool rowok[4];
+  int nch = 0;
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     const int fy = 2 * j + (q & 1), fz = 2 * k + (q >> 1);
     rowok[q] = fy < gf.ny && fz < gf.nz;
     rowb[q] = rowok[q] ? 3 * (((int64_t)fz * gf.ny + fy) * gf.nx + fx0) : rowb[0];
+    cb[q] = rowb[q] / V;
+    nch = max(nch, (int)((rowb[q] + L + V - 1) / V - cb[q]));
   }
   const float sf = (float)s;
   T zq = T(0), zr = T(0);  // per-thread partials in the vectors' precision
-  for (int dl = threadIdx.x; dl < L; dl += blockDim.x) {
-    const int fl = dl / 3, c = dl - 3 * fl;
-    const int ce = 3 * (fl >> 1) + c;
-    T mv[4], rv[4], qv[4];
+  for (int ch = threadIdx.x; ch < nch; ch += blockDim.x) {
+    T mv[4][V], rv[4][V], qv[4][V];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      mv[q] = minv[rowb[q] + dl];
-      rv[q] = r[rowb[q] + dl];
-      qv[q] = q_old ? q_old[rowb[q] + dl] : T(0);
+      const int64_t d0 = (cb[q] + ch) * V;
+      if (d0 + V <= nv) {
+        *reinterpret_cast<VecT*>(mv[q]) = *reinterpret_cast<const VecT*>(minv + d0);
+        *reinterpret_cast<VecT*>(rv[q]) = *reinterpret_cast<const VecT*>(r + d0);
+        if (q_old)
+          *reinterpret_cast<VecT*>(qv[q]) = *reinterpret_cast<const VecT*>(q_old + d0);
+        else
+#pragma unroll
+          for (int e = 0; e < V; ++e) qv[q][e] = T(0);
+      } else {
+#pragma unroll
+        for (int e = 0; e < V; ++e) {
+          const bool in = d0 + e < nv;
+          mv[q][e] = in ? minv[d0 + e] : T(0);
+          rv[q][e] = in ? r[d0 + e] : T(0);
+          qv[q][e] = (in && q_old) ? q_old[d0 + e] : T(0);
+        }
+      }
     }
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       if (!rowok[q]) continue;
-      const float a = (fl & 1) ? 0.5f * (cyz[q][ce] + cyz[q][ce + 3]) : cyz[q][ce];
-      // the correction is BF16-accurate: formed in FP32
-      const T zi = mv[q] * rv[q] + (T)(sf * dinv_sqrt((float)mv[q]) * a);
-      z[rowb[q] + dl] = zi;
-      zq += zi * qv[q];
-      zr += zi * rv[q];
+      const int64_t d0 = (cb[q] + ch) * V;
+      T zo[V];
+      bool whole = true;
+#pragma unroll
+      for (int e = 0; e < V; ++e) {
+        const int dl = (int)(d0 + e - rowb[q]);
+        const bool mine = dl >= 0 && dl < L;
+        whole = whole && mine;
+        const int fl = mine ? dl / 3 : 0, c = mine ? dl - 3 * fl : 0;
+        const int ce = 3 * (fl >> 1) + c;
+        const float a = (fl & 1) ? 0.5f * (cyz[q][ce] + cyz[q][ce + 3]) : cyz[q][ce];
+        // the correction is BF16-accurate: formed in FP32
+        const T zi = mv[q][e] * rv[q][e] + (T)(sf * dinv_sqrt((float)mv[q][e]) * a);
+        zo[e] = zi;
+        if (mine) {
+          zq += zi * qv[q][e];
+          zr += zi * rv[q][e];
+        }
+      }
+      if (whole) {
+        *reinterpret_cast<VecT*>(z + d0) = *reinterpret_cast<const VecT*>(zo);
+      } else {
+#pragma unroll
+        for (int e = 0; e < V; ++e) {
+          const int dl = (int)(d0 + e - rowb[q]);
+          if (dl >= 0 && dl < L) z[d0 + e] = zo[e];
+        }
+      }
     }
   }
   if (!q_old) return;
@@ -713,8 +803,11 @@ void launch_restrict_ys(cudaStream_t s, const __nv_bfloat16* ys, const CgState* 
                                  (int)restrict_ys_smem(RES_CX)));
   });
   const int cxw = (int)cdiv(gc.nx, cdiv(gc.nx, RES_CX));
-  const dim3 grid((unsigned)cdiv(gc.nx, cxw), (unsigned)cdiv(gc.ny, YS_JB), (unsigned)gc.nz);
-  k_restrict_ys<<<grid, 256, restrict_ys_smem(cxw), s>>>(ys, sst, scale_mul, out, gf, gc, cxw);
+  const int kseg = ys_kseg(gc, cxw);
+  const dim3 grid((unsigned)cdiv(gc.nx, cxw), (unsigned)cdiv(gc.ny, YS_JB),
+                  (unsigned)cdiv(gc.nz, kseg));
+  k_restrict_ys<<<grid, 256, restrict_ys_smem(cxw), s>>>(ys, sst, scale_mul, out, gf, gc, cxw,
+                                                         kseg);
   HX_CHECK_LAUNCH();
 }
 
@@ -754,6 +847,9 @@ void launch_net_output(cudaStream_t s, const T* r, const T* minv, const float* t
                        double* partials) {
   // two block partials per coarse row chunk: `partials` must hold
   // 2 net_output_blocks(gf) values
+  auto a16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+  HX_REQUIRE(a16(r) && a16(minv) && a16(z) && (!q_old || a16(q_old)),
+             "preconditioner vectors must be 16-byte aligned");
   const int cxw = row_chunk(gc.nx);
   const dim3 grid((unsigned)cdiv(gc.nx, cxw), (unsigned)gc.ny, (unsigned)gc.nz);
   k_net_output<T><<<grid, 256, 0, s>>>(r, minv, t, gf, gc, cxw, st, scale_mul, z, q_old,

@@ -32,9 +32,12 @@
 // variant with a 2-stage load ring, at 2 CTAs per SM, measured slower; so
 // did TZ = 4, with twice the MMAs per CTA and half the CTAs: 12.9 against
 // 11.7 us per layer on a 81 x 41 x 41 grid).
-// Thread 0 issues the tile's TMA loads and the bulk copy of the layer's
-// weights (pre-packed in this order) on one mbarrier, then the 54 MMAs
-// and a tcgen05.commit on a second.  Every wait is bounded (1 s of
+// Thread 0 issues the bulk copy of the layer's weights (pre-packed in this
+// order) and the tile's TMA loads on one mbarrier, then the 54 MMAs and a
+// tcgen05.commit on a second.  Layers are launched as programmatic
+// dependents of the preceding kernel: a CTA allocates TMEM, initialises its
+// barriers and starts the weight copy while the previous layer finishes,
+// and waits for it (griddepcontrol.wait) before loading its tile.  Every wait is bounded (1 s of
 // %globaltimer time); on timeout the CTA records it in *err, waits once more
 // (bounded) for its own loads or MMAs, frees its TMEM and returns, and the
 // host reports the error.  Residual hazard: if that second wait also runs
@@ -208,12 +211,11 @@ __global__ void __launch_bounds__(NTHREADS) k_conv3_tc(const __grid_constant__ C
     mbar_init(mma_bar, 1);
     *fail = 0;
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // barriers visible to TMA
-    // the input tile (two 8-channel planes) and the layer's weights on one barrier
+    // the layer's weights and the input tile (two 8-channel planes) on one
+    // barrier; the weights are not written by the preceding kernel, so
+    // their copy starts before the wait for it
     if (!selftest) {
       mbar_expect_tx(load_bar, TMA_BYTES + W_BYTES);
-      for (int h = 0; h < 2; ++h)
-        tma_load_4d(xb + (uint32_t)(h * PLANE_BYTES), &xmap, load_bar, h * 8, x0 - 1, y0 - 1,
-                    z0 - 1);
       asm volatile(
           "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
           "[%3];" ::"r"(wsb),
@@ -221,6 +223,16 @@ __global__ void __launch_bounds__(NTHREADS) k_conv3_tc(const __grid_constant__ C
           : "memory");
     }
   }
+  // Programmatic dependent launch: the set-up above may overlap the
+  // preceding kernel (the previous layer); every access to the activations
+  // follows this wait for its completion.  Then this grid lets the next
+  // layer's CTAs start their own set-up.
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  if (threadIdx.x == 0 && !selftest)
+    for (int h = 0; h < 2; ++h)
+      tma_load_4d(xb + (uint32_t)(h * PLANE_BYTES), &xmap, load_bar, h * 8, x0 - 1, y0 - 1,
+                  z0 - 1);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -342,10 +354,21 @@ static void conv3_launch(cudaStream_t s, int cout, const __nv_bfloat16* X, __nv_
   });
   const CUtensorMap map = activation_map(X, g);
   const dim3 grid((unsigned)cdiv(g.nx, TX), (unsigned)cdiv(g.ny, TY), (unsigned)cdiv(g.nz, TZ));
+  // launched as a programmatic dependent of the preceding kernel on s
+  cudaLaunchConfig_t lc{};
+  lc.gridDim = grid;
+  lc.blockDim = dim3(NTHREADS);
+  lc.dynamicSmemBytes = SMEM_BYTES;
+  lc.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  lc.attrs = at;
+  lc.numAttrs = 1;
   if (cout == 16)
-    k_conv3_tc<16><<<grid, NTHREADS, SMEM_BYTES, s>>>(map, W, Y, g, err, selftest);
+    HX_CUDA(cudaLaunchKernelEx(&lc, k_conv3_tc<16>, map, W, Y, g, err, selftest));
   else
-    k_conv3_tc<8><<<grid, NTHREADS, SMEM_BYTES, s>>>(map, W, Y, g, err, selftest);
+    HX_CUDA(cudaLaunchKernelEx(&lc, k_conv3_tc<8>, map, W, Y, g, err, selftest));
   HX_CHECK_LAUNCH();
 }
 
