@@ -293,7 +293,12 @@ void gmg_setup(hx_ctx* c, const double* fac, double shift) {
     }
     L.lmax = (float)lam;
   }
-  G.coarse_st.ensure(1);
+  // the coarse solve's state: zeroed once, so that its reduction tickets
+  // start at 0 (k_coarse_reset renews the other fields every cycle)
+  if (!G.coarse_st.p) {
+    G.coarse_st.ensure(1);
+    HX_CUDA(cudaMemsetAsync(G.coarse_st.p, 0, sizeof(CgState), s));
+  }
   G.p0.ensure(G.lv[G.nl - 1].g.dofs());
   G.p1.ensure(G.lv[G.nl - 1].g.dofs());
   G.ready = true;
@@ -458,7 +463,7 @@ CgState solve_gmg(hx_ctx* c, const double* fac, const double* b, double* x, bool
                             c->d_partials.p);
     launch_cg_update2<double>(c->stream, r, q, minv, n, st, c->d_partials.p);
     // best-iterate snapshot (the reference's failure handling returns it)
-    if (xbest) launch_axpy_state<double>(c->stream, xbest, x, pout, n, st, 1);
+    if (xbest) launch_axpy_state<double>(c->stream, xbest, x, pout, n, st, pout == P0 ? 1 : 2);
   };
   auto body = [&]() {
     one(P1, P0);

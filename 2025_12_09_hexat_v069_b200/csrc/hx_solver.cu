@@ -247,7 +247,7 @@ CgState pcg_fused(hx_ctx* c, int slot, const T* fac, const T* b, T* x, bool warm
     launch_pcg_step<T>(c->stream, P0, P1, r, minv, x, q, fac, c->d_nmask.p, g, K, shift, st,
                        c->d_partials.p);
     launch_cg_update2<T>(c->stream, r, q, minv, n, st, c->d_partials.p);
-    if (xbest) launch_axpy_state<T>(c->stream, xbest, x, P1, n, st, 1);
+    if (xbest) launch_axpy_state<T>(c->stream, xbest, x, P1, n, st, 2);
   };
   const int reps = std::max(1, check_every / 2);
   CgState sf = run_batched(c, slot, reps, body, wall_ms, t0, timed_out, 0);

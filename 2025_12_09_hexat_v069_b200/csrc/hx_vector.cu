@@ -241,7 +241,12 @@ template <typename T>
 __global__ void k_axpy_state(T* __restrict__ dst, const T* __restrict__ x,
                              const T* __restrict__ p, int64_t n, const CgState* st,
                              int when_snap) {
-  if (when_snap && !st->snap) return;
+  // when_snap 1 / 2: a best-iterate snapshot, taken only if the last
+  // iteration asked for one and its direction p_k is the buffer given (P0
+  // after iteration k = iter - 1 even, P1 after an odd one).  Launches of a
+  // batch that run after the loop stopped then rewrite the same snapshot
+  // instead of combining x with an older direction.
+  if (when_snap && !(st->snap && ((st->iter - 1) & 1) == when_snap - 1)) return;
   const T a = (T)st->alpha;
   for (int64_t i = gtid(); i < n; i += gstride()) dst[i] = x[i] + a * p[i];
 }
