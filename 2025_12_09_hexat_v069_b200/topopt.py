@@ -114,6 +114,7 @@ def run_oc_device(ctx: Context, bc_indicator, f, volfrac, radius, n_iter, p=3.0,
     res = OCResult()
     res.finetune_ms = []
     res.pc_used = []
+    res.fallback = []  # learned solves that fell back or were finished by Jacobi
     use_learned = preconditioner == 1 and not adaptive
     jac_ms = jac_its = None
     retry_at = 0
@@ -144,6 +145,7 @@ def run_oc_device(ctx: Context, bc_indicator, f, volfrac, radius, n_iter, p=3.0,
         ms = (time.perf_counter() - t0) * 1e3
         res.solve_ms.append(ms)
         res.pc_used.append(pc)
+        res.fallback.append(int(pc == 1 and (bool(rep.fallback_used) or finished_by_jacobi)))
         if preconditioner == 1 and adaptive:
             if pc == 0:
                 jac_ms, jac_its = ms, rep.iterations
