@@ -14,14 +14,20 @@
 // Transfers: trilinear prolongation P and its exact transpose R = P^T
 // (full weighting), the kernels of the learned preconditioner's levels.
 //
+// Levels are added until one has at most GMG_STOP_DOFS DOFs (or an element
+// count turns odd).
+//
 // V-cycle (FP32): on each level Chebyshev smoothing of degree GMG_DEGREE
 // with Jacobi scaling on [0.05, 1.1] x lambda_max(D^-1 A) (estimated by
 // power iteration at set-up), from zero before the restriction and from the
-// prolonged correction after it; on the coarsest level GMG_COARSE_ITERS
-// iterations of FP32 Jacobi-PCG on the fused kernels.  The cycle is
-// symmetric positive definite up to the coarse solve's early stop and FP32
-// rounding, which the flexible CG around it absorbs (Notay's FCG, the same
-// step kernels as the learned preconditioner).
+// prolonged correction after it.  The coarsest level, when it has at most
+// GMG_DIRECT_DOFS DOFs, is solved by its dense inverse: assembled from the
+// element matrices and inverted by Gauss-Jordan in FP64 at set-up, applied
+// as one FP32 matrix-vector product per cycle; a larger coarsest level gets
+// GMG_COARSE_ITERS iterations of FP32 Jacobi-PCG on the fused kernels.  The
+// cycle is symmetric positive definite up to FP32 rounding (and a PCG coarse
+// solve's early stop), which the flexible CG around it absorbs (Notay's FCG,
+// the same step kernels as the learned preconditioner).
 #include <cmath>
 #include <limits>
 
@@ -33,8 +39,9 @@ namespace hx {
 namespace {
 
 constexpr int GMG_DEGREE = 2;          // Chebyshev degree per smoothing
-constexpr int GMG_COARSE_ITERS = 64;   // PCG iterations on the coarsest level
-constexpr int64_t GMG_COARSE_NODES = 4096;
+constexpr int GMG_COARSE_ITERS = 64;   // PCG iterations on a large coarsest level
+constexpr int64_t GMG_STOP_DOFS = 1536;    // coarsen until a level has at most this many DOFs
+constexpr int64_t GMG_DIRECT_DOFS = 2048;  // coarsest levels up to this size are solved directly
 constexpr float GMG_LO = 0.05f, GMG_HI = 1.1f;  // Chebyshev range / lambda_max
 
 __device__ __forceinline__ int64_t gt() { return blockIdx.x * (int64_t)blockDim.x + threadIdx.x; }
@@ -200,6 +207,111 @@ __global__ void k_fcg_coeffs(const T* __restrict__ z, const T* __restrict__ q_ol
   }
 }
 
+// Dense FP64 operator of a (small) level: every element adds f Ke, its
+// 24 x 24 stiffness, at its nodes' DOFs (one thread per element and column:
+// the column is Ke applied to a unit vector).  A must be zero on entry.
+__global__ void k_dense_assemble(const float* __restrict__ fac, Grid g, ElemCoef<double> K,
+                                 double* __restrict__ A, int64_t n) {
+  const int64_t ne = g.elems();
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ne * 24;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e = t / 24;
+    const int col = (int)(t - e * 24), cc = col / 8, cb = col % 8;
+    const int i = (int)(e % g.nxe);
+    const int64_t r = e / g.nxe;
+    const int j = (int)(r % g.nye), k = (int)(r / g.nye);
+    double u[3][8], y[3][8];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int b = 0; b < 8; ++b) u[c][b] = (c == cc && b == cb) ? 1.0 : 0.0;
+    elem_apply(K, (double)fac[e], u, y);
+    auto dof = [&](int b, int c) -> int64_t {
+      const int64_t node = ((int64_t)(k + (b >> 2)) * g.nyn + j + ((b >> 1) & 1)) * g.nxn + i +
+                           (b & 1);
+      return 3 * node + c;
+    };
+    const int64_t dc = dof(cb, cc);
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int b = 0; b < 8; ++b)
+        if (y[c][b] != 0.0) atomicAdd(&A[dof(b, c) * n + dc], y[c][b]);
+  }
+}
+
+// Fixed DOFs (mask bit clear) get identity rows and columns; free ones the
+// shift on the diagonal -- the operator the structured kernels apply.
+__global__ void k_dense_mask(double* __restrict__ A, const uint8_t* __restrict__ nmask,
+                             double shift, int64_t n) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n * n;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = t / n, j = t - i * n;
+    const bool fi = (nmask[i / 3] >> (i % 3)) & 1u, fj = (nmask[j / 3] >> (j % 3)) & 1u;
+    if (!fi || !fj)
+      A[t] = (i == j) ? 1.0 : 0.0;
+    else if (i == j)
+      A[t] += shift;
+  }
+}
+
+// row and column `k` of A into rk, ck (the first pivot's, before step 0)
+__global__ void k_gj_copy(const double* __restrict__ A, int64_t n, int64_t k,
+                          double* __restrict__ rk, double* __restrict__ ck) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    rk[t] = A[k * n + t];
+    ck[t] = A[t * n + k];
+  }
+}
+
+// One pivot of the in-place Gauss-Jordan inversion (no pivoting: the matrix
+// is symmetric positive definite).  rk, ck: row and column k before this
+// step; each thread rewrites its own entry and copies the entries of row and
+// column k+1 into rn, cn for the next step.
+__global__ void k_gj_step(double* __restrict__ A, int64_t n, int64_t k,
+                          const double* __restrict__ rk, const double* __restrict__ ck,
+                          double* __restrict__ rn, double* __restrict__ cn) {
+  const double inv = 1.0 / rk[k];
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n * n;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = t / n, j = t - i * n;
+    double a;
+    if (i == k && j == k)
+      a = inv;
+    else if (i == k)
+      a = rk[j] * inv;
+    else if (j == k)
+      a = -ck[i] * inv;
+    else
+      a = A[t] - ck[i] * rk[j] * inv;
+    A[t] = a;
+    if (i == k + 1) rn[j] = a;
+    if (j == k + 1) cn[i] = a;
+  }
+}
+
+template <typename TD>
+__global__ void k_cvt_f64(TD* __restrict__ d, const double* __restrict__ s, int64_t n) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+       t += (int64_t)gridDim.x * blockDim.x)
+    d[t] = (TD)s[t];
+}
+
+// x = Ainv b (n x n, FP32): one warp per row, b read through the cache
+__global__ void k_dense_gemv(const float* __restrict__ Ainv, const float* __restrict__ b,
+                             float* __restrict__ x, int64_t n) {
+  const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= n) return;
+  const float* row = Ainv + w * n;
+  float s = 0.f;
+  for (int64_t j = lane; j < n; j += 32) s = fmaf(row[j], __ldg(&b[j]), s);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) x[w] = s;
+}
+
 unsigned gblocks(int64_t n) {
   return (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv(n, 256), 16LL * sm_count()));
 }
@@ -256,7 +368,7 @@ void gmg_setup(hx_ctx* c, const double* fac, double shift) {
     }
     G.nl = l + 1;
     const bool even = g.nxe % 2 == 0 && g.nye % 2 == 0 && g.nze % 2 == 0;
-    if (!even || nn <= GMG_COARSE_NODES || g.nxe < 4 || g.nye < 4 || g.nze < 4) break;
+    if (!even || n <= GMG_STOP_DOFS || g.nxe < 4 || g.nye < 4 || g.nze < 4) break;
     Grid gc{};
     gc.nxe = g.nxe / 2;
     gc.nye = g.nye / 2;
@@ -292,6 +404,34 @@ void gmg_setup(hx_ctx* c, const double* fac, double shift) {
       HX_CHECK_LAUNCH();
     }
     L.lmax = (float)lam;
+  }
+  // Coarsest level: its dense inverse when small enough (Gauss-Jordan in
+  // FP64, one launch per pivot), else a fixed-count FP32 PCG at every cycle.
+  {
+    auto& L = G.lv[G.nl - 1];
+    const int64_t n = L.g.dofs();
+    G.direct = n <= GMG_DIRECT_DOFS;
+    if (G.direct) {
+      const int64_t nn2 = n * n;
+      double* A = G.dense.ensure(nn2);
+      double* gj = G.gj.ensure(4 * n);
+      HX_CUDA(cudaMemsetAsync(A, 0, nn2 * sizeof(double), s));
+      const ElemCoef<double> K = make_elem_coef(L.h[0], L.h[1], L.h[2], c->nu);
+      k_dense_assemble<<<gblocks(L.g.elems() * 24), 256, 0, s>>>(L.fac.p, L.g, K, A, n);
+      HX_CHECK_LAUNCH();
+      k_dense_mask<<<gblocks(nn2), 256, 0, s>>>(A, L.nmask.p, (double)L.shift, n);
+      HX_CHECK_LAUNCH();
+      k_gj_copy<<<gblocks(n), 256, 0, s>>>(A, n, 0, gj, gj + n);
+      HX_CHECK_LAUNCH();
+      for (int64_t k = 0; k < n; ++k) {
+        double* cur = gj + (k & 1) * 2 * n;
+        double* nxt = gj + ((k + 1) & 1) * 2 * n;
+        k_gj_step<<<gblocks(nn2), 256, 0, s>>>(A, n, k, cur, cur + n, nxt, nxt + n);
+        HX_CHECK_LAUNCH();
+      }
+      k_cvt_f64<float><<<gblocks(nn2), 256, 0, s>>>(G.ainv.ensure(nn2), A, nn2);
+      HX_CHECK_LAUNCH();
+    }
   }
   // the coarse solve's state: zeroed once, so that its reduction tickets
   // start at 0 (k_coarse_reset renews the other fields every cycle)
@@ -362,9 +502,14 @@ void gmg_vcycle(hx_ctx* c, const T* r, T* z) {
     k_mask3<<<gblocks(3 * C.g.nodes()), 256, 0, s>>>(C.b.p, C.nmask.p, C.g.nodes());
     HX_CHECK_LAUNCH();
   }
-  {
-    // coarsest level (the only one for small grids): fixed-count FP32
-    // Jacobi-PCG from zero
+  if (G.direct) {
+    // coarsest level (the only one for small grids): its dense inverse
+    auto& L = G.lv[nl - 1];
+    const int64_t n = L.g.dofs();
+    k_dense_gemv<<<(unsigned)cdiv(n * 32, 256), 256, 0, s>>>(G.ainv.p, L.b.p, L.x.p, n);
+    HX_CHECK_LAUNCH();
+  } else {
+    // a large coarsest level: fixed-count FP32 Jacobi-PCG from zero
     auto& L = G.lv[nl - 1];
     const int64_t n = L.g.dofs();
     CgState* st = G.coarse_st.p;

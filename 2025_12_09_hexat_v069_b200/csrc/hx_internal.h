@@ -227,6 +227,11 @@ struct hx_ctx {
     hx::DevBuf<hx::CgState> coarse_st;
     hx::DevBuf<float> p0, p1;   // coarse PCG directions
     hx::DevBuf<double> z, s;    // FCG: preconditioned residual, scratch
+    // direct coarsest-level solve: dense inverse (FP32, n x n) of the masked
+    // coarsest operator, formed in FP64 at set-up
+    bool direct = false;
+    hx::DevBuf<double> dense, gj;  // FP64 matrix being inverted; pivot row/column buffers
+    hx::DevBuf<float> ainv;
   } gmg;
 
   // lattice origin of the mesh (the minimum node coordinates; 0 for hx_set_grid)
