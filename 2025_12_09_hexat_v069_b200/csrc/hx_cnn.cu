@@ -591,7 +591,9 @@ __global__ void k_unlift(const __nv_bfloat16* __restrict__ Y, const float* __res
 // coarse rows j, j+1 x k, k+1 are first interpolated in y and z into shared
 // memory (one row per fine (fy, fz)); each fine DOF then needs two shared
 // loads for its x interpolation.
-template <typename T>
+// VEC: 16-byte chunks (every vector 16-byte aligned); else one value per
+// chunk (vectors that are rows of a matrix with an odd row length).
+template <typename T, bool VEC>
 __global__ void __launch_bounds__(256)
     k_net_output(const T* __restrict__ r, const T* __restrict__ minv, const float* __restrict__ t,
                  GridN gf, GridN gc, int cxw, CgState* st, double scale_mul, T* __restrict__ z,
@@ -630,8 +632,9 @@ __global__ void __launch_bounds__(256)
   // hold DOFs of the neighbouring rows: those are loaded but neither used
   // nor stored.  The vectors' last chunk may reach past n: it is read per
   // DOF.  Rows past the grid are read at row 0 and not stored.
-  constexpr int V = 16 / (int)sizeof(T);
-  using VecT = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+  constexpr int V = VEC ? 16 / (int)sizeof(T) : 1;
+  using VecT = typename std::conditional<
+      VEC, typename std::conditional<sizeof(T) == 4, float4, double2>::type, T>::type;
   const int fx0 = 2 * cx0;
   const int L = 3 * (min(2 * (cx0 + w), gf.nx) - fx0);
   const int64_t nv = 3 * ((int64_t)gf.nx * gf.ny * gf.nz);
@@ -848,12 +851,15 @@ void launch_net_output(cudaStream_t s, const T* r, const T* minv, const float* t
   // two block partials per coarse row chunk: `partials` must hold
   // 2 net_output_blocks(gf) values
   auto a16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
-  HX_REQUIRE(a16(r) && a16(minv) && a16(z) && (!q_old || a16(q_old)),
-             "preconditioner vectors must be 16-byte aligned");
+  const bool vec = a16(r) && a16(minv) && a16(z) && (!q_old || a16(q_old));
   const int cxw = row_chunk(gc.nx);
   const dim3 grid((unsigned)cdiv(gc.nx, cxw), (unsigned)gc.ny, (unsigned)gc.nz);
-  k_net_output<T><<<grid, 256, 0, s>>>(r, minv, t, gf, gc, cxw, st, scale_mul, z, q_old,
-                                       partials);
+  if (vec)
+    k_net_output<T, true><<<grid, 256, 0, s>>>(r, minv, t, gf, gc, cxw, st, scale_mul, z, q_old,
+                                               partials);
+  else
+    k_net_output<T, false><<<grid, 256, 0, s>>>(r, minv, t, gf, gc, cxw, st, scale_mul, z,
+                                                q_old, partials);
   HX_CHECK_LAUNCH();
 }
 

@@ -18,8 +18,8 @@
 // count turns odd).
 //
 // V-cycle (FP32): on each level Chebyshev smoothing of degree GMG_DEGREE
-// with Jacobi scaling on [0.05, 1.1] x lambda_max(D^-1 A) (estimated by
-// power iteration at set-up), from zero before the restriction and from the
+// with Jacobi scaling on [0.05, 1.1] x lambda_max(D^-1 A) (a Lanczos
+// estimate from Jacobi-PCG steps at set-up), from zero before the restriction and from the
 // prolonged correction after it.  The coarsest level, when it has at most
 // GMG_DIRECT_DOFS DOFs, is solved by its dense inverse: assembled from the
 // element matrices and inverted by Gauss-Jordan in FP64 at set-up, applied
@@ -30,6 +30,7 @@
 // the same step kernels as the learned preconditioner).
 #include <cmath>
 #include <limits>
+#include <vector>
 
 #include "hx_cnn.h"
 #include "hx_solver.h"
@@ -43,6 +44,7 @@ constexpr int GMG_COARSE_ITERS = 64;   // PCG iterations on a large coarsest lev
 constexpr int64_t GMG_STOP_DOFS = 1536;    // coarsen until a level has at most this many DOFs
 constexpr int64_t GMG_DIRECT_DOFS = 2048;  // coarsest levels up to this size are solved directly
 constexpr float GMG_LO = 0.05f, GMG_HI = 1.1f;  // Chebyshev range / lambda_max
+constexpr int GMG_LANCZOS = 20;                  // PCG steps of the lambda_max estimate
 
 __device__ __forceinline__ int64_t gt() { return blockIdx.x * (int64_t)blockDim.x + threadIdx.x; }
 __device__ __forceinline__ int64_t gs() { return (int64_t)gridDim.x * blockDim.x; }
@@ -121,14 +123,8 @@ __global__ void k_copy_cvt(TD* __restrict__ d, const TS* __restrict__ s, int64_t
   for (int64_t i = gt(); i < n; i += gs()) d[i] = (TD)s[i];
 }
 
-// d = a * s
-__global__ void k_scale_copy(float* __restrict__ d, const float* __restrict__ s, float a,
-                             int64_t n) {
-  for (int64_t i = gt(); i < n; i += gs()) d[i] = a * s[i];
-}
-
-// power-iteration start: a pseudo-random vector (hash of the index), zero on
-// fixed DOFs
+// a pseudo-random vector (hash of the index), zero on fixed DOFs: the
+// right-hand side of the lambda_max estimate
 __global__ void k_rand_vec(float* __restrict__ v, const uint8_t* __restrict__ nmask, int64_t nn) {
   for (int64_t i = gt(); i < 3 * nn; i += gs()) {
     uint32_t h = (uint32_t)i * 2654435761u + 0x9E3779B9u;
@@ -137,24 +133,6 @@ __global__ void k_rand_vec(float* __restrict__ v, const uint8_t* __restrict__ nm
     h ^= h >> 13;
     const float u = (float)(h & 0xFFFFFF) / 16777216.f - 0.5f;
     v[i] = ((nmask[i / 3] >> (i % 3)) & 1u) ? u : 0.f;
-  }
-}
-
-// w = minv * w (in place); out[0] = |w|^2, out[1] = |v|^2 (FP64 sums)
-__global__ void k_power_norms(float* __restrict__ w, const float* __restrict__ minv,
-                              const float* __restrict__ v, int64_t n, double* partials,
-                              CgState* st, double* out) {
-  double a = 0.0, b = 0.0;
-  for (int64_t i = gt(); i < n; i += gs()) {
-    const float wi = minv[i] * w[i];
-    w[i] = wi;
-    a += (double)wi * wi;
-    b += (double)v[i] * v[i];
-  }
-  double vv[2] = {a, b};
-  if (grid_reduce<2>(vv, partials, &st->ticket[TK_AUX]) && threadIdx.x == 0) {
-    out[0] = vv[0];
-    out[1] = vv[1];
   }
 }
 
@@ -312,6 +290,39 @@ __global__ void k_dense_gemv(const float* __restrict__ Ainv, const float* __rest
   if (lane == 0) x[w] = s;
 }
 
+// Largest eigenvalue of the Lanczos tridiagonal T of a PCG run (alpha_j,
+// beta_j its step lengths and direction coefficients): T_jj = 1/alpha_j +
+// beta_{j-1}/alpha_{j-1}, T_j,j+1 = sqrt(beta_j)/alpha_j; by bisection on
+// the Sturm count, from the Gershgorin bound down.
+double lanczos_max(const std::vector<double>& al, const std::vector<double>& be) {
+  const size_t k = al.size();
+  std::vector<double> d(k), e(k, 0.0);
+  for (size_t j = 0; j < k; ++j) {
+    d[j] = 1.0 / al[j] + (j > 0 ? be[j - 1] / al[j - 1] : 0.0);
+    if (j + 1 < k) e[j] = std::sqrt(std::max(be[j], 0.0)) / al[j];
+  }
+  double lo = 0.0, hi = 0.0;
+  for (size_t j = 0; j < k; ++j)
+    hi = std::max(hi, d[j] + std::fabs(e[j]) + (j > 0 ? std::fabs(e[j - 1]) : 0.0));
+  // eigenvalues below x: sign changes of the LDL^T pivots of T - x I
+  auto below = [&](double x) {
+    int cnt = 0;
+    double q = 1.0;
+    for (size_t j = 0; j < k; ++j) {
+      const double off = j > 0 ? e[j - 1] * e[j - 1] : 0.0;
+      q = d[j] - x - (j > 0 ? off / q : 0.0);
+      if (q == 0.0) q = -1e-300;
+      if (q < 0.0) ++cnt;
+    }
+    return cnt;
+  };
+  for (int it = 0; it < 100; ++it) {
+    const double mid = 0.5 * (lo + hi);
+    if (below(mid) >= (int)k) hi = mid; else lo = mid;
+  }
+  return hi;
+}
+
 unsigned gblocks(int64_t n) {
   return (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv(n, 256), 16LL * sm_count()));
 }
@@ -379,31 +390,37 @@ void gmg_setup(hx_ctx* c, const double* fac, double shift) {
     g = gc;
     for (int a = 0; a < 3; ++a) h[a] *= 2.0;
   }
-  // lambda_max(D^-1 A) of every smoothed level (all but the coarsest):
-  // 12 power iterations each
+  // lambda_max(D^-1 A) of every smoothed level (all but the coarsest), from
+  // the Lanczos tridiagonal of GMG_LANCZOS Jacobi-PCG steps on a random
+  // right-hand side.  The largest Ritz value converges to lambda_max from
+  // below much faster than power iteration; an estimate below lambda_max
+  // leaves the top of the spectrum outside the Chebyshev interval, where
+  // the smoother is not positive definite.
+  G.p0.ensure(G.lv[0].g.dofs());
+  G.p1.ensure(G.lv[0].g.dofs());
   for (int l = 0; l + 1 < G.nl; ++l) {
     auto& L = G.lv[l];
     const int64_t nn = L.g.nodes(), n = L.g.dofs();
-    k_rand_vec<<<gblocks(n), 256, 0, s>>>(L.x.p, L.nmask.p, nn);
+    CgState* st = c->d_state.p + 3;
+    k_rand_vec<<<gblocks(n), 256, 0, s>>>(L.b.p, L.nmask.p, nn);
     HX_CHECK_LAUNCH();
-    double lam = 1.0;
-    for (int it = 0; it < 12; ++it) {
-      launch_matvec<float>(s, 0, L.x.p, L.q.p, L.fac.p, L.nmask.p, L.g, L.K, L.shift,
-                           c->d_state.p + 3, c->d_partials.p, nullptr);
-      put_state(c, 3, CgState{});
-      k_power_norms<<<gblocks(n), 256, 0, s>>>(L.q.p, L.minv.p, L.x.p, n, c->d_partials.p,
-                                                c->d_state.p + 3, c->d_scalars.p);
-      HX_CHECK_LAUNCH();
-      double nv[2];
-      HX_CUDA(cudaMemcpyAsync(nv, c->d_scalars.p, sizeof(nv), cudaMemcpyDeviceToHost, s));
-      HX_CUDA(cudaStreamSynchronize(s));
-      if (!(nv[1] > 0.0) || !(nv[0] > 0.0)) break;
-      lam = std::sqrt(nv[0] / nv[1]);
-      // next iterate: w / |w|
-      k_scale_copy<<<gblocks(n), 256, 0, s>>>(L.x.p, L.q.p, (float)(1.0 / std::sqrt(nv[0])), n);
-      HX_CHECK_LAUNCH();
+    launch_fill_zero(s, L.x.p, n * sizeof(float));
+    put_state(c, 3, fresh_state(0.0, 1 << 30, 1, false, false));
+    launch_cg_init<float>(s, L.b.p, nullptr, L.minv.p, L.r.p, G.p1.p, n, st, c->d_partials.p);
+    std::vector<double> al, be;
+    for (int it = 0; it < GMG_LANCZOS; ++it) {
+      float* pin = (it % 2 == 0) ? G.p1.p : G.p0.p;
+      float* pout = (it % 2 == 0) ? G.p0.p : G.p1.p;
+      launch_pcg_step<float>(s, pin, pout, L.r.p, L.minv.p, L.x.p, L.q.p, L.fac.p, L.nmask.p, L.g,
+                             L.K, L.shift, st, c->d_partials.p);
+      launch_cg_update2<float>(s, L.r.p, L.q.p, L.minv.p, n, st, c->d_partials.p);
+      const CgState h = get_state(c, 3);
+      if (!(h.alpha > 0.0) || !std::isfinite(h.alpha)) break;
+      al.push_back(h.alpha);
+      be.push_back(h.beta);
+      if (h.status != HX_RUNNING) break;
     }
-    L.lmax = (float)lam;
+    L.lmax = al.empty() ? 2.0f : (float)lanczos_max(al, be);
   }
   // Coarsest level: its dense inverse when small enough (Gauss-Jordan in
   // FP64, one launch per pivot), else a fixed-count FP32 PCG at every cycle.

@@ -562,7 +562,8 @@ hx_status solve_grid(hx_ctx* c, const double* f, const double* fac, double* u,
       break;
     }
     if (!o.ref_retry || timed_out) break;
-    // Failure handling of src/Solvers/GPUSolver.jl:536-593 (no AMG switch).
+    // Failure handling of src/Solvers/GPUSolver.jl:536-593; its switch to
+    // the host AMG goes to the multigrid preconditioner here.
     const bool diverged = st.status == HX_ST_BREAKDOWN || st.status == HX_ST_NONFINITE ||
                           st.status == HX_ST_DIVERGED;
     const bool failed_badly = diverged || st.best_rel > 0.1;
@@ -739,7 +740,7 @@ hx_status time_kernel(hx_ctx* c, int kernel, int reps, double* avg_ms) {
       };
   } else if (kernel == HX_KERNEL_PCG_STEP_FP32 || kernel == HX_KERNEL_FCG_STEP_FP32) {
     HX_REQUIRE(ready(c->d_fac.n, ne) && ready(c->d_nmask.n, g.nodes()) && ready(c->d_minv.n, n) &&
-                   ready(c->d_r.n, n),
+                   (ready(c->d_r.n, n) || ready(c->d_b.n, n)),
                "run a solve first");
     float* f32 = c->d_fac32.ensure(ne);
     float* p32 = c->d_p32.ensure(n);
@@ -751,7 +752,8 @@ hx_status time_kernel(hx_ctx* c, int kernel, int reps, double* avg_ms) {
     launch_convert<float, double>(c->stream, f32, c->d_fac.p, ne);
     launch_convert<float, double>(c->stream, m32, c->d_minv.p, n);
     HX_CUDA(cudaMemsetAsync(p32, 0, n * sizeof(float), c->stream));
-    launch_convert<float, double>(c->stream, r32, c->d_r.p, n);
+    // the last residual, or the right-hand side after a solve that kept none
+    launch_convert<float, double>(c->stream, r32, ready(c->d_r.n, n) ? c->d_r.p : c->d_b.p, n);
     HX_CUDA(cudaMemsetAsync(x32, 0, n * sizeof(float), c->stream));
     const ElemCoef<float> K32 = to_float(c->K);
     if (kernel == HX_KERNEL_PCG_STEP_FP32) {
