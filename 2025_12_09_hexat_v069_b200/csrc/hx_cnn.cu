@@ -13,8 +13,6 @@
 // one tap per warp at a time; partials summed across CTAs in a fixed order.
 #include <cuda_bf16.h>
 
-#include <type_traits>
-
 #include "hx_cnn.h"
 
 namespace hx {
@@ -366,33 +364,35 @@ __global__ void __launch_bounds__(256)
 }
 
 // The same level-1 field from ys = BF16(D^-1/2 v) (k_cg_update2 writes it
-// with the residual): out = k R ys.  One CTA per (x-chunk of <= RES_CX
-// cells, block of YS_JB coarse y-rows j0.., segment of kseg coarse planes)
-// marches up the fine planes of its segment, so that each fine row is read
-// once per segment (the y-rows shared with the neighbouring blocks and the
-// plane below the segment are read twice).  Per fine plane p the rows
-// 2j0-1 .. 2(j0+YS_JB-1)+1 (clamped to the grid) are staged with 16-byte
-// cp.async chunks into a ring of YS_RING slots, planes p+1 .. p+YS_RING-1
-// in flight while p is used; each row is copied from the chunk holding its
-// first entry (a shift of 0-7 entries; the last chunk may reach 7 entries
-// past n, so ys holds n + 8 entries).  Plane p is collapsed in y per fine
-// DOF of each coarse row (S_p) and added into the z-sums of its coarse
-// planes: A_k = 0.5 S_{2k-1} + S_{2k} + 0.5 S_{2k+1} (two buffers, k even
-// and odd); a finished A_k is weighted in x and stored.
+// with the residual): out = k R ys.  One CTA per (x-chunk of w <= YS_CX
+// coarse cells, block of YS_JB coarse y-rows j0.., segment of kseg coarse
+// planes).  Thread t < 3w owns coarse cell cx0 + t/3, component t%3, and
+// keeps in registers the sums of its YS_JB coarse rows for two coarse
+// planes (k even, k odd) while the CTA marches up the fine planes of its
+// segment.  Per fine plane the rows 2j0-1 .. 2j0+2 YS_JB-1 inside the grid
+// are staged with 16-byte cp.async chunks into a ring of YS_RING slots
+// (planes p+1 .. p+YS_RING-1 in flight while p is used), each row from the
+// chunk holding its first entry (a shift of 0-7 entries; the last chunk may
+// reach 7 entries past n, so ys holds n + 8 entries).  A thread collapses
+// its three fine x-nodes of each staged row (weights 1/2, 1, 1/2), adds
+// the value into its coarse rows with the y weights and, per plane, into
+// its coarse planes with the z weight; a finished coarse plane is stored.
+// Each fine row is read once per segment (the rows shared with the
+// neighbouring row blocks and the plane below the segment twice).
+constexpr int YS_CX = 85;  // coarse cells per chunk: 3 x 85 = 255 threads
 constexpr int YS_JB = 4;
 constexpr int YS_NY = 2 * YS_JB + 1;  // staged fine y-rows per plane
 constexpr int YS_RING = 4;            // staged planes: the one in use and 3 ahead
 
-__device__ __forceinline__ int ys_chunks(int cxw) { return 3 * (2 * cxw + 1) / 8 + 3; }
+__device__ __forceinline__ float bf16_bits(unsigned short h) { return __uint_as_float((unsigned)h << 16); }
 
 __global__ void __launch_bounds__(256)
     k_restrict_ys(const __nv_bfloat16* __restrict__ ys, const CgState* sst, double scale_mul,
                   float* __restrict__ out, GridN gf, GridN gc, int cxw, int kseg) {
   extern __shared__ __align__(16) unsigned char rsm[];
   const int seg = 3 * (2 * cxw + 1);
-  const int segc = ys_chunks(cxw);  // 16-byte chunks per staged row
-  uint4* sc = reinterpret_cast<uint4*>(rsm);                          // [YS_RING][YS_NY][segc]
-  float* acc = reinterpret_cast<float*>(sc + YS_RING * YS_NY * segc);  // [2][YS_JB][seg]
+  const int segc = seg / 8 + 3;  // 16-byte chunks per staged row
+  uint4* sc = reinterpret_cast<uint4*>(rsm);  // [YS_RING][YS_NY][segc]
   const int cx0 = blockIdx.x * cxw, w = min(cxw, gc.nx - cx0);
   const int j0 = blockIdx.y * YS_JB;
   const int jn = min(YS_JB, gc.ny - j0);  // coarse rows of this block
@@ -400,21 +400,21 @@ __global__ void __launch_bounds__(256)
   const int fxa = max(2 * cx0 - 1, 0);
   const int fxb = min(2 * (cx0 + w - 1) + 1, gf.nx - 1);
   const int L = 3 * (fxb - fxa + 1);
-  const int fy_lo = max(2 * j0 - 1, 0);
-  const int fy_hi = min(2 * (j0 + jn - 1) + 1, gf.ny - 1);
-  const int ny_r = fy_hi - fy_lo + 1;  // <= YS_NY
+  const int fy0 = 2 * j0 - 1;  // fine row of staged row 0 (-1 on the first block)
   // fine planes of the segment: 2k0-1 .. 2k1-1, clipped to the grid
   const int pa = max(2 * k0 - 1, 0), pb = min(2 * k1 - 1, gf.nz - 1);
   const int np = pb - pa + 1;
   const uint4* yc = reinterpret_cast<const uint4*>(ys);
+  auto row_in = [&](int ry) { return fy0 + ry >= 0 && fy0 + ry < gf.ny; };
   auto stage = [&](int p, int slot) {
-    for (int u = threadIdx.x; u < ny_r * segc; u += blockDim.x) {
-      const int yy = u / segc, cu = u - yy * segc;
-      const int64_t e0 = 3 * (((int64_t)p * gf.ny + fy_lo + yy) * gf.nx + fxa);
+    for (int u = threadIdx.x; u < YS_NY * segc; u += blockDim.x) {
+      const int ry = u / segc, cu = u - ry * segc;
+      if (!row_in(ry)) continue;
+      const int64_t e0 = 3 * (((int64_t)p * gf.ny + fy0 + ry) * gf.nx + fxa);
       const int64_t c0 = e0 >> 3, c1 = (e0 + L + 7) >> 3;
       if (cu < c1 - c0)
         asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(
-                         (unsigned)__cvta_generic_to_shared(sc + (slot * YS_NY + yy) * segc + cu)),
+                         (unsigned)__cvta_generic_to_shared(sc + (slot * YS_NY + ry) * segc + cu)),
                      "l"(yc + c0 + cu));
     }
   };
@@ -423,22 +423,38 @@ __global__ void __launch_bounds__(256)
     if (i < np) stage(pa + i, i);
     asm volatile("cp.async.commit_group;\n" ::);
   }
+  // this thread's coarse cell and component; its fine x-nodes fx-1, fx,
+  // fx+1 (a missing neighbour reads the centre with weight 0)
+  const int t = threadIdx.x;
+  const bool act = t < 3 * w;
+  const int cl = act ? t / 3 : 0, c = act ? t - 3 * cl : 0;
+  const int fx = 2 * (cx0 + cl);
+  const int ic = 3 * (fx - fxa) + c;
+  const float wl = fx >= 1 ? 0.5f : 0.f, wr = fx + 1 < gf.nx ? 0.5f : 0.f;
+  const int il = fx >= 1 ? ic - 3 : ic, ir = fx + 1 < gf.nx ? ic + 3 : ic;
   const float kc = (float)field_coef(sst, nullptr, 0, scale_mul);
-  const __nv_bfloat16* sy = reinterpret_cast<const __nv_bfloat16*>(sc);
-  // x-weights of finished coarse plane k (buffer k & 1), stored
-  auto finish = [&](int k) {
-    const float* A = acc + (k & 1) * YS_JB * seg;
-    for (int e = threadIdx.x; e < 3 * w * jn; e += blockDim.x) {
-      const int jj = e / (3 * w), ex = e - jj * 3 * w;
-      const int cl = ex / 3, c = ex - 3 * cl;
-      const int fx = 2 * (cx0 + cl);
-      const int l = fx - fxa;
-      const float* sr = A + jj * seg;
-      float a = sr[3 * l + c];
-      if (fx >= 1) a += 0.5f * sr[3 * (l - 1) + c];
-      if (fx + 1 < gf.nx) a += 0.5f * sr[3 * (l + 1) + c];
-      out[3 * (((int64_t)k * gc.ny + j0 + jj) * gc.nx + cx0) + ex] = kc * a;
+  float accE[YS_JB], accO[YS_JB];  // coarse planes k even / k odd
+#pragma unroll
+  for (int jj = 0; jj < YS_JB; ++jj) accE[jj] = accO[jj] = 0.f;
+  // z step of fine plane p = 2 kp (+1) with its y-collapsed rows vy; lo:
+  // sums of coarse plane kp, hi: of kp + 1
+  auto zstep = [&](float (&lo)[YS_JB], float (&hi)[YS_JB], const float (&vy)[YS_JB], int kp,
+                   bool odd) {
+#pragma unroll
+    for (int jj = 0; jj < YS_JB; ++jj) {
+      if (odd) {
+        if (kp >= k0) lo[jj] += 0.5f * vy[jj];
+        if (kp + 1 < k1) hi[jj] = 0.5f * vy[jj];
+      } else {
+        lo[jj] = kp > 0 ? lo[jj] + vy[jj] : vy[jj];
+      }
     }
+  };
+  auto store = [&](const float (&a)[YS_JB], int k) {
+    if (!act) return;
+#pragma unroll
+    for (int jj = 0; jj < YS_JB; ++jj)
+      if (jj < jn) out[3 * (((int64_t)k * gc.ny + j0 + jj) * gc.nx + cx0) + t] = kc * a[jj];
   };
   for (int i = 0; i < np; ++i) {
     const int p = pa + i, slot = i % YS_RING;
@@ -446,43 +462,35 @@ __global__ void __launch_bounds__(256)
     __syncthreads();  // plane p landed for every thread; slot of plane p-1 free
     if (i + YS_RING - 1 < np) stage(p + YS_RING - 1, (i + YS_RING - 1) % YS_RING);
     asm volatile("cp.async.commit_group;\n" ::);
-    const int kp = p >> 1;     // p = 2 kp (+1)
-    const bool odd = p & 1;
-    // odd p: A_kp (if in the segment) += 0.5 S, A_{kp+1} (if in it) = 0.5 S;
-    // even p: A_kp += S, or = S on the grid's first plane
-    const bool add_lo = odd ? kp >= k0 : kp > 0;
-    const bool set_hi = odd && kp + 1 < k1;
-    const float wz = odd ? 0.5f : 1.f;
-    float* Alo = acc + (kp & 1) * YS_JB * seg;
-    float* Ahi = acc + ((kp + 1) & 1) * YS_JB * seg;
-    for (int jj = 0; jj < jn; ++jj) {
-      // the 3 fine rows of coarse row j: staged offset and weight
-      int off[3];
-      float rw[3];
+    const unsigned short* sp =
+        reinterpret_cast<const unsigned short*>(sc + slot * YS_NY * segc);
+    float vy[YS_JB];
 #pragma unroll
-      for (int dy = -1; dy <= 1; ++dy) {
-        const int fy0 = 2 * (j0 + jj) + dy;
-        const bool ok = fy0 >= 0 && fy0 < gf.ny;
-        const int yy = min(max(fy0, fy_lo), fy_hi) - fy_lo;
-        const int64_t e0 = 3 * (((int64_t)p * gf.ny + fy_lo + yy) * gf.nx + fxa);
-        off[dy + 1] = 8 * (slot * YS_NY + yy) * segc + (int)(e0 & 7);
-        rw[dy + 1] = ok ? wz * fw(dy) : 0.f;
-      }
-      for (int dl = threadIdx.x; dl < L; dl += blockDim.x) {
-        float v = 0.f;
+    for (int jj = 0; jj < YS_JB; ++jj) vy[jj] = 0.f;
 #pragma unroll
-        for (int q = 0; q < 3; ++q) v += rw[q] * __bfloat162float(sy[off[q] + dl]);
-        const int o = jj * seg + dl;
-        Alo[o] = add_lo ? Alo[o] + v : v;
-        if (set_hi) Ahi[o] = v;
+    for (int ry = 0; ry < YS_NY; ++ry) {
+      if (!row_in(ry)) continue;
+      const int64_t e0 = 3 * (((int64_t)p * gf.ny + fy0 + ry) * gf.nx + fxa);
+      const unsigned short* rp = sp + ry * segc * 8 + (int)(e0 & 7);
+      const float xv = bf16_bits(rp[ic]) + wl * bf16_bits(rp[il]) + wr * bf16_bits(rp[ir]);
+      // staged row ry is fine row 2 (j0 + jj) + d with d = ry - 1 - 2 jj
+#pragma unroll
+      for (int jj = 0; jj < YS_JB; ++jj) {
+        const int d = ry - 1 - 2 * jj;
+        if (d == 0) vy[jj] += xv;
+        else if (d == 1 || d == -1) vy[jj] += 0.5f * xv;
       }
     }
+    const int kp = p >> 1;
+    const bool odd = p & 1;
+    if ((kp & 1) == 0) zstep(accE, accO, vy, kp, odd);
+    else zstep(accO, accE, vy, kp, odd);
     // a coarse plane is complete after its top fine plane 2k+1, or after
     // plane 2k when that is the grid's last
     const int kdone = odd ? kp : (p == gf.nz - 1 ? kp : -1);
     if (kdone >= k0) {
-      __syncthreads();
-      finish(kdone);
+      if ((kdone & 1) == 0) store(accE, kdone);
+      else store(accO, kdone);
     }
   }
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
@@ -490,14 +498,14 @@ __global__ void __launch_bounds__(256)
 
 static int ys_kseg(const GridN& gc, int cxw) {
   const int64_t cols = cdiv(gc.nx, cxw) * cdiv(gc.ny, YS_JB);
-  const int64_t want = 4LL * sm_count();  // CTAs: 4 per SM
+  const int64_t want = 6LL * sm_count();  // CTAs: 6 per SM (shared memory)
   const int64_t segs = std::max<int64_t>(1, std::min<int64_t>(gc.nz, cdiv(want, cols)));
   return (int)cdiv(gc.nz, segs);
 }
 
 static size_t restrict_ys_smem(int cxw) {
   const size_t seg = 3 * (2 * (size_t)cxw + 1);
-  return (size_t)YS_RING * YS_NY * (seg / 8 + 3) * 16 + 2 * YS_JB * seg * sizeof(float);
+  return (size_t)YS_RING * YS_NY * (seg / 8 + 3) * 16;
 }
 
 // Prolongation, the exact transpose of k_restrict (without normalisation):
@@ -591,9 +599,7 @@ __global__ void k_unlift(const __nv_bfloat16* __restrict__ Y, const float* __res
 // coarse rows j, j+1 x k, k+1 are first interpolated in y and z into shared
 // memory (one row per fine (fy, fz)); each fine DOF then needs two shared
 // loads for its x interpolation.
-// VEC: 16-byte chunks (every vector 16-byte aligned); else one value per
-// chunk (vectors that are rows of a matrix with an odd row length).
-template <typename T, bool VEC>
+template <typename T>
 __global__ void __launch_bounds__(256)
     k_net_output(const T* __restrict__ r, const T* __restrict__ minv, const float* __restrict__ t,
                  GridN gf, GridN gc, int cxw, CgState* st, double scale_mul, T* __restrict__ z,
@@ -626,85 +632,40 @@ __global__ void __launch_bounds__(256)
     }
   }
   __syncthreads();
-  // the (up to) 4 fine rows, each L DOFs from DOF rowb[q]: a thread takes
-  // the same 16-byte chunk offset in every row (12 vector loads in flight).
-  // Chunks are aligned in the vectors, so a row's first and last chunks
-  // hold DOFs of the neighbouring rows: those are loaded but neither used
-  // nor stored.  The vectors' last chunk may reach past n: it is read per
-  // DOF.  Rows past the grid are read at row 0 and not stored.
-  constexpr int V = VEC ? 16 / (int)sizeof(T) : 1;
-  using VecT = typename std::conditional<
-      VEC, typename std::conditional<sizeof(T) == 4, float4, double2>::type, T>::type;
+  // the (up to) 4 fine rows, each L DOFs: a thread takes the same DOF
+  // offset in every row (12 loads in flight); rows past the grid are read at
+  // row 0 and not stored
   const int fx0 = 2 * cx0;
   const int L = 3 * (min(2 * (cx0 + w), gf.nx) - fx0);
-  const int64_t nv = 3 * ((int64_t)gf.nx * gf.ny * gf.nz);
-  int64_t rowb[4], cb[4];
+  int64_t rowb[4];
   bool rowok[4];
-  int nch = 0;
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     const int fy = 2 * j + (q & 1), fz = 2 * k + (q >> 1);
     rowok[q] = fy < gf.ny && fz < gf.nz;
     rowb[q] = rowok[q] ? 3 * (((int64_t)fz * gf.ny + fy) * gf.nx + fx0) : rowb[0];
-    cb[q] = rowb[q] / V;
-    nch = max(nch, (int)((rowb[q] + L + V - 1) / V - cb[q]));
   }
   const float sf = (float)s;
   T zq = T(0), zr = T(0);  // per-thread partials in the vectors' precision
-  for (int ch = threadIdx.x; ch < nch; ch += blockDim.x) {
-    T mv[4][V], rv[4][V], qv[4][V];
+  for (int dl = threadIdx.x; dl < L; dl += blockDim.x) {
+    const int fl = dl / 3, c = dl - 3 * fl;
+    const int ce = 3 * (fl >> 1) + c;
+    T mv[4], rv[4], qv[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      const int64_t d0 = (cb[q] + ch) * V;
-      if (d0 + V <= nv) {
-        *reinterpret_cast<VecT*>(mv[q]) = *reinterpret_cast<const VecT*>(minv + d0);
-        *reinterpret_cast<VecT*>(rv[q]) = *reinterpret_cast<const VecT*>(r + d0);
-        if (q_old)
-          *reinterpret_cast<VecT*>(qv[q]) = *reinterpret_cast<const VecT*>(q_old + d0);
-        else
-#pragma unroll
-          for (int e = 0; e < V; ++e) qv[q][e] = T(0);
-      } else {
-#pragma unroll
-        for (int e = 0; e < V; ++e) {
-          const bool in = d0 + e < nv;
-          mv[q][e] = in ? minv[d0 + e] : T(0);
-          rv[q][e] = in ? r[d0 + e] : T(0);
-          qv[q][e] = (in && q_old) ? q_old[d0 + e] : T(0);
-        }
-      }
+      mv[q] = minv[rowb[q] + dl];
+      rv[q] = r[rowb[q] + dl];
+      qv[q] = q_old ? q_old[rowb[q] + dl] : T(0);
     }
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       if (!rowok[q]) continue;
-      const int64_t d0 = (cb[q] + ch) * V;
-      T zo[V];
-      bool whole = true;
-#pragma unroll
-      for (int e = 0; e < V; ++e) {
-        const int dl = (int)(d0 + e - rowb[q]);
-        const bool mine = dl >= 0 && dl < L;
-        whole = whole && mine;
-        const int fl = mine ? dl / 3 : 0, c = mine ? dl - 3 * fl : 0;
-        const int ce = 3 * (fl >> 1) + c;
-        const float a = (fl & 1) ? 0.5f * (cyz[q][ce] + cyz[q][ce + 3]) : cyz[q][ce];
-        // the correction is BF16-accurate: formed in FP32
-        const T zi = mv[q][e] * rv[q][e] + (T)(sf * dinv_sqrt((float)mv[q][e]) * a);
-        zo[e] = zi;
-        if (mine) {
-          zq += zi * qv[q][e];
-          zr += zi * rv[q][e];
-        }
-      }
-      if (whole) {
-        *reinterpret_cast<VecT*>(z + d0) = *reinterpret_cast<const VecT*>(zo);
-      } else {
-#pragma unroll
-        for (int e = 0; e < V; ++e) {
-          const int dl = (int)(d0 + e - rowb[q]);
-          if (dl >= 0 && dl < L) z[d0 + e] = zo[e];
-        }
-      }
+      const float a = (fl & 1) ? 0.5f * (cyz[q][ce] + cyz[q][ce + 3]) : cyz[q][ce];
+      // the correction is BF16-accurate: formed in FP32
+      const T zi = mv[q] * rv[q] + (T)(sf * dinv_sqrt((float)mv[q]) * a);
+      z[rowb[q] + dl] = zi;
+      zq += zi * qv[q];
+      zr += zi * rv[q];
     }
   }
   if (!q_old) return;
@@ -803,9 +764,9 @@ void launch_restrict_ys(cudaStream_t s, const __nv_bfloat16* ys, const CgState* 
   static PerDeviceOnce configured;
   configured.run([&] {
     HX_CUDA(cudaFuncSetAttribute(k_restrict_ys, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)restrict_ys_smem(RES_CX)));
+                                 (int)restrict_ys_smem(YS_CX)));
   });
-  const int cxw = (int)cdiv(gc.nx, cdiv(gc.nx, RES_CX));
+  const int cxw = (int)cdiv(gc.nx, cdiv(gc.nx, YS_CX));
   const int kseg = ys_kseg(gc, cxw);
   const dim3 grid((unsigned)cdiv(gc.nx, cxw), (unsigned)cdiv(gc.ny, YS_JB),
                   (unsigned)cdiv(gc.nz, kseg));
@@ -850,16 +811,10 @@ void launch_net_output(cudaStream_t s, const T* r, const T* minv, const float* t
                        double* partials) {
   // two block partials per coarse row chunk: `partials` must hold
   // 2 net_output_blocks(gf) values
-  auto a16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
-  const bool vec = a16(r) && a16(minv) && a16(z) && (!q_old || a16(q_old));
   const int cxw = row_chunk(gc.nx);
   const dim3 grid((unsigned)cdiv(gc.nx, cxw), (unsigned)gc.ny, (unsigned)gc.nz);
-  if (vec)
-    k_net_output<T, true><<<grid, 256, 0, s>>>(r, minv, t, gf, gc, cxw, st, scale_mul, z, q_old,
-                                               partials);
-  else
-    k_net_output<T, false><<<grid, 256, 0, s>>>(r, minv, t, gf, gc, cxw, st, scale_mul, z,
-                                                q_old, partials);
+  k_net_output<T><<<grid, 256, 0, s>>>(r, minv, t, gf, gc, cxw, st, scale_mul, z, q_old,
+                                       partials);
   HX_CHECK_LAUNCH();
 }
 
