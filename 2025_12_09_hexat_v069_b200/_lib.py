@@ -117,6 +117,7 @@ PROTOTYPES = {
     "hx_net_forward_backward": (_i32, [_vp, _i32, _i32, _i32, _vp, _vp, _vp, _vp]),
     "hx_net_prepare": (_i32, [_vp, _vp]),
     "hx_net_apply": (_i32, [_vp, _vp, _vp]),
+    "hx_gmg_apply": (_i32, [_vp, _vp, _vp]),
     "hx_selftest_wait_timeout": (_i32, [_vp, C.POINTER(_i32)]),
     "hx_simp_device": (_i32, [_vp, _vp, _dbl, _dbl, _dbl, _vp]),
     "hx_sensitivity_device": (_i32, [_vp, _vp, _vp, _dbl, _dbl, _dbl, _vp]),
@@ -352,6 +353,10 @@ class Context:
     def net_apply(self, r_ptr, z_ptr):
         self.check(self.lib.hx_net_apply(self.h, C.c_void_p(r_ptr), C.c_void_p(z_ptr)),
                    "hx_net_apply")
+
+    def gmg_apply(self, r_ptr, z_ptr):
+        self.check(self.lib.hx_gmg_apply(self.h, C.c_void_p(r_ptr), C.c_void_p(z_ptr)),
+                   "hx_gmg_apply")
 
     def net_train_step(self, r_ptr, e_ptr, lr, loss_kind=0):
         loss = C.c_double()

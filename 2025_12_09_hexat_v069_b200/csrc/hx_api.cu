@@ -1057,6 +1057,18 @@ HX_API hx_status hx_net_apply(hx_ctx* c, const double* r, double* z) {
   });
 }
 
+HX_API hx_status hx_gmg_apply(hx_ctx* c, const double* r, double* z) {
+  return guard(c, [&] {
+    need_mesh(c);
+    HX_REQUIRE(r && z, "null argument");
+    HX_REQUIRE(c->gmg.ready && c->gmg.nl > 0 && c->gmg.lv[0].g.nodes() == c->g.nodes(),
+               "no multigrid hierarchy for this grid: run a multigrid solve first");
+    hx::gmg_vcycle<double>(c, r, z);
+    HX_CUDA(cudaStreamSynchronize(c->stream));
+    return HX_OK;
+  });
+}
+
 HX_API hx_status hx_net_train_step(hx_ctx* c, const double* r, const double* e, double lr,
                                    int32_t loss_kind, double* loss) {
   return hx_net_train_batch(c, &r, e ? &e : nullptr, 1, lr, loss_kind, loss);

@@ -461,6 +461,12 @@ HX_API hx_status hx_selftest_wait_timeout(hx_ctx *ctx, int32_t *detected);
 /* z = P r, the learned preconditioner of the prepared operator (FP64 device
  * vectors, grid numbering); z = 0 when r vanishes on the free DOFs. */
 HX_API hx_status hx_net_apply(hx_ctx *ctx, const double *r_dev, double *z_dev);
+/* z = V r, one V-cycle of the geometric multigrid preconditioner of the last
+ * multigrid-preconditioned solve (HX_PC_MULTIGRID) on this context: FP64
+ * device vectors, grid numbering, r zero on the fixed DOFs.  No reference
+ * counterpart (the reference's AMG is applied inside its solve only,
+ * src/Solvers/GPUSolver.jl:513-516).  HX_BAD_ARG before such a solve. */
+HX_API hx_status hx_gmg_apply(hx_ctx *ctx, const double *r_dev, double *z_dev);
 /* One Adam step on a residual (and error) of the prepared operator (FP64
  * device vectors, grid numbering; r = f - K x, e = u* - x).  With z the
  * preconditioned vector of r:  loss_kind 0: *loss = (z-e)^T K (z-e) / e^T K e

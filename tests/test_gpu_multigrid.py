@@ -73,3 +73,38 @@ def test_reference_shaped_solve_reports_gmg(ctx, hx):
     x, rel, name = api.solve_system_gpu(nodes, el, 1.0, 0.3, bc, f.astype(np.float32), dens,
                                         max_iter=60, tol=1e-7, shift_factor=1e-9, ctx=ctx)
     assert name == "GMG" and rel < 1e-7
+
+
+def test_vcycle_is_a_symmetric_linear_operator(ctx, hx):
+    """hx_gmg_apply after a multigrid solve: the V-cycle (Chebyshev smoothing
+    on a Lanczos lambda_max, direct coarsest solve) is linear and symmetric
+    up to FP32 rounding, positive on the free DOFs, and zero on the fixed
+    ones -- what flexible CG needs from a preconditioner."""
+    import torch
+    dims = (64, 16, 16)
+    nodes, el, bc, f, fac = _problem(ctx, hx, dims)
+    dev = torch.device("cuda", 0)
+    f_d = torch.from_numpy(f).to(dev)
+    fac_d = torch.from_numpy(fac).to(dev)
+    u = torch.zeros_like(f_d)
+    rep = ctx.solve_device(f_d.data_ptr(), fac_d.data_ptr(), u.data_ptr(),
+                           opts=hx.default_opts(tol=1e-8, preconditioner=3))
+    assert rep.status == 0 and rep.iterations < 40, rep.as_dict()
+    free = torch.from_numpy(bc.reshape(-1) == 0).to(dev)
+    g = torch.Generator(device="cpu").manual_seed(0)
+    r = [torch.randn(f_d.numel(), generator=g, dtype=torch.float64).to(dev) * free
+         for _ in range(2)]
+    z = []
+    for v in r:
+        out = torch.empty_like(v)
+        ctx.gmg_apply(v.data_ptr(), out.data_ptr())
+        z.append(out)
+    a, b = float(r[0] @ z[1]), float(r[1] @ z[0])
+    scale = np.sqrt(float(r[0] @ z[0]) * float(r[1] @ z[1]))
+    assert float(r[0] @ z[0]) > 0 and float(r[1] @ z[1]) > 0
+    assert abs(a - b) <= 1e-5 * scale, (a, b)
+    out = torch.empty_like(r[0])
+    ctx.gmg_apply((2 * r[0] + r[1]).data_ptr(), out.data_ptr())
+    ref = 2 * z[0] + z[1]
+    assert float(torch.linalg.norm(out - ref) / torch.linalg.norm(ref)) < 1e-5
+    assert not torch.any(z[0][~free])
