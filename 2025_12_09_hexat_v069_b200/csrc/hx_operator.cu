@@ -120,10 +120,6 @@ struct OpArgs {
   double* out;
 };
 
-// Ring slot of plane k >= -1.
-template <int N>
-__device__ __forceinline__ int ring(int k) { return (k + N) % N; }
-
 // 2D sum/difference transform of a node-plane face: v = corners (bx + 2by)
 // -> P = coefficients (sigma_x + 2 sigma_y).
 template <typename T>
@@ -219,11 +215,10 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
     ccv[q] = cc * V;
     cbase[q] = b * RS + ccv[q];
   }
-  // global index of a chunk's first value in plane kp (a multiple of V)
-  auto chunk_start = [&](int q, int64_t base) -> int64_t {
-    const int64_t o = base + row_off[q];
-    return o - (o & (V - 1)) + ccv[q];
-  };
+  // The first staged value of a chunk's row in plane kp has global index
+  // o = 3 nplane kp + row_off; the chunk's first value is o rounded down to
+  // a multiple of V plus ccv.
+  const int64_t P3 = 3 * nplane;
 
   // One commit group per call, empty for planes past k1, so that the
   // wait counts below hold to the end of the chunk.  Chunks outside the
@@ -232,21 +227,21 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
   // inside.  Other values outside the grid (halo nodes beyond a row's end,
   // halo rows beyond the plane) are copied as they lie in memory: they only
   // feed element columns with factor 0, whose products are zero.
-  auto issue = [&](int kp) {
+  auto issue = [&](int kp, int slp, int slr) {
     if (kp > k1) {
       cp_async_commit();
       return;
     }
     const bool kin = kp >= 0 && kp < g.nzn;
-    const int64_t base = (int64_t)kp * nplane * 3;
-    const unsigned sp = smem_u32(&sm.p[ring<NP>(kp)][0]);
-    const unsigned sr = smem_u32(&sm.r[FUSED ? ring<NR>(kp) : 0][0]);
-    const unsigned smv = smem_u32(&sm.m[FUSED ? ring<NR>(kp) : 0][0]);
-    const unsigned sx = smem_u32(&sm.x[FUSED ? ring<NR>(kp) : 0][0]);
+    const unsigned sp = smem_u32(&sm.p[slp][0]);
+    const unsigned sr = smem_u32(&sm.r[FUSED ? slr : 0][0]);
+    const unsigned smv = smem_u32(&sm.m[FUSED ? slr : 0][0]);
+    const unsigned sx = smem_u32(&sm.x[FUSED ? slr : 0][0]);
 #pragma unroll
     for (int q = 0; q < NCT; ++q) {
       if (q == NCT - 1 && tid + q * NT >= NCH) continue;
-      const int64_t s = chunk_start(q, base);
+      const int64_t o = (int64_t)kp * P3 + row_off[q];
+      const int64_t s = o - (o & (V - 1)) + ccv[q];
       const int64_t left = ndof - s;
       const unsigned bytes =
           (kin && s >= 0 && left > 0) ? (unsigned)((left < V ? left : (int64_t)V) * sizeof(T)) : 0u;
@@ -266,17 +261,17 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
   // by chunk; the values of owned nodes of owned planes are stored to p and
   // advance x with the old direction (16-byte stores where a whole chunk is
   // owned).
-  auto transform = [&](int kp) {
+  auto transform = [&](int kp, int slp, int slr) {
     if (!FUSED) return;
     const bool kown = kp >= k0 && kp < k1;
-    const int64_t base = (int64_t)kp * nplane * 3;
-    T* ps = &sm.p[ring<NP>(kp)][0];
-    const T* rs = &sm.r[ring<NR>(kp)][0];
-    const T* ms = &sm.m[ring<NR>(kp)][0];
-    const T* xs = &sm.x[ring<NR>(kp)][0];
+    T* ps = &sm.p[slp][0];
+    const T* rs = &sm.r[slr][0];
+    const T* ms = &sm.m[slr][0];
+    const T* xs = &sm.x[slr][0];
 #pragma unroll
     for (int q = 0; q < NCT; ++q) {
       if (q == NCT - 1 && tid + q * NT >= NCH) continue;
+      const int64_t ob = (int64_t)kp * P3 + row_off[q];
       const int o = cbase[q];
       T pnew[V], xv[V];
       {
@@ -297,8 +292,8 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
       }
       *reinterpret_cast<VecT*>(ps + o) = *reinterpret_cast<const VecT*>(pnew);
       if (!kown || !((own_rows >> q) & 1u)) continue;
-      const int64_t s = chunk_start(q, base);
-      const int64_t lo = base + row_off[q] + 3, hi = lo + own_len;
+      const int64_t s = ob - (ob & (V - 1)) + ccv[q];
+      const int64_t lo = ob + 3, hi = lo + own_len;
       if (s >= lo && s + V <= hi) {
         *reinterpret_cast<VecT*>(A.pout + s) = *reinterpret_cast<const VecT*>(pnew);
         *reinterpret_cast<VecT*>(A.x + s) = *reinterpret_cast<const VecT*>(xv);
@@ -314,14 +309,14 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
   };
 
   // Shared-memory offsets of this thread's nodes (lx, ly) and (lx, ly + 1)
-  // in plane kp: row start + the row's lead in that plane (see Stage) + 3 lx.
+  // in a plane: row start + the row's lead in that plane (see Stage) + 3 lx.
+  // The leads of planes ke and ke + 1 advance by 3 nplane mod V per plane.
   const int rowA = 3 * (jn * g.nxn + i0 - 1), rowB = rowA + 3 * g.nxn;
-  auto offA = [&](int kp) -> int {
-    return ly * RS + (int)(((int64_t)kp * nplane * 3 + rowA) & (V - 1)) + 3 * lx;
-  };
-  auto offB = [&](int kp) -> int {
-    return (ly + 1) * RS + (int)(((int64_t)kp * nplane * 3 + rowB) & (V - 1)) + 3 * lx;
-  };
+  const int p3m = (int)(P3 & (V - 1));
+  int lA0 = (int)(((int64_t)(k0 - 1) * P3 + rowA) & (V - 1));
+  int lB0 = (int)(((int64_t)(k0 - 1) * P3 + rowB) & (V - 1));
+  int lA1 = (lA0 + p3m) & (V - 1), lB1 = (lB0 + p3m) & (V - 1);
+  const int baseA = ly * RS + 3 * lx, baseB = (ly + 1) * RS + 3 * lx;
   // the four corners (bx + 2 by) of component c of the element face
   auto face = [&](const T* ps, int a, int b, int c, T (&v)[4]) {
     v[0] = ps[a + c];
@@ -330,16 +325,22 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
     v[3] = ps[b + 3 + c];
   };
 
+  // Ring slots: plane kp sits in slot (kp - k0 + 1) mod NP of the p ring
+  // and mod NR of the r / M^-1 / x ring.
   // prologue: planes k0-1 .. k0+PF-3 requested (one group each); k0-1 and
   // k0 staged and transformed; then k0+PF-2 into the r/M^-1/x slot of k0-1
 #pragma unroll
-  for (int d = -1; d <= PF - 3; ++d) issue(k0 + d);
+  for (int d = 0; d <= PF - 2; ++d) issue(k0 - 1 + d, d, d % NR);
   cp_async_wait<PF - 3>();
   __syncthreads();
-  transform(k0 - 1);
-  transform(k0);
+  transform(k0 - 1, 0, 0);
+  transform(k0, 1, 1 % NR);
   __syncthreads();
-  issue(k0 + PF - 2);
+  issue(k0 + PF - 2, PF - 1, (PF - 1) % NR);
+  // slots of iteration it = ke - k0 + 1: planes ke (c0), ke+1 (c1), ke+2
+  // (c2, r2: transformed), ke+PF (cm = slot of ke-1, r1: issued)
+  int c0 = 0, c1 = 1, c2 = 2, cm = NP - 1, r2 = 2 % NR, r1 = 1 % NR;
+  auto step = [](int v, int n) { return v + 1 == n ? 0 : v + 1; };
   T Ytp[3][4];
 #pragma unroll
   for (int c = 0; c < 3; ++c)
@@ -385,12 +386,12 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
     }
     cp_async_wait<PF - 3>();  // groups up to ke+2 complete
     __syncthreads();  // A: planes ke, ke+1 ready; ke+2 landed; ke-1 and red consumed
-    if (ke + 2 <= k1) transform(ke + 2);
-    issue(ke + PF);  // into the slot of plane ke-1
+    if (ke + 2 <= k1) transform(ke + 2, c2, r2);
+    issue(ke + PF, cm, r1);  // into the slot of plane ke-1
 
-    const T* pl0 = &sm.p[ring<NP>(ke)][0];
-    const T* pl1 = &sm.p[ring<NP>(ke + 1)][0];
-    const int a0 = offA(ke), a1 = offA(ke + 1), b1 = offB(ke + 1);
+    const T* pl0 = &sm.p[c0][0];
+    const T* pl1 = &sm.p[c1][0];
+    const int a0 = baseA + lA0, a1 = baseA + lA1, b1 = baseB + lB1;
     T U[3][8];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -399,7 +400,7 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
 #pragma unroll
         for (int q = 0; q < 4; ++q) Pb[q] = Pcarry[c][q];
       } else {
-        face(pl0, a0, offB(ke), c, v);
+        face(pl0, a0, baseB + lB0, c, v);
         face_fwd(v, Pb);
       }
       face(pl1, a1, b1, c, v);
@@ -459,6 +460,16 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
       }
       if (MODE != 0) dsum += (double)pdot;
     }
+    c0 = step(c0, NP);
+    c1 = step(c1, NP);
+    c2 = step(c2, NP);
+    cm = step(cm, NP);
+    r2 = step(r2, NR);
+    r1 = step(r1, NR);
+    lA0 = lA1;
+    lB0 = lB1;
+    lA1 = (lA1 + p3m) & (V - 1);
+    lB1 = (lB1 + p3m) & (V - 1);
   }
 
   if (MODE == 4) {
