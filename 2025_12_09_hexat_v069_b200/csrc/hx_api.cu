@@ -34,6 +34,15 @@ hx_status guard(hx_ctx* c, F&& f) {
       c->err = std::string("cudaSetDevice: ") + cudaGetErrorString(e);
       return HX_CUDA_ERROR;
     }
+    // The context's stream does not synchronise with the legacy default
+    // stream by itself; every call first waits for the work queued there
+    // (device inputs written by, e.g., PyTorch's default stream).
+    e = cudaEventRecord(c->ev_in, cudaStreamLegacy);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, c->ev_in, 0);
+    if (e != cudaSuccess) {
+      c->err = std::string("ordering after the default stream: ") + cudaGetErrorString(e);
+      return HX_CUDA_ERROR;
+    }
     hx_status s = f();
     if (s == HX_OK) c->err.clear();
     return s;
@@ -324,8 +333,10 @@ HX_API hx_status hx_create(hx_ctx** out, int32_t device) {
   if (!c) return HX_OOM;
   c->device = device;
   if (cudaSetDevice(device) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_in, cudaEventDisableTiming) != cudaSuccess) {
     cudaGetLastError();
+    if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return HX_CUDA_ERROR;
   }
@@ -344,6 +355,7 @@ HX_API void hx_destroy(hx_ctx* c) {
     if (c->net.ev_x[i]) cudaEventDestroy(c->net.ev_x[i]);
   }
   if (c->net.ev_fork) cudaEventDestroy(c->net.ev_fork);
+  if (c->ev_in) cudaEventDestroy(c->ev_in);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }

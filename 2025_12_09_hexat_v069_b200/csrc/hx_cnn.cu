@@ -383,6 +383,7 @@ constexpr int YS_CX = 85;  // coarse cells per chunk: 3 x 85 = 255 threads
 constexpr int YS_JB = 4;
 constexpr int YS_NY = 2 * YS_JB + 1;  // staged fine y-rows per plane
 constexpr int YS_RING = 4;            // staged planes: the one in use and 3 ahead
+constexpr int YS_CPT = (YS_NY * (3 * (2 * YS_CX + 1) / 8 + 3) + 255) / 256;  // chunks per thread
 
 __device__ __forceinline__ float bf16_bits(unsigned short h) { return __uint_as_float((unsigned)h << 16); }
 
@@ -406,23 +407,43 @@ __global__ void __launch_bounds__(256)
   const int np = pb - pa + 1;
   const uint4* yc = reinterpret_cast<const uint4*>(ys);
   auto row_in = [&](int ry) { return fy0 + ry >= 0 && fy0 + ry < gf.ny; };
-  auto stage = [&](int p, int slot) {
-    for (int u = threadIdx.x; u < YS_NY * segc; u += blockDim.x) {
-      const int ry = u / segc, cu = u - ry * segc;
-      if (!row_in(ry)) continue;
-      const int64_t e0 = 3 * (((int64_t)p * gf.ny + fy0 + ry) * gf.nx + fxa);
-      const int64_t c0 = e0 >> 3, c1 = (e0 + L + 7) >> 3;
-      if (cu < c1 - c0)
+  // Staged row ry of plane p starts at entry e(p, ry) = 3 ((p ny + fy0 + ry)
+  // nx + fxa); planes are staged in order, so each of this thread's chunks
+  // (YS_CPT of them, fixed row and chunk index) keeps e of its row in its
+  // next plane and advances it by one plane (PN entries) per staging.
+  const int64_t PN = 3LL * gf.ny * gf.nx;
+  int s_cu[YS_CPT], s_dst[YS_CPT];
+  int64_t s_e[YS_CPT];
+#pragma unroll
+  for (int i = 0; i < YS_CPT; ++i) {
+    const int u = threadIdx.x + i * 256;
+    const int ry = u / segc;
+    s_cu[i] = (u < YS_NY * segc && row_in(ry)) ? u - ry * segc : -1;  // -1: no chunk
+    s_dst[i] = ry * segc + (u - ry * segc);
+    s_e[i] = 3 * (((int64_t)pa * gf.ny + fy0 + ry) * gf.nx + fxa);
+  }
+  auto stage = [&](int slot) {
+#pragma unroll
+    for (int i = 0; i < YS_CPT; ++i) {
+      const int64_t e0 = s_e[i];
+      s_e[i] = e0 + PN;
+      if (s_cu[i] < 0) continue;
+      const int64_t c0 = e0 >> 3;
+      if (s_cu[i] < (int)(((e0 + L + 7) >> 3) - c0))
         asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(
-                         (unsigned)__cvta_generic_to_shared(sc + (slot * YS_NY + ry) * segc + cu)),
-                     "l"(yc + c0 + cu));
+                         (unsigned)__cvta_generic_to_shared(sc + slot * YS_NY * segc + s_dst[i])),
+                     "l"(yc + c0 + s_cu[i]));
     }
   };
 #pragma unroll
   for (int i = 0; i < YS_RING - 1; ++i) {
-    if (i < np) stage(pa + i, i);
+    if (i < np) stage(i);
     asm volatile("cp.async.commit_group;\n" ::);
   }
+  // lead of staged row ry in plane p: e(p, ry) mod 8 = (lb(p) + ry rs) mod 8,
+  // lb advancing by PN mod 8 per plane
+  const int rs = (int)((3LL * gf.nx) & 7), pn8 = (int)(PN & 7);
+  int lb = (int)((pa * PN + 3 * ((int64_t)fy0 * gf.nx + fxa)) & 7);
   // this thread's coarse cell and component; its fine x-nodes fx-1, fx,
   // fx+1 (a missing neighbour reads the centre with weight 0)
   const int t = threadIdx.x;
@@ -460,7 +481,7 @@ __global__ void __launch_bounds__(256)
     const int p = pa + i, slot = i % YS_RING;
     asm volatile("cp.async.wait_group %0;\n" ::"n"(YS_RING - 2) : "memory");
     __syncthreads();  // plane p landed for every thread; slot of plane p-1 free
-    if (i + YS_RING - 1 < np) stage(p + YS_RING - 1, (i + YS_RING - 1) % YS_RING);
+    if (i + YS_RING - 1 < np) stage((i + YS_RING - 1) % YS_RING);
     asm volatile("cp.async.commit_group;\n" ::);
     const unsigned short* sp =
         reinterpret_cast<const unsigned short*>(sc + slot * YS_NY * segc);
@@ -470,8 +491,7 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
     for (int ry = 0; ry < YS_NY; ++ry) {
       if (!row_in(ry)) continue;
-      const int64_t e0 = 3 * (((int64_t)p * gf.ny + fy0 + ry) * gf.nx + fxa);
-      const unsigned short* rp = sp + ry * segc * 8 + (int)(e0 & 7);
+      const unsigned short* rp = sp + ry * segc * 8 + ((lb + ry * rs) & 7);
       const float xv = bf16_bits(rp[ic]) + wl * bf16_bits(rp[il]) + wr * bf16_bits(rp[ir]);
       // staged row ry is fine row 2 (j0 + jj) + d with d = ry - 1 - 2 jj
 #pragma unroll
@@ -481,6 +501,7 @@ __global__ void __launch_bounds__(256)
         else if (d == 1 || d == -1) vy[jj] += 0.5f * xv;
       }
     }
+    lb = (lb + pn8) & 7;
     const int kp = p >> 1;
     const bool odd = p & 1;
     if ((kp & 1) == 0) zstep(accE, accO, vy, kp, odd);

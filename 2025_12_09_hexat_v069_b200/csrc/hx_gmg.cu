@@ -8,7 +8,8 @@
 // Hierarchy: level l+1 halves every element count of level l (built while
 // all three are even); its element factor is the mean of its 8 children and
 // its element size doubles, so the coarse operator is the same matrix-free
-// structured operator (hx_operator.cu) on the coarse grid.  A coarse node is
+// structured operator (hx_operator.cu) on the coarse grid, with 8 times the
+// finer level's diagonal shift.  A coarse node is
 // the fine node at twice its index; it is fixed where that fine node's BC
 // bit is set, and nodes without stiffness are held at 0 as on level 0.
 // Transfers: trilinear prolongation P and its exact transpose R = P^T
@@ -370,12 +371,17 @@ void gmg_setup(hx_ctx* c, const double* fac, double shift) {
       HX_CHECK_LAUNCH();
       k_coarse_bc<<<gblocks(nn), 256, 0, s>>>(F.bc.p, bc, F.g, g);
       HX_CHECK_LAUNCH();
+      // the fine level's shift s I seen through the transfers: P^T (s I) P
+      // has row sums 8 s (trilinear P), so a coarse level carries 8 times
+      // its parent's shift on the diagonal.  A shift that regularises a
+      // free rigid mode on the mesh then keeps the coarse operators (and
+      // the dense coarsest inverse) nonsingular too.
+      L.shift = 8.f * F.shift;
       put_state(c, 3, CgState{});
       launch_node_diag<float>(s, fl, bc, nm, minv, g, make_elem_coef(h[0], h[1], h[2], c->nu),
                               c->d_partials.p, c->d_state.p + 3, c->d_scalars.p);
-      launch_minv<float>(s, nm, minv, minv, nn, 0.0);
+      launch_minv<float>(s, nm, minv, minv, nn, (double)L.shift);
       HX_CUDA(cudaStreamSynchronize(s));  // the pinned state mirror is reused below
-      L.shift = 0.f;
     }
     G.nl = l + 1;
     const bool even = g.nxe % 2 == 0 && g.nye % 2 == 0 && g.nze % 2 == 0;

@@ -166,6 +166,7 @@ void launch_oc(cudaStream_t s, const double* x, const double* dc, const double* 
 struct hx_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaEvent_t ev_in = nullptr;  // orders the stream after the legacy default stream
   std::string err;
 
   // mesh

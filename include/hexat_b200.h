@@ -15,6 +15,11 @@
  *    (dof = 3*node + component);  per-element arrays have length nE.
  *  - Every call is blocking: results are in the caller's buffers on return.
  *    The caller owns all buffers; no pointer is retained after a call.
+ *  - Device-array calls read their inputs on the context's own stream.  Each
+ *    call first orders that stream after the work already queued on the
+ *    legacy default CUDA stream (stream 0, where e.g. PyTorch queues by
+ *    default); inputs written on any other stream must be complete (the
+ *    caller synchronises that stream first).
  *  - Every call returns an hx_status and never throws across the ABI.
  *    hx_last_error() describes the last failure of a context.
  *  - Nothing falls back to the CPU: without a usable device, calls return

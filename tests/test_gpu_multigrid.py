@@ -99,6 +99,7 @@ def test_vcycle_is_a_symmetric_linear_operator(ctx, hx):
         out = torch.empty_like(v)
         ctx.gmg_apply(v.data_ptr(), out.data_ptr())
         z.append(out)
+    # (each call waits for the default stream, where torch wrote r)
     a, b = float(r[0] @ z[1]), float(r[1] @ z[0])
     scale = np.sqrt(float(r[0] @ z[0]) * float(r[1] @ z[1]))
     assert float(r[0] @ z[0]) > 0 and float(r[1] @ z[1]) > 0
