@@ -683,14 +683,21 @@ static CgState learned_fcg(hx_ctx* c, const double* fac, const double* b, double
 // from the current iterate when FCG breaks down or stalls (stagnation is
 // measured on the true residual).
 // ---------------------------------------------------------------------------
+// multigrid: the FP32 V-cycle (hx_gmg.cu) as the variable preconditioner
+// in place of the networks; everything else is shared.
 static CgState learned_fcg_mixed(hx_ctx* c, const double* fac, const double* b, double* x,
                                  bool warm, double shift, const hx_solve_opts& o, double t0,
-                                 bool* timed_out, int* fallback, int* iters_out) {
-  HX_REQUIRE(c->net.ready, "learned preconditioner requested but no network is loaded");
+                                 bool* timed_out, int* fallback, int* iters_out,
+                                 bool multigrid = false) {
+  HX_REQUIRE(multigrid || c->net.ready,
+             "learned preconditioner requested but no network is loaded");
   auto& N = c->net;
   const Grid& g = c->g;
   const int64_t n = g.dofs(), ne = g.elems();
-  net_operator_inputs(c, fac);
+  if (multigrid)
+    gmg_setup(c, fac, shift);
+  else
+    net_operator_inputs(c, fac);
   float* fac32 = c->d_fac32.ensure(ne);
   float* minv32 = c->d_minv32.ensure(n);
   float* r32 = c->d_r32.ensure(n);
@@ -759,15 +766,20 @@ static CgState learned_fcg_mixed(hx_ctx* c, const double* fac, const double* b, 
   int best_it = 0;
   bool stalled = false;
   CgState sf{};
-  __nv_bfloat16* ys = N.ys.ensure(n + 8);
+  __nv_bfloat16* ys = multigrid ? nullptr : N.ys.ensure(n + 8);
   for (;;) {
     float* Pin = parity ? P0 : P1;
     float* Pout = parity ? P1 : P0;
     // ys = BF16(D^-1/2 r32) of the (replaced) residual; then every residual
     // update keeps it current
-    launch_dinv_bf16<float>(c->stream, r32, minv32, ys, n);
+    if (!multigrid) launch_dinv_bf16<float>(c->stream, r32, minv32, ys, n);
     auto one = [&](float* pi, float* po) {
-      precond_z<float>(c, r32, minv32, si, scale_mul, z32, q32, false, ys);
+      if (multigrid) {
+        gmg_vcycle<float>(c, r32, z32);
+        launch_fcg_coeffs<float>(c->stream, z32, q32, r32, n, c->d_partials.p, si);
+      } else {
+        precond_z<float>(c, r32, minv32, si, scale_mul, z32, q32, false, ys);
+      }
       launch_fcg_step<float>(c->stream, pi, po, z32, d32, q32, fac32, c->d_nmask.p, g, K32,
                              sh32, si, c->d_partials.p);
       launch_cg_update2<float>(c->stream, r32, q32, minv32, n, si, c->d_partials.p, ys);
@@ -855,6 +867,13 @@ CgState solve_learned_mixed(hx_ctx* c, const double* fac, const double* b, doubl
       learned_fcg_mixed(c, fac, b, x, warm, shift, o, t0, timed_out, fallback, iters_out);
   check_conv_error(c);
   return s;
+}
+
+CgState solve_gmg_mixed(hx_ctx* c, const double* fac, const double* b, double* x, bool warm,
+                        double shift, const hx_solve_opts& o, double t0, bool* timed_out,
+                        int* fallback, int* iters_out) {
+  return learned_fcg_mixed(c, fac, b, x, warm, shift, o, t0, timed_out, fallback, iters_out,
+                           true);
 }
 
 // FP64 Jacobi-PCG from zero, storing x every `every` iterations (at most

@@ -457,8 +457,6 @@ hx_status solve_grid(hx_ctx* c, const double* f, const double* fac, double* u,
   HX_REQUIRE(o.preconditioner == HX_PC_JACOBI || o.preconditioner == HX_PC_LEARNED ||
                  o.preconditioner == HX_PC_MULTIGRID,
              "unknown preconditioner");
-  HX_REQUIRE(o.preconditioner != HX_PC_MULTIGRID || o.precision == HX_PREC_FP64,
-             "the multigrid preconditioner runs with FP64 vectors");
   HX_REQUIRE(o.preconditioner != HX_PC_LEARNED || o.precision == HX_PREC_FP64 ||
                  o.precision == HX_PREC_MIXED32,
              "the learned preconditioner runs with FP64 or FP32 (mixed) vectors");
@@ -511,9 +509,16 @@ hx_status solve_grid(hx_ctx* c, const double* f, const double* fac, double* u,
       R.fallback_used = fb;
     } else if (use_mg) {
       int its = 0;
-      st = solve_gmg(c, fac, b, u, warm, shift, o, t0, &timed_out, &its);
+      if (o.precision == HX_PREC_FP64) {
+        st = solve_gmg(c, fac, b, u, warm, shift, o, t0, &timed_out, &its);
+        if (o.preconditioner != HX_PC_MULTIGRID) R.fallback_used = 1;
+      } else {
+        int fb = 0;
+        st = solve_gmg_mixed(c, fac, b, u, warm, shift, o, t0, &timed_out, &fb, &its);
+        R.refinements = c->h_state[0].iter;
+        R.fallback_used = fb || o.preconditioner != HX_PC_MULTIGRID;
+      }
       total_iters += its;
-      if (o.preconditioner != HX_PC_MULTIGRID) R.fallback_used = 1;
     } else if (o.precision == HX_PREC_FP64) {
       st = pcg_fp64(c, fac, b, u, warm, shift, o, t0, &timed_out);
       total_iters += st.iter;

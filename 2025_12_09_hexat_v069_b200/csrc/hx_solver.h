@@ -45,6 +45,11 @@ CgState solve_learned(hx_ctx* c, const double* fac, const double* b, double* x, 
 CgState solve_learned_mixed(hx_ctx* c, const double* fac, const double* b, double* x, bool warm,
                             double shift, const hx_solve_opts& o, double t0, bool* timed_out,
                             int* fallback, int* iters_out);
+// Mixed-precision flexible CG with the multigrid V-cycle (hx_net.cu's FP32
+// loop with FP64 reliable updates; Jacobi-PCG finishes a stalled solve).
+CgState solve_gmg_mixed(hx_ctx* c, const double* fac, const double* b, double* x, bool warm,
+                            double shift, const hx_solve_opts& o, double t0, bool* timed_out,
+                            int* fallback, int* iters_out);
 CgState solve_mixed(hx_ctx* c, const double* fac, const double* b, double* x, bool warm,
                     double shift, const hx_solve_opts& o, double t0, bool* timed_out,
                     int* inner_total);

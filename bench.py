@@ -130,11 +130,13 @@ def c1_inputs(hx, ctx, dims=DIMS):
 
 
 FORMS = {"fp64_jacobi": (0, 0), "mixed32_jacobi": (1, 0), "fp64_learned_fcg": (0, 1),
-         "mixed32_learned_fcg": (1, 1), "fp64_multigrid_fcg": (0, 3)}
+         "mixed32_learned_fcg": (1, 1), "fp64_multigrid_fcg": (0, 3),
+         "mixed32_multigrid_fcg": (1, 3)}
 DTYPES = {"fp64_jacobi": "f64", "mixed32_jacobi": "f32 in f64 reliable updates",
           "fp64_learned_fcg": "f64 vectors, bf16 network",
           "mixed32_learned_fcg": "f32 vectors in f64 reliable updates, bf16 network",
-          "fp64_multigrid_fcg": "f64 vectors, f32 V-cycle"}
+          "fp64_multigrid_fcg": "f64 vectors, f32 V-cycle",
+          "mixed32_multigrid_fcg": "f32 vectors in f64 reliable updates, f32 V-cycle"}
 
 
 def run_ours(args):

@@ -63,7 +63,8 @@ typedef enum hx_preconditioner {
   HX_PC_LEARNED = 1, /* CNN preconditioner inside flexible CG (needs weights) */
   HX_PC_NONE = 2,
   HX_PC_MULTIGRID = 3 /* geometric multigrid V-cycle (FP32) inside flexible CG
-                         (FP64 vectors): the GPU replacement of the reference's
+                         (FP64 vectors, or FP32 with FP64 reliable updates under
+                         HX_PREC_MIXED32): the GPU replacement of the reference's
                          CPU algebraic multigrid (GPUSolver.jl:168-268) */
 } hx_preconditioner;
 

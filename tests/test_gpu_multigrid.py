@@ -109,3 +109,21 @@ def test_vcycle_is_a_symmetric_linear_operator(ctx, hx):
     ref = 2 * z[0] + z[1]
     assert float(torch.linalg.norm(out - ref) / torch.linalg.norm(ref)) < 1e-5
     assert not torch.any(z[0][~free])
+
+
+def test_mixed_precision_multigrid_fcg(ctx, hx, orc):
+    """FP32 flexible CG with FP64 reliable updates around the V-cycle reaches
+    the FP64 true residual and the oracle's solution."""
+    dims = (64, 16, 16)
+    nodes, el, bc, f, fac = _problem(ctx, hx, dims)
+    uj, rj = ctx.solve(f, fac, tol=1e-10, max_iter=100000)
+    um, rm = ctx.solve(f, fac, tol=1e-8, max_iter=100000, precision=1, preconditioner=3)
+    assert rm.status == 0 and rm.true_rel_res < 1e-8 and rm.fallback_used == 0, rm.as_dict()
+    assert rm.iterations < 60, rm.as_dict()
+    c0 = hx.mesh.connectivity0(el)
+    ke = orc.canonical_ke()
+    free = orc.free_mask_from(bc, orc.diagonal(c0, nodes.shape[0], ke, fac))
+    ku = orc.apply_stiffness(c0, nodes.shape[0], ke, fac, um)
+    b = f * free
+    assert np.linalg.norm((b - ku) * free) / np.linalg.norm(b) < 1e-8
+    assert np.abs(um - uj).max() <= 1e-5 * np.abs(uj).max()
