@@ -137,6 +137,15 @@ __global__ void k_rand_vec(float* __restrict__ v, const uint8_t* __restrict__ nm
   }
 }
 
+// (alpha, beta, status) of the last PCG step, for the lambda_max estimate
+__global__ void k_record_step(const CgState* st, double* out) {
+  if (threadIdx.x == 0) {
+    out[0] = st->alpha;
+    out[1] = st->beta;
+    out[2] = (double)st->status;
+  }
+}
+
 // fresh coarse-solve state (inside a captured cycle: no host round trip)
 __global__ void k_coarse_reset(CgState* st, int max_iter, double tol) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
@@ -413,18 +422,28 @@ void gmg_setup(hx_ctx* c, const double* fac, double shift) {
     launch_fill_zero(s, L.x.p, n * sizeof(float));
     put_state(c, 3, fresh_state(0.0, 1 << 30, 1, false, false));
     launch_cg_init<float>(s, L.b.p, nullptr, L.minv.p, L.r.p, G.p1.p, n, st, c->d_partials.p);
-    std::vector<double> al, be;
+    // all steps queued at once; each leaves (alpha, beta, status) in rec
+    double* rec = G.lanczos.ensure(3 * GMG_LANCZOS);
     for (int it = 0; it < GMG_LANCZOS; ++it) {
       float* pin = (it % 2 == 0) ? G.p1.p : G.p0.p;
       float* pout = (it % 2 == 0) ? G.p0.p : G.p1.p;
       launch_pcg_step<float>(s, pin, pout, L.r.p, L.minv.p, L.x.p, L.q.p, L.fac.p, L.nmask.p, L.g,
                              L.K, L.shift, st, c->d_partials.p);
       launch_cg_update2<float>(s, L.r.p, L.q.p, L.minv.p, n, st, c->d_partials.p);
-      const CgState h = get_state(c, 3);
-      if (!(h.alpha > 0.0) || !std::isfinite(h.alpha)) break;
-      al.push_back(h.alpha);
-      be.push_back(h.beta);
-      if (h.status != HX_RUNNING) break;
+      k_record_step<<<1, 32, 0, s>>>(st, rec + 3 * it);
+      HX_CHECK_LAUNCH();
+    }
+    double h[3 * GMG_LANCZOS];
+    HX_CUDA(cudaMemcpyAsync(h, rec, sizeof(h), cudaMemcpyDeviceToHost, s));
+    HX_CUDA(cudaStreamSynchronize(s));
+    std::vector<double> al, be;
+    for (int it = 0; it < GMG_LANCZOS; ++it) {
+      const double a = h[3 * it], bt = h[3 * it + 1];
+      const int stt = (int)h[3 * it + 2];
+      if (stt == HX_ST_BREAKDOWN || !(a > 0.0) || !std::isfinite(a)) break;
+      al.push_back(a);
+      be.push_back(bt);
+      if (stt != HX_RUNNING) break;
     }
     L.lmax = al.empty() ? 2.0f : (float)lanczos_max(al, be);
   }
