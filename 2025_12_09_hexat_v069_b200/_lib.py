@@ -40,7 +40,8 @@ class SolveReport(C.Structure):
         ("rel_res", C.c_double), ("true_rel_res", C.c_double), ("shift", C.c_double),
         ("time_setup_ms", C.c_double), ("time_solve_ms", C.c_double),
         ("time_total_ms", C.c_double), ("time_device_ms", C.c_double),
-        ("kernel_launches", C.c_double), ("reserved", C.c_double * 2),
+        ("kernel_launches", C.c_double), ("time_precond_setup_ms", C.c_double),
+        ("reserved", C.c_double * 1),
     ]
 
     def as_dict(self):

@@ -29,6 +29,7 @@
 // cycle is symmetric positive definite up to FP32 rounding (and a PCG coarse
 // solve's early stop), which the flexible CG around it absorbs (Notay's FCG,
 // the same step kernels as the learned preconditioner).
+#include <chrono>
 #include <cmath>
 #include <limits>
 #include <vector>
@@ -347,6 +348,7 @@ GridN node_grid(const Grid& g) { return GridN{g.nxn, g.nyn, g.nzn}; }
 // ---------------------------------------------------------------------------
 void gmg_setup(hx_ctx* c, const double* fac, double shift) {
   auto& G = c->gmg;
+  const auto t_start = std::chrono::steady_clock::now();
   cudaStream_t s = c->stream;
   G.nl = 0;
   Grid g = c->g;
@@ -485,6 +487,8 @@ void gmg_setup(hx_ctx* c, const double* fac, double shift) {
   G.p1.ensure(G.lv[G.nl - 1].g.dofs());
   G.ready = true;
   HX_CUDA(cudaStreamSynchronize(s));
+  G.setup_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() -
+                                                          t_start).count();
 }
 
 // Chebyshev smoothing of A x = b on level L (GMG_DEGREE steps): from x = 0

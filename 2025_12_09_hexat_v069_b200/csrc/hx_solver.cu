@@ -466,6 +466,7 @@ hx_status solve_grid(hx_ctx* c, const double* f, const double* fac, double* u,
   const int64_t n = g.dofs();
   double* b = c->d_b.ensure(n);
   hx_solve_report R{};
+  c->gmg.setup_ms = 0;
   const int attempts = o.ref_retry ? 3 : 1;
   double factor = o.shift_factor;
   double maxd = 0, shift = 0;
@@ -621,6 +622,7 @@ hx_status solve_grid(hx_ctx* c, const double* f, const double* fac, double* u,
   R.time_setup_ms = t_setup;
   R.time_total_ms = now_ms() - t0;
   R.time_solve_ms = R.time_total_ms - t_setup;
+  R.time_precond_setup_ms = c->gmg.setup_ms;
   if (rep) *rep = R;
   return (hx_status)R.status;
 }

@@ -112,7 +112,9 @@ typedef struct hx_solve_report {
   double time_total_ms;
   double time_device_ms;   /* CUDA-event time of the call on the context stream */
   double kernel_launches;  /* kernels launched by the call (graph nodes included) */
-  double reserved[2];
+  double time_precond_setup_ms; /* multigrid hierarchy set-up (part of time_solve_ms;
+                                   0 for the other preconditioners) */
+  double reserved[1];
 } hx_solve_report;
 
 typedef struct hx_ctx hx_ctx;
