@@ -23,7 +23,7 @@
 // estimate from Jacobi-PCG steps at set-up), from zero before the restriction and from the
 // prolonged correction after it.  The coarsest level, when it has at most
 // GMG_DIRECT_DOFS DOFs, is solved by its dense inverse: assembled from the
-// element matrices and inverted by Gauss-Jordan in FP64 at set-up, applied
+// element matrices and inverted by blocked Gauss-Jordan in FP64 at set-up, applied
 // as one FP32 matrix-vector product per cycle; a larger coarsest level gets
 // GMG_COARSE_ITERS iterations of FP32 Jacobi-PCG on the fused kernels.  The
 // cycle is symmetric positive definite up to FP32 rounding (and a PCG coarse
@@ -244,39 +244,75 @@ __global__ void k_dense_mask(double* __restrict__ A, const uint8_t* __restrict__
   }
 }
 
-// row and column `k` of A into rk, ck (the first pivot's, before step 0)
-__global__ void k_gj_copy(const double* __restrict__ A, int64_t n, int64_t k,
-                          double* __restrict__ rk, double* __restrict__ ck) {
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+// Blocked in-place Gauss-Jordan inversion (no pivoting: the matrix is
+// symmetric positive definite), GJB pivots per step.  With K the step's
+// block of rows and columns, P = inv(A_KK):
+//   A_KJ <- P A_KJ,  A_IJ <- A_IJ - A_IK P A_KJ,  A_IK <- -A_IK P,  A_KK <- P
+// (I, J outside K), in three launches: the pivot block's inverse, the row
+// panel P A_KJ and a copy of the column panel A_IK into buffers, and the
+// update of every other entry from the buffers (so no entry is read after
+// another thread rewrote it).
+constexpr int GJB = 32;
+
+// A_KK <- inv(A_KK) in shared memory: unblocked Gauss-Jordan, one thread
+// per entry (GJB x GJB threads), b <= GJB rows.
+__global__ void k_gj_pivot_block(double* __restrict__ A, int64_t n, int64_t k0, int b) {
+  __shared__ double P[GJB][GJB + 1];
+  const int i = threadIdx.y, j = threadIdx.x;
+  const bool in = i < b && j < b;
+  P[i][j] = in ? A[(k0 + i) * n + k0 + j] : 0.0;
+  __syncthreads();
+  for (int k = 0; k < b; ++k) {
+    const double inv = 1.0 / P[k][k];
+    const double aik = P[i][k], akj = P[k][j], aij = P[i][j];
+    double v;
+    if (i == k && j == k)
+      v = inv;
+    else if (i == k)
+      v = akj * inv;
+    else if (j == k)
+      v = -aik * inv;
+    else
+      v = aij - aik * akj * inv;
+    __syncthreads();
+    P[i][j] = v;
+    __syncthreads();
+  }
+  if (in) A[(k0 + i) * n + k0 + j] = P[i][j];
+}
+
+// rowbuf[m][j] = (P A_KJ)[m][j] for every column j (used for j outside K);
+// colbuf[i][m] = A[i][k0 + m] for every row i (used for i outside K).
+__global__ void k_gj_panels(const double* __restrict__ A, int64_t n, int64_t k0, int b,
+                            double* __restrict__ rowbuf, double* __restrict__ colbuf) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < b * n;
        t += (int64_t)gridDim.x * blockDim.x) {
-    rk[t] = A[k * n + t];
-    ck[t] = A[t * n + k];
+    const int64_t m = t / n, j = t - m * n;
+    double s = 0.0;
+    for (int q = 0; q < b; ++q) s += A[(k0 + m) * n + k0 + q] * A[(k0 + q) * n + j];
+    rowbuf[m * n + j] = s;
+    const int64_t i = t / b, m2 = t - i * b;
+    colbuf[i * GJB + m2] = A[i * n + k0 + m2];
   }
 }
 
-// One pivot of the in-place Gauss-Jordan inversion (no pivoting: the matrix
-// is symmetric positive definite).  rk, ck: row and column k before this
-// step; each thread rewrites its own entry and copies the entries of row and
-// column k+1 into rn, cn for the next step.
-__global__ void k_gj_step(double* __restrict__ A, int64_t n, int64_t k,
-                          const double* __restrict__ rk, const double* __restrict__ ck,
-                          double* __restrict__ rn, double* __restrict__ cn) {
-  const double inv = 1.0 / rk[k];
+__global__ void k_gj_update(double* __restrict__ A, int64_t n, int64_t k0, int b,
+                            const double* __restrict__ rowbuf, const double* __restrict__ colbuf) {
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n * n;
        t += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = t / n, j = t - i * n;
-    double a;
-    if (i == k && j == k)
-      a = inv;
-    else if (i == k)
-      a = rk[j] * inv;
-    else if (j == k)
-      a = -ck[i] * inv;
-    else
-      a = A[t] - ck[i] * rk[j] * inv;
-    A[t] = a;
-    if (i == k + 1) rn[j] = a;
-    if (j == k + 1) cn[i] = a;
+    const bool iK = i >= k0 && i < k0 + b, jK = j >= k0 && j < k0 + b;
+    if (iK) {
+      if (!jK) A[t] = rowbuf[(i - k0) * n + j];
+    } else if (jK) {
+      double s = 0.0;
+      for (int m = 0; m < b; ++m) s += colbuf[i * GJB + m] * A[(k0 + m) * n + j];
+      A[t] = -s;
+    } else {
+      double s = A[t];
+      for (int m = 0; m < b; ++m) s -= colbuf[i * GJB + m] * rowbuf[m * n + j];
+      A[t] = s;
+    }
   }
 }
 
@@ -449,8 +485,8 @@ void gmg_setup(hx_ctx* c, const double* fac, double shift) {
     }
     L.lmax = al.empty() ? 2.0f : (float)lanczos_max(al, be);
   }
-  // Coarsest level: its dense inverse when small enough (Gauss-Jordan in
-  // FP64, one launch per pivot), else a fixed-count FP32 PCG at every cycle.
+  // Coarsest level: its dense inverse when small enough (blocked
+  // Gauss-Jordan in FP64), else a fixed-count FP32 PCG at every cycle.
   {
     auto& L = G.lv[G.nl - 1];
     const int64_t n = L.g.dofs();
@@ -458,19 +494,20 @@ void gmg_setup(hx_ctx* c, const double* fac, double shift) {
     if (G.direct) {
       const int64_t nn2 = n * n;
       double* A = G.dense.ensure(nn2);
-      double* gj = G.gj.ensure(4 * n);
+      double* gj = G.gj.ensure(2 * GJB * n);  // row panel [GJB][n], column panel [n][GJB]
       HX_CUDA(cudaMemsetAsync(A, 0, nn2 * sizeof(double), s));
       const ElemCoef<double> K = make_elem_coef(L.h[0], L.h[1], L.h[2], c->nu);
       k_dense_assemble<<<gblocks(L.g.elems() * 24), 256, 0, s>>>(L.fac.p, L.g, K, A, n);
       HX_CHECK_LAUNCH();
       k_dense_mask<<<gblocks(nn2), 256, 0, s>>>(A, L.nmask.p, (double)L.shift, n);
       HX_CHECK_LAUNCH();
-      k_gj_copy<<<gblocks(n), 256, 0, s>>>(A, n, 0, gj, gj + n);
-      HX_CHECK_LAUNCH();
-      for (int64_t k = 0; k < n; ++k) {
-        double* cur = gj + (k & 1) * 2 * n;
-        double* nxt = gj + ((k + 1) & 1) * 2 * n;
-        k_gj_step<<<gblocks(nn2), 256, 0, s>>>(A, n, k, cur, cur + n, nxt, nxt + n);
+      for (int64_t k0 = 0; k0 < n; k0 += GJB) {
+        const int b = (int)std::min<int64_t>(GJB, n - k0);
+        k_gj_pivot_block<<<1, dim3(GJB, GJB), 0, s>>>(A, n, k0, b);
+        HX_CHECK_LAUNCH();
+        k_gj_panels<<<gblocks(b * n), 256, 0, s>>>(A, n, k0, b, gj, gj + GJB * n);
+        HX_CHECK_LAUNCH();
+        k_gj_update<<<gblocks(nn2), 256, 0, s>>>(A, n, k0, b, gj, gj + GJB * n);
         HX_CHECK_LAUNCH();
       }
       k_cvt_f64<float><<<gblocks(nn2), 256, 0, s>>>(G.ainv.ensure(nn2), A, nn2);
