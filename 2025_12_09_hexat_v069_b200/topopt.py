@@ -122,7 +122,7 @@ def run_oc_device(ctx: Context, bc_indicator, f, volfrac, radius, n_iter, p=3.0,
         if preconditioner == 1 and adaptive and not use_learned and jac_ms is not None \
                 and it >= retry_at:
             use_learned = True
-        pc = 1 if use_learned else 0
+        pc = 1 if use_learned else (3 if preconditioner == 3 else 0)
         ctx.filter_device(x.data_ptr(), rho.data_ptr(), radius, ref_compat, filter_tol,
                           filter_max_iter)
         ctx.simp_device(rho.data_ptr(), fac.data_ptr(), p, e0, emin)
