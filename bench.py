@@ -160,7 +160,7 @@ def run_ours(args):
     fac_d = torch.from_numpy(fac).to(dev)
     u_d = torch.zeros(n, dtype=torch.float64, device=dev)
     prec, pc = FORMS[args.solver]
-    if pc:
+    if pc == 1:
         learned.load_into(ctx)
     opts = hx.default_opts(tol=1e-6, max_iter=100000, precision=prec, preconditioner=pc)
     lib_stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
@@ -217,7 +217,8 @@ def run_ours(args):
     tensor_roof = None
     if pc:
         roof = fcg_step_roofline(ctx, L, n, ne, peaks)
-        tensor_roof = conv_roofline(ctx, L, args.dims, peaks)
+        if pc == 1:
+            tensor_roof = conv_roofline(ctx, L, args.dims, peaks)
     else:
         dom = max(("pcg_step_fp64", "pcg_update_fp64"), key=lambda k: kern[k]["ms"])
         roof = {"bound": "hbm", "kernel": dom, "achieved": kern[dom]["gbs"],
