@@ -697,7 +697,10 @@ CgState solve_gmg(hx_ctx* c, const double* fac, const double* b, double* x, bool
     one(P1, P0);
     one(P0, P1);
   };
-  const int reps = std::max(1, std::min(8, auto_batch(g, o.check_every) / 2));
+  // a multigrid solve takes tens of iterations and the V-cycle's kernels run
+  // whole even after the state has stopped: two iterations per graph launch
+  // waste at most one cycle
+  const int reps = 1;
   CgState sf = run_batched(c, 0, reps, body, o.wall_limit_ms, t0, timed_out, 0);
   if (sf.status != HX_ST_BREAKDOWN && sf.iter > 0) {
     double* pk = ((sf.iter - 1) % 2 == 0) ? P0 : P1;

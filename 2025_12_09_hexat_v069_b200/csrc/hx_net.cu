@@ -760,7 +760,9 @@ static CgState learned_fcg_mixed(hx_ctx* c, const double* fac, const double* b, 
   st.aux[2] = st.rr;
   st.max_iter = o.max_iter;
   put_state(c, 1, st);
-  const int reps = std::max(1, auto_batch(g, o.check_every) / 2);
+  // the V-cycle's kernels run whole after the state has stopped: batches of
+  // two iterations for multigrid (tens of iterations per solve)
+  const int reps = multigrid ? 1 : std::max(1, auto_batch(g, o.check_every) / 2);
   int parity = 0;  // which P buffer holds p_{k-1}: P1 when parity == 0
   double best = so_h.rel_res;
   int best_it = 0;
