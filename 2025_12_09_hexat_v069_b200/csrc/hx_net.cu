@@ -745,7 +745,9 @@ static CgState learned_fcg_mixed(hx_ctx* c, const double* fac, const double* b, 
   if (so_h.status != HX_RUNNING || o.max_iter <= 0) return so_h;
   // FP32 iteration state: rz, rr of the replaced residual; no previous
   // direction (p_old = q_old = 0, pq = 0 gives beta = 0, alpha = 0)
-  const double delta = (o.inner_tol > 0 && o.inner_tol < 1) ? o.inner_tol : 0.1;
+  // multigrid drops the residual ~5x per iteration: replace after inner_tol^3
+  const double d1 = (o.inner_tol > 0 && o.inner_tol < 1) ? o.inner_tol : 0.1;
+  const double delta = multigrid ? d1 * d1 * d1 : d1;
   put_state(c, 1, fresh_state(o.tol, o.max_iter, 1, false, false));
   launch_fill_zero(c->stream, d32, n * sizeof(float));
   launch_fill_zero(c->stream, P1, n * sizeof(float));

@@ -80,7 +80,8 @@ typedef struct hx_solve_opts {
   int32_t keep_best;       /* 1: keep the best iterate (reference semantics) */
   double inner_tol;        /* mixed precision: the FP32 recursive residual is
                               replaced by the FP64 true residual each time it
-                              has dropped by this factor (default 0.1) */
+                              has dropped by this factor (default 0.1); with
+                              HX_PC_MULTIGRID by its cube */
   int32_t max_refine;      /* reserved */
   int32_t ref_retry;       /* 1: reference retry/shift-escalation semantics */
   int32_t divergence_checks; /* 1: explosion and 100x-over-best checks */
