@@ -29,7 +29,7 @@ class SolveOpts(C.Structure):
         ("inner_tol", C.c_double), ("max_refine", C.c_int32), ("ref_retry", C.c_int32),
         ("divergence_checks", C.c_int32), ("verify_true_residual", C.c_int32),
         ("learned_no_fallback", C.c_int32), ("multigrid_fallback", C.c_int32),
-        ("reserved", C.c_int32 * 4),
+        ("mg_smooth_degree", C.c_int32), ("reserved", C.c_int32 * 3),
     ]
 
 

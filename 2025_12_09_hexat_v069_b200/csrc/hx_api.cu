@@ -272,6 +272,8 @@ hx_solve_opts sanitize(const hx_solve_opts* o) {
   HX_REQUIRE(r.shift_factor >= 0 && std::isfinite(r.shift_factor), "shift_factor must be >= 0");
   HX_REQUIRE(r.precision >= HX_PREC_FP64 && r.precision <= HX_PREC_MIXED32,
              "unsupported precision");
+  HX_REQUIRE(r.mg_smooth_degree >= 0 && r.mg_smooth_degree <= 8,
+             "mg_smooth_degree must be 0 (default) .. 8");
   return r;
 }
 

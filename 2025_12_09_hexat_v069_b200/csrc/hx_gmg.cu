@@ -18,7 +18,8 @@
 // Levels are added until one has at most GMG_STOP_DOFS DOFs (or an element
 // count turns odd).
 //
-// V-cycle (FP32): on each level Chebyshev smoothing of degree GMG_DEGREE
+// V-cycle (FP32): on each level Chebyshev smoothing of degree G.degree
+// (hx_solve_opts.mg_smooth_degree, default GMG_DEFAULT_DEGREE)
 // with Jacobi scaling on [0.05, 1.1] x lambda_max(D^-1 A) (a Lanczos
 // estimate from Jacobi-PCG steps at set-up), from zero before the restriction and from the
 // prolonged correction after it.  The coarsest level, when it has at most
@@ -41,7 +42,6 @@ namespace hx {
 
 namespace {
 
-constexpr int GMG_DEGREE = 2;          // Chebyshev degree per smoothing
 constexpr int GMG_COARSE_ITERS = 64;   // PCG iterations on a large coarsest level
 constexpr int64_t GMG_STOP_DOFS = 1536;    // coarsen until a level has at most this many DOFs
 constexpr int64_t GMG_DIRECT_DOFS = 2048;  // coarsest levels up to this size are solved directly
@@ -528,7 +528,7 @@ void gmg_setup(hx_ctx* c, const double* fac, double shift) {
                                                           t_start).count();
 }
 
-// Chebyshev smoothing of A x = b on level L (GMG_DEGREE steps): from x = 0
+// Chebyshev smoothing of A x = b on level L (c->gmg.degree steps): from x = 0
 // when xzero, else from x; leaves r = b - A x when want_residual.
 static void cheb_smooth(hx_ctx* c, hx_ctx::GmgLevel& L, bool xzero, bool want_residual) {
   cudaStream_t s = c->stream;
@@ -547,7 +547,7 @@ static void cheb_smooth(hx_ctx* c, hx_ctx::GmgLevel& L, bool xzero, bool want_re
                                   xzero ? 1 : 0, 1.0f / theta, n);
   HX_CHECK_LAUNCH();
   float rho = 1.0f / sigma;
-  for (int k = 1; k < GMG_DEGREE; ++k) {
+  for (int k = 1; k < c->gmg.degree; ++k) {
     A(L.d.p, L.q.p);
     const float rho_n = 1.0f / (2.0f * sigma - rho);
     k_cheb_step<<<nb, 256, 0, s>>>(L.q.p, L.minv.p, L.r.p, L.d.p, L.x.p, rho_n * rho,
@@ -653,6 +653,7 @@ CgState solve_gmg(hx_ctx* c, const double* fac, const double* b, double* x, bool
                   int* iters_out) {
   const Grid& g = c->g;
   const int64_t n = g.dofs();
+  c->gmg.degree = o.mg_smooth_degree > 0 ? o.mg_smooth_degree : GMG_DEFAULT_DEGREE;
   gmg_setup(c, fac, shift);
   double* r = c->d_r.ensure(n);
   double* P0 = c->d_p.ensure(n);

@@ -235,6 +235,7 @@ struct hx_ctx {
     hx::DevBuf<float> ainv;
     hx::DevBuf<double> lanczos;  // (alpha, beta, status) per step of the lambda_max estimate
     double setup_ms = 0;         // set-up time accumulated over the current solve
+    int degree = 2;              // Chebyshev degree per smoothing
   } gmg;
 
   // lattice origin of the mesh (the minimum node coordinates; 0 for hx_set_grid)

@@ -694,10 +694,12 @@ static CgState learned_fcg_mixed(hx_ctx* c, const double* fac, const double* b, 
   auto& N = c->net;
   const Grid& g = c->g;
   const int64_t n = g.dofs(), ne = g.elems();
-  if (multigrid)
+  if (multigrid) {
+    c->gmg.degree = o.mg_smooth_degree > 0 ? o.mg_smooth_degree : GMG_DEFAULT_DEGREE;
     gmg_setup(c, fac, shift);
-  else
+  } else {
     net_operator_inputs(c, fac);
+  }
   float* fac32 = c->d_fac32.ensure(ne);
   float* minv32 = c->d_minv32.ensure(n);
   float* r32 = c->d_r32.ensure(n);

@@ -80,6 +80,8 @@ hx_status export_webdata(hx_ctx* c, const char* path, const T* dens, const T* l1
 // geometric multigrid (hx_gmg.cu): hierarchy for `fac` (after the Jacobi
 // set-up of the solve), one V-cycle z = V(r), the flexible-CG coefficients
 // of a preconditioned residual, and the FP64 FCG solve it preconditions
+// default Chebyshev degree of the multigrid smoothing
+constexpr int GMG_DEFAULT_DEGREE = 2;
 void gmg_setup(hx_ctx* c, const double* fac, double shift);
 template <typename T>
 void gmg_vcycle(hx_ctx* c, const T* r, T* z);

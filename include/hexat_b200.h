@@ -91,7 +91,9 @@ typedef struct hx_solve_opts {
                                   Jacobi attempt switch to HX_PC_MULTIGRID, as the
                                   reference's "jacobi_amg" switches to AMG
                                   (GPUSolver.jl:540-579) */
-  int32_t reserved[4];
+  int32_t mg_smooth_degree;    /* multigrid: Chebyshev degree of each pre- and
+                                  post-smoothing, 1..8 (0: the default, 2) */
+  int32_t reserved[3];
 } hx_solve_opts;
 
 typedef struct hx_solve_report {
