@@ -509,7 +509,8 @@ def run_c4_loop(args):
                            "solve_s_total": float(np.sum(res.solve_ms)) / 1e3,
                            "finetune_s_total": float(np.sum(getattr(res, "finetune_ms", []))) / 1e3,
                            "pnorm_vm_P8": pn, "max_vm": vmax, "final_change": res.change[-1],
-                           "learned_solves": int(np.sum(getattr(res, "pc_used", [0])))}
+                           "learned_solves": int(np.sum(np.asarray(getattr(res, "pc_used", [0]))
+                                                        == 1))}
         if kw["preconditioner"]:
             # per 20-iteration window: solves run with the networks, and how
             # many of those fell back or were finished by Jacobi-PCG
@@ -518,7 +519,7 @@ def run_c4_loop(args):
             its = np.asarray(res.iterations)
             out_forms[name]["windows"] = [
                 {"iters": f"{w}-{min(w + 20, len(pcu)) - 1}",
-                 "learned": int(pcu[w:w + 20].sum()),
+                 "learned": int((pcu[w:w + 20] == 1).sum()),
                  "fallbacks": int(fb[w:w + 20].sum()),
                  "mean_solve_iterations": float(its[w:w + 20].mean())}
                 for w in range(0, len(pcu), 20)]
