@@ -46,7 +46,7 @@ constexpr int GMG_COARSE_ITERS = 64;   // PCG iterations on a large coarsest lev
 constexpr int64_t GMG_STOP_DOFS = 1536;    // coarsen until a level has at most this many DOFs
 constexpr int64_t GMG_DIRECT_DOFS = 2048;  // coarsest levels up to this size are solved directly
 constexpr float GMG_LO = 0.05f, GMG_HI = 1.1f;  // Chebyshev range / lambda_max
-constexpr int GMG_LANCZOS = 20;                  // PCG steps of the lambda_max estimate
+constexpr int GMG_LANCZOS = 12;                  // PCG steps of the lambda_max estimate
 
 __device__ __forceinline__ int64_t gt() { return blockIdx.x * (int64_t)blockDim.x + threadIdx.x; }
 __device__ __forceinline__ int64_t gs() { return (int64_t)gridDim.x * blockDim.x; }
@@ -87,37 +87,10 @@ __global__ void k_mask3(float* __restrict__ v, const uint8_t* __restrict__ nmask
     if (!((nmask[i / 3] >> (i % 3)) & 1u)) v[i] = 0.f;
 }
 
-// Chebyshev start: r = b - q (q may be null: x = 0), d = minv r / theta,
-// x = (x0 or 0) + d
-__global__ void k_cheb_start(const float* __restrict__ b, const float* __restrict__ q,
-                             const float* __restrict__ minv, float* __restrict__ r,
-                             float* __restrict__ d, float* __restrict__ x, int xzero,
-                             float inv_theta, int64_t n) {
-  for (int64_t i = gt(); i < n; i += gs()) {
-    const float ri = q ? b[i] - q[i] : b[i];
-    const float di = minv[i] * ri * inv_theta;
-    r[i] = ri;
-    d[i] = di;
-    x[i] = xzero ? di : x[i] + di;
-  }
-}
-
-// Chebyshev step: r -= q (q = A d), d = a d + c minv r, x += d
-__global__ void k_cheb_step(const float* __restrict__ q, const float* __restrict__ minv,
-                            float* __restrict__ r, float* __restrict__ d, float* __restrict__ x,
-                            float a, float cc, int64_t n) {
-  for (int64_t i = gt(); i < n; i += gs()) {
-    const float ri = r[i] - q[i];
-    const float di = a * d[i] + cc * minv[i] * ri;
-    r[i] = ri;
-    d[i] = di;
-    x[i] += di;
-  }
-}
-
-// r -= q
-__global__ void k_sub(float* __restrict__ r, const float* __restrict__ q, int64_t n) {
-  for (int64_t i = gt(); i < n; i += gs()) r[i] -= q[i];
+// first Chebyshev step from x = 0: x = (1/theta) M^-1 b
+__global__ void k_cheb_first(const float* __restrict__ b, const float* __restrict__ minv,
+                             float* __restrict__ x, float inv_theta, int64_t n) {
+  for (int64_t i = gt(); i < n; i += gs()) x[i] = inv_theta * minv[i] * b[i];
 }
 
 template <typename TD, typename TS>
@@ -528,38 +501,55 @@ void gmg_setup(hx_ctx* c, const double* fac, double shift) {
                                                           t_start).count();
 }
 
-// Chebyshev smoothing of A x = b on level L (c->gmg.degree steps): from x = 0
-// when xzero, else from x; leaves r = b - A x when want_residual.
+// Chebyshev smoothing of A x = b on level L (c->gmg.degree steps, Jacobi
+// scaling on [GMG_LO, GMG_HI] lambda_max): from x = 0 when xzero, else from
+// x; leaves r = b - A x in L.r when want_residual.  Three-term form:
+//   x_1 = x_0 + (1/theta) M^-1 (b - A x_0),
+//   x_{k+1} = x_k + rho_k rho_{k-1} (x_k - x_{k-1}) + (2 rho_k / delta) M^-1 (b - A x_k),
+// rho_0 = 1/sigma, rho_k = 1/(2 sigma - rho_{k-1}): each step is one operator
+// launch whose epilogue forms x_{k+1} (MODE 5 of the structured kernel).
+// x_k and x_{k-1} alternate between L.x and L.d; the start is chosen so
+// that the result lands in L.x.
 static void cheb_smooth(hx_ctx* c, hx_ctx::GmgLevel& L, bool xzero, bool want_residual) {
   cudaStream_t s = c->stream;
   const int64_t n = L.g.dofs();
-  const unsigned nb = gblocks(n);
+  const int m = c->gmg.degree;
   const float lmax = L.lmax;
   const float lo = GMG_LO * lmax, hi = GMG_HI * lmax;
   const float theta = 0.5f * (hi + lo), delta = 0.5f * (hi - lo);
   const float sigma = theta / delta;
-  auto A = [&](const float* v, float* out) {
-    launch_matvec<float>(s, 0, v, out, L.fac.p, L.nmask.p, L.g, L.K, L.shift, c->d_state.p + 3,
-                         c->d_partials.p, nullptr);
-  };
-  if (!xzero) A(L.x.p, L.q.p);
-  k_cheb_start<<<nb, 256, 0, s>>>(L.b.p, xzero ? nullptr : L.q.p, L.minv.p, L.r.p, L.d.p, L.x.p,
-                                  xzero ? 1 : 0, 1.0f / theta, n);
-  HX_CHECK_LAUNCH();
+  float* buf[2] = {L.x.p, L.d.p};
+  int cur;  // buffer holding x_k
+  int k;    // steps done
+  if (xzero) {
+    cur = (m % 2 == 1) ? 0 : 1;  // x_1 .. x_m alternate, x_m in L.x
+    k_cheb_first<<<gblocks(n), 256, 0, s>>>(L.b.p, L.minv.p, buf[cur], 1.0f / theta, n);
+    HX_CHECK_LAUNCH();
+    k = 1;
+  } else {
+    cur = 0;
+    if (m % 2 == 1) {  // an odd count of steps from L.x would end in L.d
+      HX_CUDA(cudaMemcpyAsync(L.d.p, L.x.p, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+      cur = 1;
+    }
+    k = 0;
+  }
   float rho = 1.0f / sigma;
-  for (int k = 1; k < c->gmg.degree; ++k) {
-    A(L.d.p, L.q.p);
-    const float rho_n = 1.0f / (2.0f * sigma - rho);
-    k_cheb_step<<<nb, 256, 0, s>>>(L.q.p, L.minv.p, L.r.p, L.d.p, L.x.p, rho_n * rho,
-                                   2.0f * rho_n / delta, n);
-    HX_CHECK_LAUNCH();
-    rho = rho_n;
+  for (; k < m; ++k) {
+    float omega = 0.f, gamma = 1.0f / theta;
+    if (k > 0) {
+      const float rho_n = 1.0f / (2.0f * sigma - rho);
+      omega = rho_n * rho;
+      gamma = 2.0f * rho_n / delta;
+      rho = rho_n;
+    }
+    // after a start from x = 0, x_prev = x_0 = 0
+    launch_cheb_step<float>(s, buf[cur], buf[cur ^ 1], xzero && k == 1, L.b.p, L.minv.p, omega,
+                            gamma, L.fac.p, L.nmask.p, L.g, L.K, L.shift);
+    cur ^= 1;
   }
-  if (want_residual) {
-    A(L.d.p, L.q.p);  // r tracks b - A x: subtract A of the last increment
-    k_sub<<<nb, 256, 0, s>>>(L.r.p, L.q.p, n);
-    HX_CHECK_LAUNCH();
-  }
+  if (want_residual)
+    launch_residual<float>(s, L.x.p, L.b.p, L.r.p, L.fac.p, L.nmask.p, L.g, L.K, L.shift);
 }
 
 // z = V(r): one V-cycle on r (FP64 or FP32 DOF vector of level 0).

@@ -71,6 +71,17 @@ template <typename T>
 void launch_fcg_step(cudaStream_t s, const T* pin, T* pout, const T* z, T* x, T* q, const T* fac,
                      const uint8_t* nmask, const Grid& g, const ElemCoef<T>& K, T shift,
                      CgState* st, double* partials);
+// Multigrid smoothing (FP32): one Chebyshev step as a three-term recurrence,
+// xprev_new <- x + omega (x - xprev_new) + gamma M^-1 (b - (K + sI) x) on the
+// free DOFs (0 on the fixed ones; xprev_zero: x_prev = 0, not read); and the
+// residual r = mask(b - (K + sI) x).
+template <typename T>
+void launch_cheb_step(cudaStream_t s, const T* x, T* xprev_new, bool xprev_zero, const T* b,
+                      const T* minv, T omega, T gamma, const T* fac, const uint8_t* nmask,
+                      const Grid& g, const ElemCoef<T>& K, T shift);
+template <typename T>
+void launch_residual(cudaStream_t s, const T* x, const T* b, T* r, const T* fac,
+                     const uint8_t* nmask, const Grid& g, const ElemCoef<T>& K, T shift);
 template <typename T>
 void launch_node_diag(cudaStream_t s, const T* fac, const uint8_t* bcfree, uint8_t* nmask, T* diag,
                       const Grid& g, const ElemCoef<double>& K, double* partials, CgState* st,

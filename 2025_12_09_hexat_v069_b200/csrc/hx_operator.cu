@@ -104,9 +104,10 @@ struct OpSmem {
 template <typename T>
 struct OpArgs {
   const T* pin;   // vector to multiply (MODE 0-2) or p_old (FUSED)
-  const T* r;     // MODE 3: residual
-  const T* minv;  // MODE 3: Jacobi inverse diagonal; MODE 4: preconditioned z
-  T* x;           // FUSED: solution (x += alpha_old p_old on owned nodes)
+  const T* r;     // MODE 3: residual; MODE 5, 6: right-hand side b
+  const T* minv;  // MODE 3, 5: Jacobi inverse diagonal; MODE 4: preconditioned z
+  T* x;           // FUSED: solution (x += alpha_old p_old on owned nodes); MODE 5:
+                  // x_prev in, x_new out
   T* pout;        // FUSED: new direction p
   T* q;           // output K p (masked, shifted)
   const T* fac;
@@ -115,6 +116,8 @@ struct OpArgs {
   int kchunk;
   ElemCoef<T> K;
   T shift;
+  T omega, gamma;  // MODE 5: recurrence coefficients
+  int xprev_zero;  // MODE 5: x_prev = 0 (not read)
   CgState* st;
   double* partials;
   double* out;
@@ -153,6 +156,12 @@ __device__ __forceinline__ void lambda_row(const ElemCoef<T>& K, const T (&U)[3]
 }
 
 // MODE 0: q = mask(K x + s x);  MODE 1: also out[0] = x.q;
+// MODE 5: Chebyshev step of the multigrid smoother as a three-term
+//         recurrence on x: x_new = x + omega (x - x_prev) + gamma M^-1 (b - A x)
+//         with A x = mask(K x + s x); x_prev (A.x) is overwritten by x_new
+//         (each node's x_prev is read and written by its owner only; the
+//         staged x, read by the neighbours, is not written).
+// MODE 6: residual r = mask(b - K x - s x) into A.q;
 // MODE 2: CG matvec, st->pq = p.q, st->alpha = rz / pq, breakdown test;
 // MODE 3: fused PCG step (see file header), then as MODE 2;
 // MODE 4: flexible-CG step: p = z + beta p_old (z from a variable
@@ -162,7 +171,8 @@ __device__ __forceinline__ void lambda_row(const ElemCoef<T>& K, const T (&U)[3]
 //         vanish, so r is not staged.
 template <typename T, int BY, int MODE, int MINB>
 __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
-  constexpr bool FUSED = MODE >= 3;
+  constexpr bool FUSED = MODE == 3 || MODE == 4;
+  constexpr bool DOT = MODE >= 1 && MODE <= 4;  // reduces p.q / x.q
   constexpr int NT = MV_BX * BY;
   constexpr int V = Stage<T>::V;
   constexpr int CPR = Stage<T>::CPR;
@@ -173,7 +183,7 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
   constexpr int NP = OpSmem<T, BY, FUSED>::NP;
   constexpr int NR = OpSmem<T, BY, FUSED>::NR;
   using VecT = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
-  if (MODE >= 2 && A.st->status != HX_RUNNING) return;
+  if (MODE >= 2 && MODE <= 4 && A.st->status != HX_RUNNING) return;
   extern __shared__ __align__(16) unsigned char smraw[];
   OpSmem<T, BY, FUSED>& sm = *reinterpret_cast<OpSmem<T, BY, FUSED>*>(smraw);
   const Grid g = A.g;
@@ -454,11 +464,23 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
       for (int c = 0; c < 3; ++c) {
         T v = rowS[c] + sm.red[ly - 1][c][lx];
         const T xv = own[c];
-        v = ((m >> c) & 1u) ? v + A.shift * xv : T(0);
-        A.q[3 * node + c] = v;
-        if (MODE != 0) pdot = fma(xv, v, pdot);
+        const bool fr = (m >> c) & 1u;
+        v = fr ? v + A.shift * xv : T(0);
+        const int64_t dof = 3 * node + c;
+        if (MODE == 5) {
+          // x_prev: read, or 0 (the step after a start from x = 0), or
+          // unused (the first step: omega = 0)
+          const T xp = A.xprev_zero ? T(0) : (A.omega != T(0) ? A.x[dof] : xv);
+          A.x[dof] = fr ? xv + A.omega * (xv - xp) + A.gamma * A.minv[dof] * (A.r[dof] - v)
+                        : T(0);
+        } else if (MODE == 6) {
+          A.q[dof] = fr ? A.r[dof] - v : T(0);
+        } else {
+          A.q[dof] = v;
+        }
+        if (DOT) pdot = fma(xv, v, pdot);
       }
-      if (MODE != 0) dsum += (double)pdot;
+      if (DOT) dsum += (double)pdot;
     }
     c0 = step(c0, NP);
     c1 = step(c1, NP);
@@ -482,7 +504,7 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
       else
         A.st->alpha = zr / pq;
     }
-  } else if (MODE != 0) {
+  } else if (DOT) {
     double v[1] = {dsum};
     if (grid_reduce<1>(v, A.partials, &A.st->ticket[TK_MATVEC]) && tid == 0) {
       if (MODE == 1) {
@@ -557,7 +579,7 @@ inline dim3 mv_grid(const Grid& g, int kchunk) {
 
 template <typename T, int MODE>
 void launch_struct(cudaStream_t s, const OpArgs<T>& a) {
-  constexpr bool FUSED = MODE >= 3;
+  constexpr bool FUSED = MODE == 3 || MODE == 4;
   constexpr int MINB = 2;
   const size_t smem = sizeof(OpSmem<T, MV_BY, FUSED>);
   static PerDeviceOnce configured;  // per instantiation and device
@@ -619,6 +641,49 @@ void launch_matvec(cudaStream_t s, int mode, const T* x, T* y, const T* fac, con
   else
     launch_struct<T, 2>(s, a);
 }
+
+template <typename T>
+void launch_cheb_step(cudaStream_t s, const T* x, T* xprev_new, bool xprev_zero, const T* b,
+                      const T* minv, T omega, T gamma, const T* fac, const uint8_t* nmask,
+                      const Grid& g, const ElemCoef<T>& K, T shift) {
+  OpArgs<T> a{};
+  a.pin = x;
+  a.x = xprev_new;
+  a.xprev_zero = xprev_zero ? 1 : 0;
+  a.r = b;
+  a.minv = minv;
+  a.omega = omega;
+  a.gamma = gamma;
+  a.fac = fac;
+  a.nmask = nmask;
+  a.g = g;
+  a.kchunk = mv_kchunk(g);
+  a.K = K;
+  a.shift = shift;
+  launch_struct<T, 5>(s, a);
+}
+template void launch_cheb_step<float>(cudaStream_t, const float*, float*, bool, const float*,
+                                      const float*, float, float, const float*, const uint8_t*,
+                                      const Grid&, const ElemCoef<float>&, float);
+
+template <typename T>
+void launch_residual(cudaStream_t s, const T* x, const T* b, T* r, const T* fac,
+                     const uint8_t* nmask, const Grid& g, const ElemCoef<T>& K, T shift) {
+  OpArgs<T> a{};
+  a.pin = x;
+  a.r = b;
+  a.q = r;
+  a.fac = fac;
+  a.nmask = nmask;
+  a.g = g;
+  a.kchunk = mv_kchunk(g);
+  a.K = K;
+  a.shift = shift;
+  launch_struct<T, 6>(s, a);
+}
+template void launch_residual<float>(cudaStream_t, const float*, const float*, float*,
+                                     const float*, const uint8_t*, const Grid&,
+                                     const ElemCoef<float>&, float);
 
 template <typename T>
 void launch_pcg_step(cudaStream_t s, const T* pin, T* pout, const T* r, const T* minv, T* x, T* q,
