@@ -150,3 +150,23 @@ def test_multigrid_on_a_shifted_singular_system(ctx, hx, precision):
     assert rm.status == 0 and rm.true_rel_res < 1e-8 and rm.fallback_used == 0, rm.as_dict()
     assert rm.iterations < 60, rm.as_dict()
     assert np.abs(um - uj).max() <= 1e-5 * np.abs(uj).max()
+
+
+def test_smoothing_degree_option(ctx, hx):
+    """mg_smooth_degree selects the Chebyshev degree (odd degrees end the
+    buffer alternation on the other buffer, which the smoother corrects):
+    every degree 1..4 converges to the same solution; out-of-range values are
+    rejected before any work."""
+    dims = (48, 16, 16)
+    nodes, el, bc, f, fac = _problem(ctx, hx, dims)
+    us = []
+    for deg in (1, 2, 3, 4):
+        u, rep = ctx.solve(f, fac, tol=1e-9, max_iter=500, preconditioner=3,
+                           mg_smooth_degree=deg)
+        assert rep.status == 0 and rep.true_rel_res < 1e-9, (deg, rep.as_dict())
+        us.append(u)
+    for u in us[1:]:
+        assert np.abs(u - us[0]).max() <= 1e-6 * np.abs(us[0]).max()
+    with pytest.raises(hx.HexatError) as err:
+        ctx.solve(f, fac, tol=1e-9, preconditioner=3, mg_smooth_degree=9)
+    assert err.value.status == 6  # HX_BAD_ARG
