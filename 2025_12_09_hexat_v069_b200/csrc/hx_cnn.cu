@@ -210,7 +210,7 @@ __device__ __forceinline__ void prolong_axis(int f, int nc, int (&i)[2], float (
 // sum of the weights inside the grid (a weighted average; for features).
 template <int CH>
 __global__ void k_restrict(const float* __restrict__ in, float* __restrict__ out, GridN gf,
-                           GridN gc, int normalise) {
+                           GridN gc, int normalise, const uint8_t* __restrict__ cmask) {
   const int64_t nc = (int64_t)gc.nx * gc.ny * gc.nz;
   for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nc;
        n += (int64_t)gridDim.x * blockDim.x) {
@@ -247,8 +247,10 @@ __global__ void k_restrict(const float* __restrict__ in, float* __restrict__ out
       }
     }
     const float sc = (normalise && wsum > 0.f) ? 1.f / wsum : 1.f;
+    // cmask (3 channels): bit c clear -> component c is a fixed DOF, set to 0
+    const unsigned m = cmask ? cmask[n] : 0xffu;
 #pragma unroll
-    for (int c = 0; c < CH; ++c) out[n * CH + c] = acc[c] * sc;
+    for (int c = 0; c < CH; ++c) out[n * CH + c] = ((m >> c) & 1u) ? acc[c] * sc : 0.f;
   }
 }
 
@@ -532,7 +534,7 @@ static size_t restrict_ys_smem(int cxw) {
 // Prolongation, the exact transpose of k_restrict (without normalisation):
 // fine[j][c] = (accumulate ? fine[j][c] : 0) + sum_{i: |j - 2i| <= 1} w(j - 2i) coarse[i][c].
 __global__ void k_prolong(const float* __restrict__ coarse, float* __restrict__ fine, GridN gf,
-                          GridN gc, int accumulate) {
+                          GridN gc, int accumulate, const uint8_t* __restrict__ fmask) {
   const int64_t nf = (int64_t)gf.nx * gf.ny * gf.nz;
   for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nf;
        n += (int64_t)gridDim.x * blockDim.x) {
@@ -563,9 +565,11 @@ __global__ void k_prolong(const float* __restrict__ coarse, float* __restrict__ 
       a1 += fine[3 * n + 1];
       a2 += fine[3 * n + 2];
     }
-    fine[3 * n + 0] = a0;
-    fine[3 * n + 1] = a1;
-    fine[3 * n + 2] = a2;
+    // fmask: bit c clear -> component c is a fixed DOF, set to 0
+    const unsigned m = fmask ? fmask[n] : 7u;
+    fine[3 * n + 0] = (m & 1u) ? a0 : 0.f;
+    fine[3 * n + 1] = (m & 2u) ? a1 : 0.f;
+    fine[3 * n + 2] = (m & 4u) ? a2 : 0.f;
   }
 }
 
@@ -797,21 +801,22 @@ void launch_restrict_ys(cudaStream_t s, const __nv_bfloat16* ys, const CgState* 
 }
 
 void launch_restrict(cudaStream_t s, int ch, const float* in, float* out, const GridN& gf,
-                     const GridN& gc, bool normalise) {
+                     const GridN& gc, bool normalise, const uint8_t* cmask) {
   const int64_t nc = (int64_t)gc.nx * gc.ny * gc.nz;
+  HX_REQUIRE(ch == 3 || !cmask, "a DOF mask needs 3 channels");
   if (ch == 3)
-    k_restrict<3><<<vec_blocks(nc), 256, 0, s>>>(in, out, gf, gc, normalise ? 1 : 0);
+    k_restrict<3><<<vec_blocks(nc), 256, 0, s>>>(in, out, gf, gc, normalise ? 1 : 0, cmask);
   else if (ch == 1)
-    k_restrict<1><<<vec_blocks(nc), 256, 0, s>>>(in, out, gf, gc, normalise ? 1 : 0);
+    k_restrict<1><<<vec_blocks(nc), 256, 0, s>>>(in, out, gf, gc, normalise ? 1 : 0, nullptr);
   else
     throw Error{HX_BAD_ARG, "unsupported channel count"};
   HX_CHECK_LAUNCH();
 }
 
 void launch_prolong(cudaStream_t s, const float* coarse, float* fine, const GridN& gf,
-                    const GridN& gc, bool accumulate) {
+                    const GridN& gc, bool accumulate, const uint8_t* fmask) {
   const int64_t nf = (int64_t)gf.nx * gf.ny * gf.nz;
-  k_prolong<<<vec_blocks(nf), 256, 0, s>>>(coarse, fine, gf, gc, accumulate ? 1 : 0);
+  k_prolong<<<vec_blocks(nf), 256, 0, s>>>(coarse, fine, gf, gc, accumulate ? 1 : 0, fmask);
   HX_CHECK_LAUNCH();
 }
 

@@ -42,11 +42,13 @@ void launch_restrict_dof(cudaStream_t s, const T* v, const T* minv, const CgStat
 // the same field (mode 0) from ys = BF16(D^-1/2 v), n + 8 entries
 void launch_restrict_ys(cudaStream_t s, const __nv_bfloat16* ys, const CgState* sst,
                         double scale_mul, float* out, const GridN& gf, const GridN& gc);
-// full-weighting restriction fine -> coarse node grid (ch 3 or 1), and its transpose
+// full-weighting restriction fine -> coarse node grid (ch 3 or 1), and its
+// transpose; an optional node mask (3 channels: free-DOF bits) zeroes the
+// fixed components of the output
 void launch_restrict(cudaStream_t s, int ch, const float* in, float* out, const GridN& gf,
-                     const GridN& gc, bool normalise);
+                     const GridN& gc, bool normalise, const uint8_t* cmask = nullptr);
 void launch_prolong(cudaStream_t s, const float* coarse, float* fine, const GridN& gf,
-                    const GridN& gc, bool accumulate);
+                    const GridN& gc, bool accumulate, const uint8_t* fmask = nullptr);
 // lifting E: [node][3] FP32 -> [node][16] BF16 (x, feat * x), and its transpose
 void launch_lift(cudaStream_t s, const float* x, const float* feat, __nv_bfloat16* X, int64_t nn);
 void launch_unlift(cudaStream_t s, const __nv_bfloat16* Y, const float* feat, float* acc,

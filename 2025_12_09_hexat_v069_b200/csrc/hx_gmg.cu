@@ -33,6 +33,7 @@
 #include <chrono>
 #include <cmath>
 #include <limits>
+#include <type_traits>
 #include <vector>
 
 #include "hx_cnn.h"
@@ -79,12 +80,6 @@ __global__ void k_coarse_bc(const uint8_t* __restrict__ bf, uint8_t* __restrict_
     const int j = (int)(t % gc.nyn), k = (int)(t / gc.nyn);
     bc[n] = bf[((int64_t)(2 * k) * gf.nyn + 2 * j) * gf.nxn + 2 * i];
   }
-}
-
-// v[3n + c] = 0 where bit c of nmask[n] is clear (fixed DOF)
-__global__ void k_mask3(float* __restrict__ v, const uint8_t* __restrict__ nmask, int64_t nn) {
-  for (int64_t i = gt(); i < 3 * nn; i += gs())
-    if (!((nmask[i / 3] >> (i % 3)) & 1u)) v[i] = 0.f;
 }
 
 // first Chebyshev step from x = 0: x = (1/theta) M^-1 b
@@ -508,9 +503,10 @@ void gmg_setup(hx_ctx* c, const double* fac, double shift) {
 //   x_{k+1} = x_k + rho_k rho_{k-1} (x_k - x_{k-1}) + (2 rho_k / delta) M^-1 (b - A x_k),
 // rho_0 = 1/sigma, rho_k = 1/(2 sigma - rho_{k-1}): each step is one operator
 // launch whose epilogue forms x_{k+1} (MODE 5 of the structured kernel).
-// x_k and x_{k-1} alternate between L.x and L.d; the start is chosen so
-// that the result lands in L.x.
-static void cheb_smooth(hx_ctx* c, hx_ctx::GmgLevel& L, bool xzero, bool want_residual) {
+// x_k and x_{k-1} alternate between x and L.d; the start is chosen so
+// that the result lands in x.
+static void cheb_smooth(hx_ctx* c, hx_ctx::GmgLevel& L, const float* b, float* x, bool xzero,
+                        bool want_residual) {
   cudaStream_t s = c->stream;
   const int64_t n = L.g.dofs();
   const int m = c->gmg.degree;
@@ -518,18 +514,18 @@ static void cheb_smooth(hx_ctx* c, hx_ctx::GmgLevel& L, bool xzero, bool want_re
   const float lo = GMG_LO * lmax, hi = GMG_HI * lmax;
   const float theta = 0.5f * (hi + lo), delta = 0.5f * (hi - lo);
   const float sigma = theta / delta;
-  float* buf[2] = {L.x.p, L.d.p};
+  float* buf[2] = {x, L.d.p};
   int cur;  // buffer holding x_k
   int k;    // steps done
   if (xzero) {
     cur = (m % 2 == 1) ? 0 : 1;  // x_1 .. x_m alternate, x_m in L.x
-    k_cheb_first<<<gblocks(n), 256, 0, s>>>(L.b.p, L.minv.p, buf[cur], 1.0f / theta, n);
+    k_cheb_first<<<gblocks(n), 256, 0, s>>>(b, L.minv.p, buf[cur], 1.0f / theta, n);
     HX_CHECK_LAUNCH();
     k = 1;
   } else {
     cur = 0;
     if (m % 2 == 1) {  // an odd count of steps from L.x would end in L.d
-      HX_CUDA(cudaMemcpyAsync(L.d.p, L.x.p, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+      HX_CUDA(cudaMemcpyAsync(L.d.p, x, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
       cur = 1;
     }
     k = 0;
@@ -544,12 +540,12 @@ static void cheb_smooth(hx_ctx* c, hx_ctx::GmgLevel& L, bool xzero, bool want_re
       rho = rho_n;
     }
     // after a start from x = 0, x_prev = x_0 = 0
-    launch_cheb_step<float>(s, buf[cur], buf[cur ^ 1], xzero && k == 1, L.b.p, L.minv.p, omega,
+    launch_cheb_step<float>(s, buf[cur], buf[cur ^ 1], xzero && k == 1, b, L.minv.p, omega,
                             gamma, L.fac.p, L.nmask.p, L.g, L.K, L.shift);
     cur ^= 1;
   }
   if (want_residual)
-    launch_residual<float>(s, L.x.p, L.b.p, L.r.p, L.fac.p, L.nmask.p, L.g, L.K, L.shift);
+    launch_residual<float>(s, x, b, L.r.p, L.fac.p, L.nmask.p, L.g, L.K, L.shift);
 }
 
 // z = V(r): one V-cycle on r (FP64 or FP32 DOF vector of level 0).
@@ -561,59 +557,77 @@ void gmg_vcycle(hx_ctx* c, const T* r, T* z) {
   HX_REQUIRE(G.ready, "multigrid hierarchy not set up");
   cudaStream_t s = c->stream;
   const int nl = G.nl;
-  {
-    auto& L0 = G.lv[0];
-    const int64_t n = L0.g.dofs();
-    k_copy_cvt<float, T><<<gblocks(n), 256, 0, s>>>(L0.b.p, r, n);
+  // level 0's right-hand side and solution: r and z themselves in FP32
+  // (neither is touched by anything else during the cycle), FP32 copies of
+  // FP64 vectors otherwise
+  auto& L0 = G.lv[0];
+  const int64_t n0 = L0.g.dofs();
+  const float* b0;
+  float* x0;
+  if constexpr (std::is_same<T, float>::value) {
+    b0 = r;
+    x0 = z;
+  } else {
+    k_copy_cvt<float, T><<<gblocks(n0), 256, 0, s>>>(L0.b.p, r, n0);
     HX_CHECK_LAUNCH();
+    b0 = L0.b.p;
+    x0 = L0.x.p;
   }
+  auto bx = [&](int l, const float*& b, float*& x) {
+    b = l == 0 ? b0 : G.lv[l].b.p;
+    x = l == 0 ? x0 : G.lv[l].x.p;
+  };
   for (int l = 0; l + 1 < nl; ++l) {
     auto& L = G.lv[l];
     auto& C = G.lv[l + 1];
-    cheb_smooth(c, L, true, true);
-    launch_restrict(s, 3, L.r.p, C.b.p, node_grid(L.g), node_grid(C.g), false);
-    k_mask3<<<gblocks(3 * C.g.nodes()), 256, 0, s>>>(C.b.p, C.nmask.p, C.g.nodes());
-    HX_CHECK_LAUNCH();
+    const float* b;
+    float* x;
+    bx(l, b, x);
+    cheb_smooth(c, L, b, x, true, true);
+    // coarse right-hand side R r, zero on the coarse fixed DOFs
+    launch_restrict(s, 3, L.r.p, C.b.p, node_grid(L.g), node_grid(C.g), false, C.nmask.p);
   }
-  if (G.direct) {
-    // coarsest level (the only one for small grids): its dense inverse
+  {
     auto& L = G.lv[nl - 1];
     const int64_t n = L.g.dofs();
-    k_dense_gemv<<<(unsigned)cdiv(n * 32, 256), 256, 0, s>>>(G.ainv.p, L.b.p, L.x.p, n);
-    HX_CHECK_LAUNCH();
-  } else {
-    // a large coarsest level: fixed-count FP32 Jacobi-PCG from zero
-    auto& L = G.lv[nl - 1];
-    const int64_t n = L.g.dofs();
-    CgState* st = G.coarse_st.p;
-    k_coarse_reset<<<1, 32, 0, s>>>(st, GMG_COARSE_ITERS, 1e-4);
-    HX_CHECK_LAUNCH();
-    launch_fill_zero(s, L.x.p, n * sizeof(float));
-    launch_cg_init<float>(s, L.b.p, nullptr, L.minv.p, L.r.p, G.p1.p, n, st, c->d_partials.p);
-    for (int it = 0; it < GMG_COARSE_ITERS; it += 2) {
-      launch_pcg_step<float>(s, G.p1.p, G.p0.p, L.r.p, L.minv.p, L.x.p, L.q.p, L.fac.p,
-                             L.nmask.p, L.g, L.K, L.shift, st, c->d_partials.p);
-      launch_cg_update2<float>(s, L.r.p, L.q.p, L.minv.p, n, st, c->d_partials.p);
-      launch_pcg_step<float>(s, G.p0.p, G.p1.p, L.r.p, L.minv.p, L.x.p, L.q.p, L.fac.p,
-                             L.nmask.p, L.g, L.K, L.shift, st, c->d_partials.p);
-      launch_cg_update2<float>(s, L.r.p, L.q.p, L.minv.p, n, st, c->d_partials.p);
+    const float* b;
+    float* x;
+    bx(nl - 1, b, x);
+    if (G.direct) {
+      // coarsest level (the only one for small grids): its dense inverse
+      k_dense_gemv<<<(unsigned)cdiv(n * 32, 256), 256, 0, s>>>(G.ainv.p, b, x, n);
+      HX_CHECK_LAUNCH();
+    } else {
+      // a large coarsest level: fixed-count FP32 Jacobi-PCG from zero
+      CgState* st = G.coarse_st.p;
+      k_coarse_reset<<<1, 32, 0, s>>>(st, GMG_COARSE_ITERS, 1e-4);
+      HX_CHECK_LAUNCH();
+      launch_fill_zero(s, x, n * sizeof(float));
+      launch_cg_init<float>(s, b, nullptr, L.minv.p, L.r.p, G.p1.p, n, st, c->d_partials.p);
+      for (int it = 0; it < GMG_COARSE_ITERS; it += 2) {
+        launch_pcg_step<float>(s, G.p1.p, G.p0.p, L.r.p, L.minv.p, x, L.q.p, L.fac.p,
+                               L.nmask.p, L.g, L.K, L.shift, st, c->d_partials.p);
+        launch_cg_update2<float>(s, L.r.p, L.q.p, L.minv.p, n, st, c->d_partials.p);
+        launch_pcg_step<float>(s, G.p0.p, G.p1.p, L.r.p, L.minv.p, x, L.q.p, L.fac.p,
+                               L.nmask.p, L.g, L.K, L.shift, st, c->d_partials.p);
+        launch_cg_update2<float>(s, L.r.p, L.q.p, L.minv.p, n, st, c->d_partials.p);
+      }
+      k_coarse_finish<<<gblocks(n), 256, 0, s>>>(x, G.p0.p, G.p1.p, st, n);
+      HX_CHECK_LAUNCH();
     }
-    k_coarse_finish<<<gblocks(n), 256, 0, s>>>(L.x.p, G.p0.p, G.p1.p, st, n);
-    HX_CHECK_LAUNCH();
   }
   for (int l = nl - 2; l >= 0; --l) {
     auto& L = G.lv[l];
     auto& C = G.lv[l + 1];
-    // x_l += P x_{l+1}, masked; then post-smoothing from it
-    launch_prolong(s, C.x.p, L.x.p, node_grid(L.g), node_grid(C.g), true);
-    k_mask3<<<gblocks(3 * L.g.nodes()), 256, 0, s>>>(L.x.p, L.nmask.p, L.g.nodes());
-    HX_CHECK_LAUNCH();
-    cheb_smooth(c, L, false, false);
+    const float* b;
+    float* x;
+    bx(l, b, x);
+    // x_l += P x_{l+1}, zero on the fixed DOFs; then post-smoothing from it
+    launch_prolong(s, C.x.p, x, node_grid(L.g), node_grid(C.g), true, L.nmask.p);
+    cheb_smooth(c, L, b, x, false, false);
   }
-  {
-    auto& L0 = G.lv[0];
-    const int64_t n = L0.g.dofs();
-    k_copy_cvt<T, float><<<gblocks(n), 256, 0, s>>>(z, L0.x.p, n);
+  if constexpr (!std::is_same<T, float>::value) {
+    k_copy_cvt<T, float><<<gblocks(n0), 256, 0, s>>>(z, L0.x.p, n0);
     HX_CHECK_LAUNCH();
   }
 }
