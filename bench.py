@@ -485,7 +485,8 @@ def run_c4_loop(args):
              ("mixed32_jacobi", dict(precision=1, preconditioner=0, shift_factor=1e-6)),
              ("mixed32_learned_fcg", dict(precision=1, preconditioner=1, finetune_every=20,
                                           shift_factor=1e-6)),
-             ("mixed32_multigrid_fcg", dict(precision=1, preconditioner=3, shift_factor=1e-6))]
+             ("mixed32_multigrid_fcg", dict(precision=1, preconditioner=3, shift_factor=1e-6)),
+             ("fp64_multigrid_fcg", dict(precision=0, preconditioner=3, shift_factor=1e-6))]
     if args.c4_forms:
         keep = set(args.c4_forms.split(","))
         forms = [f for f in forms if f[0] in keep]
@@ -544,9 +545,9 @@ def run_c4_loop(args):
            "forms": out_forms,
            "speedup_vs_fp64_loop": a["s_per_loop"] / b["s_per_loop"],
            "speedup_vs_mixed_jacobi_loop": mj["s_per_loop"] / b["s_per_loop"],
-           "multigrid_loop_speedup_vs_fp64_loop": (
-               a["s_per_loop"] / out_forms["mixed32_multigrid_fcg"]["s_per_loop"]
-               if "mixed32_multigrid_fcg" in out_forms else None),
+           "multigrid_loop_speedup_vs_fp64_loop": {
+               k: a["s_per_loop"] / out_forms[k]["s_per_loop"]
+               for k in ("mixed32_multigrid_fcg", "fp64_multigrid_fcg") if k in out_forms},
            "final_compliance_rel_diff": abs(b["final_compliance"] - a["final_compliance"])
            / a["final_compliance"]}
     print(json.dumps(out), flush=True)
