@@ -119,6 +119,7 @@ PROTOTYPES = {
     "hx_net_prepare": (_i32, [_vp, _vp]),
     "hx_net_apply": (_i32, [_vp, _vp, _vp]),
     "hx_gmg_apply": (_i32, [_vp, _vp, _vp]),
+    "hx_set_dropin_solver": (_i32, [_vp, C.c_int32, C.c_int32, C.c_int32]),
     "hx_selftest_wait_timeout": (_i32, [_vp, C.POINTER(_i32)]),
     "hx_simp_device": (_i32, [_vp, _vp, _dbl, _dbl, _dbl, _vp]),
     "hx_sensitivity_device": (_i32, [_vp, _vp, _vp, _dbl, _dbl, _dbl, _vp]),
@@ -354,6 +355,14 @@ class Context:
     def net_apply(self, r_ptr, z_ptr):
         self.check(self.lib.hx_net_apply(self.h, C.c_void_p(r_ptr), C.c_void_p(z_ptr)),
                    "hx_net_apply")
+
+    def set_dropin_solver(self, preconditioner=HX_PC_JACOBI, precision=HX_PREC_FP64,
+                          multigrid_fallback=1):
+        """Solver of this context's drop-in solves (api.solve_system_gpu /
+        solve_system_grid); the default is the reference's "jacobi_amg"."""
+        self.check(self.lib.hx_set_dropin_solver(self.h, int(preconditioner), int(precision),
+                                                 int(multigrid_fallback)),
+                   "hx_set_dropin_solver")
 
     def gmg_apply(self, r_ptr, z_ptr):
         self.check(self.lib.hx_gmg_apply(self.h, C.c_void_p(r_ptr), C.c_void_p(z_ptr)),

@@ -32,6 +32,29 @@ def _p(a):
     return a.ctypes.data_as(C.c_void_p) if a is not None else None
 
 
+# config["solver_parameters"]["preconditioner"] -> (preconditioner, precision,
+# multigrid fallback) of the drop-in solve, as the reference reads it on every
+# solve (src/Solvers/GPUSolver.jl:320-324; the multigrid preconditioner takes
+# AMG's place)
+_PRECONDITIONERS = {"jacobi": (_lib.HX_PC_JACOBI, _lib.HX_PREC_FP64, 0),
+                    "jacobi_amg": (_lib.HX_PC_JACOBI, _lib.HX_PREC_FP64, 1),
+                    "amg": (_lib.HX_PC_MULTIGRID, _lib.HX_PREC_FP64, 0)}
+
+
+def _apply_solver_config(ctx, config):
+    """Select the drop-in solver from the reference's config, if it names
+    one (its default, as the reference's code default, is "jacobi")."""
+    if not config:
+        return
+    sp = config.get("solver_parameters", {}) or {}
+    if "preconditioner" not in sp:
+        return
+    name = str(sp["preconditioner"]).lower()
+    if name not in _PRECONDITIONERS:
+        raise ValueError(f"unknown preconditioner {sp['preconditioner']!r}")
+    ctx.set_dropin_solver(*_PRECONDITIONERS[name])
+
+
 def solve_system_gpu(nodes, elements, E, nu, bc_indicator, f, density, *, max_iter=40000,
                      tol=1e-6, method="native", solver="cg", use_precond=True,
                      shift_factor=1.0e-6, min_stiffness_threshold=1.0e-3, u_guess=None,
@@ -39,8 +62,11 @@ def solve_system_gpu(nodes, elements, E, nu, bc_indicator, f, density, *, max_it
     """GPUSolver.solve_system_gpu -> (x_full::float32[3nN], final_rel_res, prec_name).
 
     As in the reference, a solve whose every attempt fails still returns the
-    best iterate (with a warning); bad input raises."""
+    best iterate (with a warning); bad input raises.  A config naming
+    solver_parameters.preconditioner ("jacobi", "jacobi_amg", "amg") selects
+    the solver as the reference does ("amg": the multigrid preconditioner)."""
     ctx = ctx or default_context()
+    _apply_solver_config(ctx, config)
     nodes_cm = np.asfortranarray(nodes, dtype=np.float32)
     el_cm = np.asfortranarray(elements, dtype=np.int64)
     bc_cm = np.asfortranarray(bc_indicator, dtype=np.float32)

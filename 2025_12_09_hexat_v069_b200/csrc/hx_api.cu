@@ -534,6 +534,29 @@ HX_API hx_status hx_solve_device(hx_ctx* c, const double* f, const double* fac, 
   });
 }
 
+// Name of the preconditioner that finished a drop-in solve (the reference
+// returns "Jacobi" or "AMG"; the multigrid preconditioner replaces AMG).
+static const char* dropin_prec_name(int32_t pc, const hx_solve_report& R) {
+  if (R.zero_rhs) return "None";
+  if (pc == HX_PC_MULTIGRID) return "GMG";
+  if (pc == HX_PC_LEARNED) return R.fallback_used ? "Jacobi" : "Learned";
+  return R.fallback_used ? "GMG" : "Jacobi";
+}
+
+HX_API hx_status hx_set_dropin_solver(hx_ctx* c, int32_t preconditioner, int32_t precision,
+                                      int32_t multigrid_fallback) {
+  return guard(c, [&] {
+    HX_REQUIRE(preconditioner == HX_PC_JACOBI || preconditioner == HX_PC_LEARNED ||
+                   preconditioner == HX_PC_MULTIGRID,
+               "drop-in preconditioner must be Jacobi, learned or multigrid");
+    HX_REQUIRE(precision == HX_PREC_FP64 || precision == HX_PREC_MIXED32, "unsupported precision");
+    c->dropin_pc = preconditioner;
+    c->dropin_prec = precision;
+    c->dropin_fallback = multigrid_fallback != 0;
+    return HX_OK;
+  });
+}
+
 HX_API hx_status hx_solve_system_gpu(hx_ctx* c, const float* nodes, int64_t nN,
                                      const int64_t* elements, int64_t nE, float E, float nu,
                                      const float* bc_indicator, const float* f,
@@ -579,9 +602,12 @@ HX_API hx_status hx_solve_system_gpu(hx_ctx* c, const float* nodes, int64_t nN,
     o.ref_retry = 1;
     o.keep_best = 1;
     o.divergence_checks = 1;
-    // the reference's default "jacobi_amg" (configs/default.yaml:191):
-    // multigrid takes over from a failed Jacobi attempt
-    o.multigrid_fallback = 1;
+    // hx_set_dropin_solver; by default the reference's "jacobi_amg"
+    // (configs/default.yaml:191): multigrid takes over from a failed Jacobi
+    // attempt
+    o.preconditioner = c->dropin_pc;
+    o.precision = c->dropin_prec;
+    o.multigrid_fallback = c->dropin_fallback;
     std::vector<float> u(3 * nN, 0.0f);
     if (u_guess) std::memcpy(u.data(), u_guess, u.size() * sizeof(float));
     hx_solve_report R{};
@@ -598,7 +624,7 @@ HX_API hx_status hx_solve_system_gpu(hx_ctx* c, const float* nodes, int64_t nN,
     down_nodes3(c, HX_F32, du, x_full);
     if (final_rel_res) *final_rel_res = R.rel_res;
     if (prec_name && prec_name_cap > 0) {
-      const char* nm = R.zero_rhs ? "None" : (R.fallback_used ? "GMG" : "Jacobi");
+      const char* nm = dropin_prec_name(c->dropin_pc, R);
       std::strncpy(prec_name, nm, (size_t)prec_name_cap - 1);
       prec_name[prec_name_cap - 1] = '\0';
     }
@@ -651,9 +677,12 @@ HX_API hx_status hx_solve_system_grid(hx_ctx* c, int64_t nx, int64_t ny, int64_t
     o.ref_retry = 1;
     o.keep_best = 1;
     o.divergence_checks = 1;
-    // the reference's default "jacobi_amg" (configs/default.yaml:191):
-    // multigrid takes over from a failed Jacobi attempt
-    o.multigrid_fallback = 1;
+    // hx_set_dropin_solver; by default the reference's "jacobi_amg"
+    // (configs/default.yaml:191): multigrid takes over from a failed Jacobi
+    // attempt
+    o.preconditioner = c->dropin_pc;
+    o.precision = c->dropin_prec;
+    o.multigrid_fallback = c->dropin_fallback;
     hx_solve_report R{};
     hx_status s = hx::solve_grid(c, df, dfac, du, o, &R);
     float* so = (float*)c->d_stage.ensure(n * sizeof(float));
@@ -662,7 +691,7 @@ HX_API hx_status hx_solve_system_grid(hx_ctx* c, int64_t nx, int64_t ny, int64_t
     HX_CUDA(cudaStreamSynchronize(c->stream));
     if (final_rel_res) *final_rel_res = R.rel_res;
     if (prec_name && prec_name_cap > 0) {
-      const char* nm = R.zero_rhs ? "None" : (R.fallback_used ? "GMG" : "Jacobi");
+      const char* nm = dropin_prec_name(c->dropin_pc, R);
       std::strncpy(prec_name, nm, (size_t)prec_name_cap - 1);
       prec_name[prec_name_cap - 1] = '\0';
     }

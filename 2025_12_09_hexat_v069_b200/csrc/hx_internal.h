@@ -178,6 +178,9 @@ struct hx_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev_in = nullptr;  // orders the stream after the legacy default stream
+  // preconditioner, precision and multigrid fallback of the reference-shaped
+  // drop-in solves (the reference's "jacobi_amg" by default)
+  int32_t dropin_pc = 0, dropin_prec = 0, dropin_fallback = 1;
   std::string err;
 
   // mesh

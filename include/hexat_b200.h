@@ -212,6 +212,20 @@ HX_API hx_status hx_solve_device(hx_ctx *ctx, const double *f_dev,
                                  const hx_solve_opts *opts,
                                  hx_solve_report *report);
 
+/* The solver of this context's drop-in solves (hx_solve_system_gpu,
+ * hx_solve_system_grid).  The reference reads
+ * config["solver_parameters"]["preconditioner"] on every solve
+ * (src/Solvers/GPUSolver.jl:320-324): "jacobi" = (HX_PC_JACOBI,
+ * HX_PREC_FP64, multigrid_fallback 0); "jacobi_amg", the default of
+ * configs/default.yaml:191 and of this library = (HX_PC_JACOBI,
+ * HX_PREC_FP64, 1); "amg" = (HX_PC_MULTIGRID, HX_PREC_FP64, 0), the
+ * multigrid preconditioner from the first attempt (prec_name "GMG").
+ * HX_PREC_MIXED32 and HX_PC_LEARNED (needs loaded networks; prec_name
+ * "Learned", or "Jacobi" when it fell back) are further choices.  The
+ * retry and shift-escalation semantics apply to every choice. */
+HX_API hx_status hx_set_dropin_solver(hx_ctx *ctx, int32_t preconditioner, int32_t precision,
+                                      int32_t multigrid_fallback);
+
 /* Drop-in for GPUSolver.solve_system_gpu(nodes, elements, E, nu,
  * bc_indicator, f, density; max_iter, tol, shift_factor,
  * min_stiffness_threshold, u_guess) -> (x_full, final_rel_res, prec_name),

@@ -170,3 +170,35 @@ def test_smoothing_degree_option(ctx, hx):
     with pytest.raises(hx.HexatError) as err:
         ctx.solve(f, fac, tol=1e-9, preconditioner=3, mg_smooth_degree=9)
     assert err.value.status == 6  # HX_BAD_ARG
+
+
+def test_dropin_solve_with_multigrid_selected(ctx, hx):
+    """hx_set_dropin_solver, and the reference's config key that selects it
+    (solver_parameters.preconditioner = "amg"): the reference-shaped
+    solve_system_gpu runs the multigrid-preconditioned solve from its first
+    attempt (prec_name "GMG") and returns the Jacobi drop-in's solution
+    within the tolerances of both solves; "jacobi_amg" brings back the
+    default."""
+    from importlib import import_module
+    api = import_module("2025_12_09_hexat_v069_b200.api")
+    dims = (40, 12, 12)
+    nodes, el, bc, f = hx.workloads.cantilever(*dims)
+    dens = np.random.default_rng(5).uniform(0.2, 1.0, el.shape[0]).astype(np.float32)
+    args = (nodes, el, 1.0, 0.3, bc, f.astype(np.float32), dens)
+    amg = {"solver_parameters": {"preconditioner": "amg"}}
+    default = {"solver_parameters": {"preconditioner": "jacobi_amg"}}
+    try:
+        xj, rj, nj = api.solve_system_gpu(*args, tol=1e-7, ctx=ctx)
+        xm, rm, nm = api.solve_system_gpu(*args, tol=1e-7, config=amg, ctx=ctx)
+        ctx.set_dropin_solver(3, 1, 0)  # mixed precision multigrid
+        xq, rq, nq = api.solve_system_gpu(*args, tol=1e-7, ctx=ctx)
+    finally:
+        ctx.set_dropin_solver(0, 0, 1)
+    assert nj == "Jacobi" and nm == "GMG" and nq == "GMG"
+    assert rj < 1e-7 and rm < 1e-7 and rq < 1e-7
+    scale = np.abs(xj).max()
+    assert np.abs(xm - xj).max() <= 1e-4 * scale and np.abs(xq - xj).max() <= 1e-4 * scale
+    _, _, n0 = api.solve_system_gpu(*args, tol=1e-7, config=default, ctx=ctx)
+    assert n0 == "Jacobi"
+    with pytest.raises(hx.HexatError):
+        ctx.set_dropin_solver(2, 0, 0)  # HX_PC_NONE is not a drop-in choice

@@ -148,3 +148,30 @@ def test_update_params_from_reference_config(hx):
     cfg["optimization_parameters"]["update"] = "bogus"
     with pytest.raises(ValueError):
         api.update_params(cfg)
+
+
+def test_reference_preconditioner_config_maps_to_dropin_solver():
+    """The reference's solver_parameters.preconditioner values select the
+    drop-in solver (src/Solvers/GPUSolver.jl:320-324): jacobi, jacobi_amg
+    (Jacobi with the multigrid fallback), amg (multigrid from the start);
+    no key leaves the context's choice; an unknown name is an error."""
+    import importlib
+    api = importlib.import_module("2025_12_09_hexat_v069_b200.api")
+
+    class Fake:
+        calls = []
+
+        def set_dropin_solver(self, *a):
+            self.calls.append(a)
+
+    ctx = Fake()
+    for name, want in [("Jacobi", (0, 0, 0)), ("jacobi_amg", (0, 0, 1)), ("AMG", (3, 0, 0))]:
+        api._apply_solver_config(ctx, {"solver_parameters": {"preconditioner": name}})
+        assert ctx.calls[-1] == want
+    n = len(ctx.calls)
+    api._apply_solver_config(ctx, {"solver_parameters": {}})
+    api._apply_solver_config(ctx, None)
+    assert len(ctx.calls) == n
+    import pytest
+    with pytest.raises(ValueError):
+        api._apply_solver_config(ctx, {"solver_parameters": {"preconditioner": "ilu"}})
