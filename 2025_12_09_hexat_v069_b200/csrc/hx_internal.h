@@ -51,8 +51,11 @@ struct DevBuf {
 };
 
 // ---- operator (hx_operator.cu) ----
-int mv_kchunk(const Grid& g);
-size_t mv_num_blocks(const Grid& g);
+// z-chunk length for `resident` CTAs per SM; CTAs of one launch; the most
+// CTAs of any precision (the reduction workspace's size)
+int mv_kchunk(const Grid& g, int resident);
+size_t mv_num_blocks(const Grid& g, int resident);
+size_t mv_max_blocks(const Grid& g);
 template <typename T>
 void launch_matvec(cudaStream_t s, int mode, const T* x, T* y, const T* fac, const uint8_t* nmask,
                    const Grid& g, const ElemCoef<T>& K, T shift, CgState* st, double* partials,

@@ -87,7 +87,7 @@ extern "C" HX_API hx_status hx_apply_stiffness_noalloc(int64_t nx, int64_t ny, i
   g.nyn = g.nye + 1;
   g.nzn = g.nze + 1;
   // The reduction writes one partial sum per CTA of the operator kernel.
-  if (hx::mv_num_blocks(g) > (size_t)HX_NOALLOC_MAX_BLOCKS) return HX_BAD_ARG;
+  if (hx::mv_num_blocks(g, 2) > (size_t)HX_NOALLOC_MAX_BLOCKS) return HX_BAD_ARG;  // FP64: 2 CTAs/SM
   unsigned char* base = nullptr;
   const hx_status st = scratch_address(&base);
   if (st != HX_OK) return st;

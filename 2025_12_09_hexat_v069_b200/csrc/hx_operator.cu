@@ -39,7 +39,11 @@ namespace {
 
 constexpr int MV_BX = 32;
 constexpr int MV_BY = 8;
-constexpr int MV_RESIDENT = 2;  // CTAs per SM (the __launch_bounds__ minimum)
+// CTAs per SM (the __launch_bounds__ minimum): FP32 instantiations fit 80
+// registers and three CTAs' rings in shared memory (3% faster than two at
+// C1); FP64 ones need 128 registers.
+template <typename T>
+constexpr int mv_resident() { return sizeof(T) == 4 ? 3 : 2; }
 
 // Planes requested ahead of the layer being computed (>= 3).  A deeper ring
 // keeps more bytes in flight per SM: FP32 runs 2% faster at depth 5 than 3
@@ -580,7 +584,7 @@ inline dim3 mv_grid(const Grid& g, int kchunk) {
 template <typename T, int MODE>
 void launch_struct(cudaStream_t s, const OpArgs<T>& a) {
   constexpr bool FUSED = MODE == 3 || MODE == 4;
-  constexpr int MINB = 2;
+  constexpr int MINB = mv_resident<T>();
   const size_t smem = sizeof(OpSmem<T, MV_BY, FUSED>);
   static PerDeviceOnce configured;  // per instantiation and device
   configured.run([&] {
@@ -593,13 +597,13 @@ void launch_struct(cudaStream_t s, const OpArgs<T>& a) {
 
 }  // namespace
 
-int mv_kchunk(const Grid& g) {
+int mv_kchunk(const Grid& g, int resident) {
   // Node planes per CTA: the chunk length kc (at least 8, so the two staged
   // halo planes stay a small share) that minimises (waves of resident CTAs)
   // x (planes each CTA stages, kc + 2).  A last wave that fills few SMs
   // costs as much as a full one; ties go to the longer chunk.
   const int64_t cols = (int64_t)cdiv(g.nxn, MV_BX - 1) * cdiv(g.nyn, MV_BY - 1);
-  const int64_t slots = (int64_t)MV_RESIDENT * sm_count();
+  const int64_t slots = (int64_t)resident * sm_count();
   int best_kc = g.nzn;
   int64_t best = INT64_MAX;
   for (int kc = std::min(8, g.nzn); kc <= g.nzn; ++kc) {
@@ -613,9 +617,13 @@ int mv_kchunk(const Grid& g) {
   return best_kc;
 }
 
-size_t mv_num_blocks(const Grid& g) {
-  const dim3 gr = mv_grid(g, mv_kchunk(g));
+size_t mv_num_blocks(const Grid& g, int resident) {
+  const dim3 gr = mv_grid(g, mv_kchunk(g, resident));
   return (size_t)gr.x * gr.y * gr.z;
+}
+
+size_t mv_max_blocks(const Grid& g) {
+  return std::max(mv_num_blocks(g, mv_resident<float>()), mv_num_blocks(g, mv_resident<double>()));
 }
 
 template <typename T>
@@ -628,7 +636,7 @@ void launch_matvec(cudaStream_t s, int mode, const T* x, T* y, const T* fac, con
   a.fac = fac;
   a.nmask = nmask;
   a.g = g;
-  a.kchunk = mv_kchunk(g);
+  a.kchunk = mv_kchunk(g, mv_resident<T>());
   a.K = K;
   a.shift = shift;
   a.st = st;
@@ -657,7 +665,7 @@ void launch_cheb_step(cudaStream_t s, const T* x, T* xprev_new, bool xprev_zero,
   a.fac = fac;
   a.nmask = nmask;
   a.g = g;
-  a.kchunk = mv_kchunk(g);
+  a.kchunk = mv_kchunk(g, mv_resident<T>());
   a.K = K;
   a.shift = shift;
   launch_struct<T, 5>(s, a);
@@ -676,7 +684,7 @@ void launch_residual(cudaStream_t s, const T* x, const T* b, T* r, const T* fac,
   a.fac = fac;
   a.nmask = nmask;
   a.g = g;
-  a.kchunk = mv_kchunk(g);
+  a.kchunk = mv_kchunk(g, mv_resident<T>());
   a.K = K;
   a.shift = shift;
   launch_struct<T, 6>(s, a);
@@ -699,7 +707,7 @@ void launch_pcg_step(cudaStream_t s, const T* pin, T* pout, const T* r, const T*
   a.fac = fac;
   a.nmask = nmask;
   a.g = g;
-  a.kchunk = mv_kchunk(g);
+  a.kchunk = mv_kchunk(g, mv_resident<T>());
   a.K = K;
   a.shift = shift;
   a.st = st;
@@ -720,7 +728,7 @@ void launch_fcg_step(cudaStream_t s, const T* pin, T* pout, const T* z, T* x, T*
   a.fac = fac;
   a.nmask = nmask;
   a.g = g;
-  a.kchunk = mv_kchunk(g);
+  a.kchunk = mv_kchunk(g, mv_resident<T>());
   a.K = K;
   a.shift = shift;
   a.st = st;

@@ -95,7 +95,7 @@ static double now_ms() {
 void ensure_workspace(hx_ctx* c) {
   if (!c->h_state) HX_CUDA(cudaMallocHost(&c->h_state, 4 * sizeof(CgState)));
   c->d_state.ensure(4);
-  const size_t nb = std::max<size_t>(mv_num_blocks(c->g), 64ull * sm_count());
+  const size_t nb = std::max<size_t>(mv_max_blocks(c->g), 64ull * sm_count());
   c->d_partials.ensure(4 * nb);
   c->d_scalars.ensure(16);
 }
