@@ -366,9 +366,10 @@ def variants(hx, ctx, f, fac, f_d, fac_d, lib_stream, dims=DIMS):
     """The solver forms on the same workload, each timed once on the device
     after one untimed run: FP64 and mixed (FP32 in FP64 reliable updates)
     Jacobi-PCG, flexible CG with the shipped learned preconditioner in FP64
-    and mixed, and flexible CG with the geometric multigrid V-cycle.  Errors of u, compliance f.u and max von Mises stress
-    against the FP64 Jacobi-PCG solution, and each solution's relative
-    residual recomputed on the host by the oracle (oracle_true_rel_res)."""
+    and mixed, and flexible CG with the geometric multigrid V-cycle.  Errors
+    of u, compliance f.u and max von Mises stress against the FP64 Jacobi-PCG
+    solution, and each solution's relative residual recomputed on the host by
+    the oracle (oracle_true_rel_res); then the mixed forms to rtol 1e-8."""
     import importlib
     import torch
     learned = importlib.import_module(hx.__name__ + ".learned")
@@ -380,14 +381,7 @@ def variants(hx, ctx, f, fac, f_d, fac_d, lib_stream, dims=DIMS):
     for name, (prec, pc) in FORMS.items():
         opts = hx.default_opts(tol=1e-6, max_iter=100000, precision=prec, preconditioner=pc)
         try:
-            ctx.solve_device(f_d.data_ptr(), fac_d.data_ptr(), u.data_ptr(), opts=opts)
-            torch.cuda.synchronize()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(lib_stream)
-            rep = ctx.solve_device(f_d.data_ptr(), fac_d.data_ptr(), u.data_ptr(), opts=opts)
-            e1.record(lib_stream)
-            e1.synchronize()
+            rep, s = _timed_solve(ctx, f_d, fac_d, u, opts, lib_stream)
         except hx.HexatError as e:  # a form that fails is reported, not timed
             out[name] = {"error": str(e)}
             continue
@@ -397,7 +391,7 @@ def variants(hx, ctx, f, fac, f_d, fac_d, lib_stream, dims=DIMS):
             ref = (uh.copy(), float(f @ uh), vm.copy(), float(np.max(vm)))
         u64, c64, vm64, vmax64 = ref
         out[name] = {
-            "s_per_solve": e0.elapsed_time(e1) / 1e3, "iterations": rep.iterations,
+            "s_per_solve": s, "iterations": rep.iterations,
             "true_rel_res": rep.true_rel_res, "fallback": rep.fallback_used,
             "refinements": rep.refinements,
             "precond_setup_s": rep.time_precond_setup_ms / 1e3,
@@ -410,9 +404,55 @@ def variants(hx, ctx, f, fac, f_d, fac_d, lib_stream, dims=DIMS):
     for v in out.values():
         if "s_per_solve" in v:
             v["speedup_vs_fp64_jacobi"] = base / v["s_per_solve"]
+    out["stretch_1e-8"] = stretch(hx, ctx, f, fac, f_d, fac_d, lib_stream, check, u)
     out["_note"] = ("learned forms use the shipped networks (weights/spd_cnn_mix.npy); "
                     "errors against the FP64 Jacobi-PCG solution at rtol 1e-6; "
                     "oracle_true_rel_res = ||b - K u|| / ||b|| with the oracle's CPU K.u")
+    return out
+
+
+def _timed_solve(ctx, f_d, fac_d, u, opts, lib_stream):
+    """One untimed solve, then one timed on the library stream: (report, s)."""
+    import torch
+    ctx.solve_device(f_d.data_ptr(), fac_d.data_ptr(), u.data_ptr(), opts=opts)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(lib_stream)
+    rep = ctx.solve_device(f_d.data_ptr(), fac_d.data_ptr(), u.data_ptr(), opts=opts)
+    e1.record(lib_stream)
+    e1.synchronize()
+    return rep, e0.elapsed_time(e1) / 1e3
+
+
+def stretch(hx, ctx, f, fac, f_d, fac_d, lib_stream, check, u):
+    """The mixed forms to the stretch tolerance rtol 1e-8; errors against an
+    FP64 multigrid-FCG solution to rtol 1e-10 of the same system."""
+    rep, _ = _timed_solve(ctx, f_d, fac_d, u, hx.default_opts(
+        tol=1e-10, max_iter=100000, precision=0, preconditioner=3), lib_stream)
+    u64 = u.cpu().numpy()
+    c64 = float(f @ u64)
+    vm64 = ctx.stress(u64, fac, 1.0, 0.3)[1]
+    vmax64 = float(np.max(vm64))
+    out = {"_reference": {"form": "fp64_multigrid_fcg", "tol": 1e-10,
+                          "true_rel_res": rep.true_rel_res, "oracle_true_rel_res": check(u64)}}
+    for name in ("mixed32_jacobi", "mixed32_learned_fcg", "mixed32_multigrid_fcg"):
+        prec, pc = FORMS[name]
+        opts = hx.default_opts(tol=1e-8, max_iter=200000, precision=prec, preconditioner=pc)
+        try:
+            rep, s = _timed_solve(ctx, f_d, fac_d, u, opts, lib_stream)
+        except hx.HexatError as e:
+            out[name] = {"error": str(e)}
+            continue
+        uh = u.cpu().numpy()
+        vm = ctx.stress(uh, fac, 1.0, 0.3)[1]
+        out[name] = {
+            "s_per_solve": s, "iterations": rep.iterations, "refinements": rep.refinements,
+            "true_rel_res": rep.true_rel_res, "fallback": rep.fallback_used,
+            "u_rel_err": float(np.linalg.norm(uh - u64) / np.linalg.norm(u64)),
+            "compliance_rel_err": abs(float(f @ uh) - c64) / abs(c64),
+            "max_von_mises_rel_err": abs(float(np.max(vm)) - vmax64) / vmax64,
+            "oracle_true_rel_res": check(uh)}
     return out
 
 
