@@ -79,16 +79,16 @@ __global__ void __launch_bounds__(NTHREADS) k_conv3_wgrad(const __nv_bfloat16* _
     const int hy = r % HY, hz = r / HY;
     const int gx = x0 - 1 + hx, gy = y0 - 1 + hy, gz = z0 - 1 + hz;
     const bool ok = gx >= 0 && gy >= 0 && gz >= 0 && gx < g.nx && gy < g.ny && gz < g.nz;
-    const int64_t gn = ok ? ((int64_t)gz * g.ny + gy) * g.nx + gx : 0;
-    cp16(xb + swz(node, h), X + gn * C + h * 8, ok);
+    const int64_t go = ok ? act16(g, (int64_t)gz * g.ny + gy, gx, h) : 0;
+    cp16(xb + swz(node, h), X + go, ok);
   }
   for (int ch = threadIdx.x; ch < TX * TY * TZ * 2; ch += NTHREADS) {
     const int node = ch >> 1, h = ch & 1;  // node = x + 16 (y + 8 z)
     const int tx = node & 15, ty = (node >> 4) & 7, tz = node >> 7;
     const int gx = x0 + tx, gy = y0 + ty, gz = z0 + tz;
     const bool ok = gx < g.nx && gy < g.ny && gz < g.nz;  // outside: zero gradient
-    const int64_t gn = ok ? ((int64_t)gz * g.ny + gy) * g.nx + gx : 0;
-    cp16(db + swz(node, h), D + gn * C + h * 8, ok);
+    const int64_t go = ok ? act16(g, (int64_t)gz * g.ny + gy, gx, h) : 0;
+    cp16(db + swz(node, h), D + go, ok);
   }
   cp_commit_wait();
   __syncthreads();
@@ -573,9 +573,11 @@ __global__ void k_prolong(const float* __restrict__ coarse, float* __restrict__ 
   }
 }
 
-// The lifting E of a nodal field: X[n] = (x (3 ch), feat * x (3 ch), 0 ...) in BF16.
+// The lifting E of a nodal field: X[n] = (x (3 ch), feat * x (3 ch), 0 ...) in
+// BF16, stored as half-rows (act16).
 __global__ void k_lift(const float* __restrict__ x, const float* __restrict__ feat,
-                       __nv_bfloat16* __restrict__ X, int64_t nn) {
+                       __nv_bfloat16* __restrict__ X, GridN g) {
+  const int64_t nn = (int64_t)g.nx * g.ny * g.nz;
   for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn;
        n += (int64_t)gridDim.x * blockDim.x) {
     __align__(16) __nv_bfloat16 o[16];
@@ -588,9 +590,10 @@ __global__ void k_lift(const float* __restrict__ x, const float* __restrict__ fe
     }
 #pragma unroll
     for (int c = 6; c < 16; ++c) o[c] = __float2bfloat16_rn(0.f);
-    uint4* dst = reinterpret_cast<uint4*>(X + n * 16);
-    dst[0] = *reinterpret_cast<uint4*>(&o[0]);
-    dst[1] = *reinterpret_cast<uint4*>(&o[8]);
+    const int64_t r = n / g.nx;
+    const int xi = (int)(n - r * g.nx);
+    *reinterpret_cast<uint4*>(X + act16(g, r, xi, 0)) = *reinterpret_cast<uint4*>(&o[0]);
+    *reinterpret_cast<uint4*>(X + act16(g, r, xi, 1)) = *reinterpret_cast<uint4*>(&o[8]);
   }
 }
 
@@ -820,8 +823,9 @@ void launch_prolong(cudaStream_t s, const float* coarse, float* fine, const Grid
   HX_CHECK_LAUNCH();
 }
 
-void launch_lift(cudaStream_t s, const float* x, const float* feat, __nv_bfloat16* X, int64_t nn) {
-  k_lift<<<vec_blocks(nn), 256, 0, s>>>(x, feat, X, nn);
+void launch_lift(cudaStream_t s, const float* x, const float* feat, __nv_bfloat16* X,
+                 const GridN& g) {
+  k_lift<<<vec_blocks((int64_t)g.nx * g.ny * g.nz), 256, 0, s>>>(x, feat, X, g);
   HX_CHECK_LAUNCH();
 }
 

@@ -10,6 +10,16 @@ struct GridN {  // node grid of the network (nodes per axis)
   int nx, ny, nz;
 };
 
+// 16-channel activations are stored in half-rows: channels 8h .. 8h + 7 of
+// node (x, y, z) start at element ((r * 2 + h) * nx + x) * 8, r = z * ny + y,
+// so that each half of a node row is one contiguous run of 16 nx bytes and a
+// convolution's TMA load copies 10 nodes per row request (with [node][16] it
+// was one node's 16 bytes per request, and the loads bounded the layer).
+// 8-channel tensors (the network output y) are plain [node][8].
+__host__ __device__ inline int64_t act16(const GridN& g, int64_t r, int x, int h) {
+  return ((r * 2 + h) * g.nx + x) * 8;
+}
+
 constexpr int NET_LAYERS = 4;
 constexpr int NET_LAYER_PARAMS = 27 * 256;  // weights [27 taps][16 co][16 ci], no bias
 constexpr int NET_NET_PARAMS = NET_LAYERS * NET_LAYER_PARAMS;  // one network
@@ -49,8 +59,9 @@ void launch_restrict(cudaStream_t s, int ch, const float* in, float* out, const 
                      const GridN& gc, bool normalise, const uint8_t* cmask = nullptr);
 void launch_prolong(cudaStream_t s, const float* coarse, float* fine, const GridN& gf,
                     const GridN& gc, bool accumulate, const uint8_t* fmask = nullptr);
-// lifting E: [node][3] FP32 -> [node][16] BF16 (x, feat * x), and its transpose
-void launch_lift(cudaStream_t s, const float* x, const float* feat, __nv_bfloat16* X, int64_t nn);
+// lifting E: [node][3] FP32 -> 16-channel BF16 activation (x, feat * x), and its transpose
+void launch_lift(cudaStream_t s, const float* x, const float* feat, __nv_bfloat16* X,
+                 const GridN& g);
 void launch_unlift(cudaStream_t s, const __nv_bfloat16* Y, const float* feat, float* acc,
                    bool accumulate, int64_t nn);
 // partials k_net_output needs (one per block)

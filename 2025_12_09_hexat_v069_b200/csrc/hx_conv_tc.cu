@@ -21,9 +21,10 @@
 // per y, of 8 consecutive x: core matrix j starts at node
 // ((z + 1 + dz) * 18 + 1 + dy + j) * 10 + 1 + dx, i.e. a fixed start plus
 // j * 160 bytes (SBO = 160).  Every tap is a start address in the same
-// staged tile, so one TMA tile load per plane (box 8 ch x 10 x 18 x 4 from
-// the [z][y][x][16 ch] activation tensor; coordinates outside the grid read
-// as zero) stages all the operands.  Row m of the accumulator is node
+// staged tile, so one TMA tile load per plane (box 10 nodes x 8 ch, 18 y,
+// 4 z from the half-row activation tensor, act16 in hx_cnn.h: each row
+// request copies 160 contiguous bytes; coordinates outside the grid read as
+// zero) stages all the operands.  Row m of the accumulator is node
 // (x0 + m % 8, y0 + m / 8).  The weights are staged as [tap][plane][co][8 ci]
 // (the B operand, N = 16 rows).
 //
@@ -231,7 +232,7 @@ __global__ void __launch_bounds__(NTHREADS) k_conv3_tc(const __grid_constant__ C
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   if (threadIdx.x == 0 && !selftest)
     for (int h = 0; h < 2; ++h)
-      tma_load_4d(xb + (uint32_t)(h * PLANE_BYTES), &xmap, load_bar, h * 8, x0 - 1, y0 - 1,
+      tma_load_4d(xb + (uint32_t)(h * PLANE_BYTES), &xmap, load_bar, (x0 - 1) * 8, h, y0 - 1,
                   z0 - 1);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -250,10 +251,11 @@ __global__ void __launch_bounds__(NTHREADS) k_conv3_tc(const __grid_constant__ C
       const uint64_t a0 = smem_desc(xb, PLANE_BYTES, BX * 16);
       const uint64_t b0 = smem_desc(wsb, 256, 128);
       constexpr uint32_t idesc = instr_desc(128, 16);
+      // tap-major: consecutive MMAs go to the TZ independent accumulators
 #pragma unroll
-      for (int z = 0; z < TZ; ++z) {
+      for (int tap = 0; tap < 27; ++tap) {
 #pragma unroll
-        for (int tap = 0; tap < 27; ++tap) {
+        for (int z = 0; z < TZ; ++z) {
           const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
           const uint32_t a_off = (uint32_t)(((z + 1 + dz) * BY + 1 + dy) * BX + 1 + dx);
           umma_f16(tmem + (uint32_t)(z * 16), a0 + a_off, b0 + (uint32_t)(tap * 32), idesc,
@@ -282,16 +284,19 @@ __global__ void __launch_bounds__(NTHREADS) k_conv3_tc(const __grid_constant__ C
       tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(z * 16), v);
       const int gz = z0 + z;
       if (gx < g.nx && gy < g.ny && gz < g.nz) {
-        const int64_t node = ((int64_t)gz * g.ny + gy) * g.nx + gx;
+        const int64_t row = (int64_t)gz * g.ny + gy;
         uint32_t o[8];
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
           const __nv_bfloat162 h2 = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
           o[i] = *reinterpret_cast<const uint32_t*>(&h2);
         }
-        uint4* dst = reinterpret_cast<uint4*>(Y + node * COUT);
-        dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
-        if (COUT == 16) dst[1] = make_uint4(o[4], o[5], o[6], o[7]);
+        if (COUT == 16) {  // half-rows (act16)
+          *reinterpret_cast<uint4*>(Y + act16(g, row, gx, 0)) = make_uint4(o[0], o[1], o[2], o[3]);
+          *reinterpret_cast<uint4*>(Y + act16(g, row, gx, 1)) = make_uint4(o[4], o[5], o[6], o[7]);
+        } else {
+          *reinterpret_cast<uint4*>(Y + (row * g.nx + gx) * 8) = make_uint4(o[0], o[1], o[2], o[3]);
+        }
       }
     }
   }
@@ -321,16 +326,18 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-// Tensor map of an activation tensor [nz][ny][nx][16 ch] BF16 with the
-// staging box (8 ch, 10 x, 18 y, TZ + 2 z).
+// Tensor map of a 16-channel activation in half-rows (act16), viewed as
+// [nz][ny][2 halves][8 nx] BF16, with the staging box (10 nodes x 8 ch, one
+// half, 18 y, TZ + 2 z): a load of half h lands as the plane [z][y][x][8 ch].
 CUtensorMap activation_map(const __nv_bfloat16* X, const GridN& g) {
   auto fn = encode_fn();
   HX_REQUIRE(fn != nullptr, "cuTensorMapEncodeTiled is not available from the driver");
   HX_REQUIRE((reinterpret_cast<uintptr_t>(X) & 15) == 0, "activations must be 16-byte aligned");
   CUtensorMap map;
-  const cuuint64_t dims[4] = {16, (cuuint64_t)g.nx, (cuuint64_t)g.ny, (cuuint64_t)g.nz};
-  const cuuint64_t strides[3] = {32, (cuuint64_t)g.nx * 32, (cuuint64_t)g.nx * g.ny * 32};
-  const cuuint32_t box[4] = {8, BX, BY, BZ};
+  const cuuint64_t dims[4] = {(cuuint64_t)g.nx * 8, 2, (cuuint64_t)g.ny, (cuuint64_t)g.nz};
+  const cuuint64_t strides[3] = {(cuuint64_t)g.nx * 16, (cuuint64_t)g.nx * 32,
+                                 (cuuint64_t)g.nx * g.ny * 32};
+  const cuuint32_t box[4] = {BX * 8, 1, BY, BZ};
   const cuuint32_t estr[4] = {1, 1, 1, 1};
   const CUresult r =
       fn(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16*>(X), dims, strides,

@@ -241,7 +241,7 @@ void precond_z(hx_ctx* c, const T* r, const T* minv, CgState* st, double scale_m
       launch_restrict(c->stream, 3, N.lv[l - 1].x.p, N.lv[l].x.p, gl[l - 1], gl[l], false);
     for (int l = NET_TOP; l >= NET_L0; --l) {
       auto& L = N.lv[l];
-      launch_lift(c->stream, L.x.p, L.feat.p, L.x0.p, nodes_of(gl[l]));
+      launch_lift(c->stream, L.x.p, L.feat.p, L.x0.p, gl[l]);
       stack_forward_train(c, l - NET_L0, gl[l], L.x0.p, L.act, L.y.p);
     }
     // acc_l = E_l^T y_l (network levels) + R^T acc_{l+1}, coarsest first
@@ -268,7 +268,7 @@ void precond_z(hx_ctx* c, const T* r, const T* minv, CgState* st, double scale_m
       HX_CUDA(cudaStreamWaitEvent(ss, side == 0 ? N.ev_fork : N.ev_x[side - 1], 0));
       launch_restrict(ss, 3, N.lv[l - 1].x.p, L.x.p, gl[l - 1], gl[l], false);
       if (l < NET_TOP) HX_CUDA(cudaEventRecord(N.ev_x[side], ss));
-      launch_lift(ss, L.x.p, L.feat.p, L.x0.p, nodes_of(gl[l]));
+      launch_lift(ss, L.x.p, L.feat.p, L.x0.p, gl[l]);
       stack_apply(c, ss, l - NET_L0, gl[l], L.x0.p, L.y.p, L.pp[0].p, L.pp[1].p);
     }
     // corrections, coarsest first: acc_l = E_l^T y_l + R^T acc_{l+1}
@@ -284,7 +284,7 @@ void precond_z(hx_ctx* c, const T* r, const T* minv, CgState* st, double scale_m
       HX_CUDA(cudaEventRecord(N.ev_join[side], ss));
     }
     auto& L1 = N.lv[NET_L0];
-    launch_lift(c->stream, L1.x.p, L1.feat.p, L1.x0.p, nodes_of(gl[NET_L0]));
+    launch_lift(c->stream, L1.x.p, L1.feat.p, L1.x0.p, gl[NET_L0]);
     stack_apply(c, c->stream, 0, gl[NET_L0], L1.x0.p, L1.y.p, N.tmp[0].p, N.tmp[1].p);
     launch_unlift(c->stream, L1.y.p, L1.feat.p, L1.acc.p, false, nodes_of(gl[NET_L0]));
     if (NET_TOP > NET_L0) {
@@ -369,6 +369,22 @@ void net_get_params(hx_ctx* c, float* params) {
   HX_CUDA(cudaStreamSynchronize(c->stream));
 }
 
+// Host [node][16] (FP32; channels >= NET_IN ignored) -> a device activation
+// in half-rows (act16), BF16.
+static void upload_act16(hx_ctx* c, const GridN& g, const float* a, __nv_bfloat16* dst) {
+  const int64_t nn = (int64_t)g.nx * g.ny * g.nz;
+  std::vector<__nv_bfloat16> h((size_t)nn * 16);
+  for (int64_t n = 0; n < nn; ++n) {
+    const int64_t r = n / g.nx;
+    const int x = (int)(n - r * g.nx);
+    for (int ch = 0; ch < 16; ++ch)
+      h[act16(g, r, x, ch >> 3) + (ch & 7)] =
+          __float2bfloat16_rn(ch < NET_IN ? a[n * 16 + ch] : 0.f);
+  }
+  HX_CUDA(cudaMemcpyAsync(dst, h.data(), h.size() * 2, cudaMemcpyHostToDevice, c->stream));
+  HX_CUDA(cudaStreamSynchronize(c->stream));
+}
+
 // y = G^T G x0 of the first network and the gradient of <dy, y> w.r.t. its
 // parameters (the other networks' gradients are zero), on a given node grid
 // from host data (FP32 arrays [node][16], channels >= NET_IN ignored); for
@@ -387,15 +403,11 @@ void net_forward_backward(hx_ctx* c, int nx, int ny, int nz, const float* x0, co
   N.da.ensure(nn * 16);
   N.db.ensure(nn * 16);
   N.part.ensure(conv_num_tiles(g) * LP);
-  std::vector<__nv_bfloat16> h((size_t)nn * 16);
-  for (size_t i = 0; i < h.size(); ++i) h[i] = __float2bfloat16_rn((i % 16) < NET_IN ? x0[i] : 0.f);
-  HX_CUDA(cudaMemcpyAsync(bx0.p, h.data(), h.size() * 2, cudaMemcpyHostToDevice, c->stream));
-  HX_CUDA(cudaStreamSynchronize(c->stream));
+  upload_act16(c, g, x0, bx0.p);
   stack_forward_train(c, 0, g, bx0.p, act, by.p);
   std::vector<__nv_bfloat16> hy((size_t)nn * 8);
   HX_CUDA(cudaMemcpyAsync(hy.data(), by.p, hy.size() * 2, cudaMemcpyDeviceToHost, c->stream));
-  for (size_t i = 0; i < h.size(); ++i) h[i] = __float2bfloat16_rn((i % 16) < NET_IN ? dy[i] : 0.f);
-  HX_CUDA(cudaMemcpyAsync(N.da.p, h.data(), h.size() * 2, cudaMemcpyHostToDevice, c->stream));
+  upload_act16(c, g, dy, N.da.p);
   HX_CUDA(cudaMemsetAsync(N.grad.p, 0, NET_PARAMS * sizeof(float), c->stream));
   HX_CUDA(cudaStreamSynchronize(c->stream));
   stack_backward_train(c, 0, g, bx0.p, act, false);
@@ -460,7 +472,7 @@ double net_loss_grad(hx_ctx* c, const double* r, const double* e, int loss_kind,
                     level_grid(g, l), false);
   for (int l = NET_L0; l <= NET_TOP; ++l) {
     const GridN gl = level_grid(g, l);
-    launch_lift(c->stream, N.lv[l].gx.p, N.lv[l].feat.p, N.da.p, nodes_of(gl));
+    launch_lift(c->stream, N.lv[l].gx.p, N.lv[l].feat.p, N.da.p, gl);
     stack_backward_train(c, l - NET_L0, gl, N.lv[l].x0.p, N.lv[l].act, !first);
   }
   double loss = 0;
