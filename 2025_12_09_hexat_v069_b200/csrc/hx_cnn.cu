@@ -159,19 +159,23 @@ __global__ void k_adam(float* __restrict__ w, float* __restrict__ m, float* __re
   w[k] -= lr * (mk / c1) / (sqrtf(vk / c2) + eps);
 }
 
-// Master FP32 parameters of one layer (W[tap][co][ci]) -> the BF16 B
-// operands of the tensor-core convolution, in its shared-memory order
-// [tap][plane][row][8] (plane = which 8 of the 16 reduced channels):
-// wf for the convolution (row = co, reduced over ci) and wb for its
-// transpose (tap flipped, row = ci, reduced over co).
+// Master FP32 parameters of one layer (W[tap][co][ci], tap = (dz + 1) * 9 +
+// s, s = (dy + 1) * 3 + dx + 1) -> the BF16 B operands of the tensor-core
+// convolution, in its shared-memory order [s][plane][row][8]: per in-plane
+// shift s, 48 rows = the three z-offsets' output channels (row = b * 16 +
+// out, b = 1 - dz: dz = +1, 0, -1), plane = which 8 of the 16 reduced
+// channels.  wf for the convolution (out = co, reduced over ci) and wb for
+// its transpose (tap flipped, out = ci, reduced over co).
 __global__ void k_pack_weights(const float* __restrict__ w, __nv_bfloat16* __restrict__ wf,
                                __nv_bfloat16* __restrict__ wb) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= 27 * 256) return;
   const int tap = k / 256, co = (k / 16) % 16, ci = k % 16;
+  const int dz = tap / 9 - 1, s = tap % 9;
   const __nv_bfloat16 v = __float2bfloat16_rn(w[k]);
-  wf[((tap * 2 + (ci >> 3)) * 16 + co) * 8 + (ci & 7)] = v;
-  wb[(((26 - tap) * 2 + (co >> 3)) * 16 + ci) * 8 + (co & 7)] = v;
+  wf[((s * 2 + (ci >> 3)) * 48 + (1 - dz) * 16 + co) * 8 + (ci & 7)] = v;
+  // transpose: tap 26 - tap, i.e. dz -> -dz and s -> 8 - s
+  wb[(((8 - s) * 2 + (co >> 3)) * 48 + (1 + dz) * 16 + ci) * 8 + (co & 7)] = v;
 }
 
 // ---------------------------------------------------------------------------

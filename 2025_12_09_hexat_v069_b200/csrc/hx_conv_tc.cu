@@ -6,10 +6,17 @@
 // The transpose (backward-data pass) is the same kernel on the flipped,
 // per-tap transposed weights.
 //
-// One CTA (4 warps) computes an 8 x 16 x TZ node tile (TZ = 2).  Implicit
-// GEMM per z-slice: M = 128 nodes (8 x by 16 y), N = 16 output channels,
-// K = 27 taps x 16 channels, as 27 MMAs of M128 N16 K16 accumulating in 16
-// TMEM columns (2 slices: 32 columns).
+// One CTA (4 warps) computes an 8 x 16 x TZ node tile (TZ = 4).  Implicit
+// GEMM with the z-offset folded into N: for input plane q of the staged
+// tile (q = 0 .. TZ + 1) and in-plane shift s = (dy, dx), one MMA of M = 128
+// nodes (8 x by 16 y), N = 48 = the output channels of the three z-offsets
+// (dz = +1, 0, -1, which send plane q to output slices q - 1, q, q + 1), K
+// = 16 input channels.  A tile is (TZ + 2) x 9 such MMAs (plus TZ + 1 that
+// start a slice's accumulator) instead of TZ x 27 of N = 16: each N = 16
+// MMA costs nearly as much as an N = 48 one (the A operand, 4 KB of shared
+// memory, is read either way), so the layer needs about half the tensor
+// time.  The accumulators of slices -1 .. TZ + 2 (relative to the tile; the
+// outer four are discarded) are 16 TMEM columns each.
 //
 // Shared-memory layout.  An MMA operand descriptor (no swizzle, K-major)
 // addresses 8-row core matrices whose rows are 16 bytes apart; the stride
@@ -17,24 +24,26 @@
 // halves of K (LBO) are descriptor fields.  The input tile with its one-node
 // halo (10 x 18 x (TZ + 2) nodes) is staged as two planes of 8 channels, 16
 // bytes per node, x fastest: node (z, y, x) at ((z * 18 + y) * 10 + x) * 16.  The
-// 128 rows of z-slice z for tap (dz, dy, dx) are then 16 core matrices, one
-// per y, of 8 consecutive x: core matrix j starts at node
-// ((z + 1 + dz) * 18 + 1 + dy + j) * 10 + 1 + dx, i.e. a fixed start plus
-// j * 160 bytes (SBO = 160).  Every tap is a start address in the same
-// staged tile, so one TMA tile load per plane (box 10 nodes x 8 ch, 18 y,
-// 4 z from the half-row activation tensor, act16 in hx_cnn.h: each row
-// request copies 160 contiguous bytes; coordinates outside the grid read as
-// zero) stages all the operands.  Row m of the accumulator is node
-// (x0 + m % 8, y0 + m / 8).  The weights are staged as [tap][plane][co][8 ci]
-// (the B operand, N = 16 rows).
+// 128 rows of plane q for shift (dy, dx) are then 16 core matrices, one per
+// y, of 8 consecutive x: core matrix j starts at node
+// (q * 18 + 1 + dy + j) * 10 + 1 + dx, i.e. a fixed start plus j * 160
+// bytes (SBO = 160).  Every shift is a start address in the same staged
+// tile, so one TMA tile load per plane (box 10 nodes x 8 ch, 18 y, TZ + 2 z
+// from the half-row activation tensor, act16 in hx_cnn.h: each row request
+// copies 160 contiguous bytes; coordinates outside the grid read as zero)
+// stages all the operands.  Row m of the accumulator is node
+// (x0 + m % 8, y0 + m / 8).  The weights are staged as [s][plane][48 rows][8]
+// (the B operand; k_pack_weights in hx_cnn.cu).
 //
-// One tile per CTA; with 37 KB of shared memory 6 CTAs share an SM, so the
-// loads of some overlap the MMAs and epilogues of others (a persistent
-// variant with a 2-stage load ring, at 2 CTAs per SM, measured slower; so
-// did TZ = 4, with twice the MMAs per CTA and half the CTAs: 12.9 against
-// 11.7 us per layer on a 81 x 41 x 41 grid).
+// One tile per CTA; with 48 KB of shared memory and 128 TMEM columns 4 CTAs
+// share an SM, so the loads of some overlap the MMAs and epilogues of
+// others.  (Measured and dropped: the unfolded form, 27 N = 16 MMAs per
+// slice, 10.0 us per layer on an 81 x 41 x 41 grid; a persistent kernel
+// running all 8 layers of all three networks with grid-wide barriers,
+// slower at one CTA per SM, the most a kernel that allocates TMEM gets in
+// a cooperative launch.)
 // Thread 0 issues the bulk copy of the layer's weights (pre-packed in this
-// order) and the tile's TMA loads on one mbarrier, then the 54 MMAs and a
+// order) and the tile's TMA loads on one mbarrier, then the 59 MMAs and a
 // tcgen05.commit on a second.  Layers are launched as programmatic
 // dependents of the preceding kernel: a CTA allocates TMEM, initialises its
 // barriers and starts the weight copy while the previous layer finishes,
@@ -58,17 +67,18 @@ namespace hx {
 namespace {
 
 #ifndef HX_CONV_TZ
-#define HX_CONV_TZ 2
+#define HX_CONV_TZ 4
 #endif
 constexpr int TX = 8, TY = 16, TZ = HX_CONV_TZ;
 constexpr int BX = TX + 2, BY = TY + 2, BZ = TZ + 2;          // staged box with halo
 constexpr int BOX_NODES = BX * BY * BZ;                       // 720
 constexpr int PLANE_BYTES = BOX_NODES * 16;                   // 11520
 constexpr int X_BYTES = 2 * PLANE_BYTES;                      // 23040: [plane]
-constexpr int W_BYTES = 27 * 2 * 16 * 16;                     // 13824: [tap][plane][co]
+constexpr int W_BYTES = 9 * 2 * 48 * 16;                      // 13824: [s][plane][48 rows]
 constexpr int SMEM_BYTES = X_BYTES + W_BYTES + 64;            // + barriers, TMEM address
 constexpr int NTHREADS = 128;
-constexpr int TMEM_COLS = TZ * 16 < 32 ? 32 : TZ * 16;       // TZ slices x 16 columns
+constexpr int ACC_COLS = (TZ + 4) * 16;                       // slices -1 .. TZ + 2
+constexpr int TMEM_COLS = ACC_COLS <= 64 ? 64 : (ACC_COLS <= 128 ? 128 : 256);
 constexpr uint32_t TMA_BYTES = (uint32_t)X_BYTES;
 // Bounded waits: a wait gives up after WAIT_NS of %globaltimer time or
 // WAIT_POLLS polls, whichever comes first (the poll count only backs up the
@@ -78,7 +88,7 @@ constexpr long long WAIT_POLLS = 1ll << 24;
 
 static_assert(TX == 8 && TX * TY == 128, "a z-slice is 16 core matrices of 8 x-nodes");
 static_assert(PLANE_BYTES % 128 == 0, "TMA destinations 128-byte aligned");
-static_assert(TZ * 16 <= TMEM_COLS, "accumulators fit the allocation");
+static_assert(ACC_COLS <= TMEM_COLS, "accumulators fit the allocation");
 
 // Shared-memory matrix descriptor (tcgen05): no swizzle, K-major.  Fields in
 // 16-byte units: start address [0,14), leading byte offset (between the two
@@ -97,6 +107,7 @@ __host__ __device__ constexpr uint32_t instr_desc(int m, int n) {
 }
 
 static_assert(instr_desc(128, 16) == 0x08040490u, "instruction descriptor encoding");
+static_assert(instr_desc(128, 48) == 0x080C0490u, "instruction descriptor encoding");
 static_assert(smem_desc(0x400, 17280, 160) ==
                   ((1ull << 46) | (10ull << 32) | (1080ull << 16) | 0x40ull),
               "shared-memory descriptor encoding");
@@ -247,19 +258,29 @@ __global__ void __launch_bounds__(NTHREADS) k_conv3_tc(const __grid_constant__ C
     } else {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       // descriptors: a fixed part plus the start address (16-byte units, low
-      // bits), so each of the 27 TZ MMAs adds a compile-time offset
+      // bits), so each MMA adds a compile-time offset.  Slice j's accumulator
+      // is at column 16 (j + 1); plane q writes slices q - 1 .. q + 1 from
+      // column 16 q.  The first write of each slice has the accumulate bit
+      // clear: plane 0's first MMA starts slices -1 .. 1, and the first
+      // shift of plane q >= 1 is split into N = 32 (slices q - 1, q) and a
+      // starting N = 16 (slice q + 1, weight rows 32 .. 47: 512 bytes on).
       const uint64_t a0 = smem_desc(xb, PLANE_BYTES, BX * 16);
-      const uint64_t b0 = smem_desc(wsb, 256, 128);
-      constexpr uint32_t idesc = instr_desc(128, 16);
-      // tap-major: consecutive MMAs go to the TZ independent accumulators
+      const uint64_t b0 = smem_desc(wsb, 768, 128);
+      constexpr uint32_t id48 = instr_desc(128, 48), id32 = instr_desc(128, 32),
+                         id16 = instr_desc(128, 16);
 #pragma unroll
-      for (int tap = 0; tap < 27; ++tap) {
+      for (int q = 0; q < TZ + 2; ++q) {
 #pragma unroll
-        for (int z = 0; z < TZ; ++z) {
-          const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
-          const uint32_t a_off = (uint32_t)(((z + 1 + dz) * BY + 1 + dy) * BX + 1 + dx);
-          umma_f16(tmem + (uint32_t)(z * 16), a0 + a_off, b0 + (uint32_t)(tap * 32), idesc,
-                   tap > 0 ? 1u : 0u);
+        for (int sh = 0; sh < 9; ++sh) {
+          const int dy = sh / 3 - 1, dx = sh % 3 - 1;
+          const uint64_t a = a0 + (uint32_t)((q * BY + 1 + dy) * BX + 1 + dx);
+          const uint64_t b = b0 + (uint32_t)(sh * 96);  // 1536 bytes per shift
+          if (sh == 0 && q > 0) {
+            umma_f16(tmem + (uint32_t)(16 * q), a, b, id32, 1u);
+            umma_f16(tmem + (uint32_t)(16 * (q + 2)), a, b + 32u, id16, 0u);
+          } else {
+            umma_f16(tmem + (uint32_t)(16 * q), a, b, id48, (q == 0 && sh == 0) ? 0u : 1u);
+          }
         }
       }
       umma_commit(mma_bar);
@@ -281,7 +302,7 @@ __global__ void __launch_bounds__(NTHREADS) k_conv3_tc(const __grid_constant__ C
 #pragma unroll
     for (int z = 0; z < TZ; ++z) {
       float v[16];
-      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(z * 16), v);
+      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(16 * (z + 2)), v);
       const int gz = z0 + z;
       if (gx < g.nx && gy < g.ny && gz < g.nz) {
         const int64_t row = (int64_t)gz * g.ny + gy;
