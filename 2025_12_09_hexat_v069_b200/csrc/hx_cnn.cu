@@ -215,6 +215,8 @@ __device__ __forceinline__ void prolong_axis(int f, int nc, int (&i)[2], float (
 template <int CH>
 __global__ void k_restrict(const float* __restrict__ in, float* __restrict__ out, GridN gf,
                            GridN gc, int normalise, const uint8_t* __restrict__ cmask) {
+  pdl_wait();
+  pdl_trigger();
   const int64_t nc = (int64_t)gc.nx * gc.ny * gc.nz;
   for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nc;
        n += (int64_t)gridDim.x * blockDim.x) {
@@ -396,6 +398,8 @@ __device__ __forceinline__ float bf16_bits(unsigned short h) { return __uint_as_
 __global__ void __launch_bounds__(256)
     k_restrict_ys(const __nv_bfloat16* __restrict__ ys, const CgState* sst, double scale_mul,
                   float* __restrict__ out, GridN gf, GridN gc, int cxw, int kseg) {
+  pdl_wait();
+  pdl_trigger();
   extern __shared__ __align__(16) unsigned char rsm[];
   const int seg = 3 * (2 * cxw + 1);
   const int segc = seg / 8 + 3;  // 16-byte chunks per staged row
@@ -523,10 +527,12 @@ __global__ void __launch_bounds__(256)
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
-static int ys_kseg(const GridN& gc, int cxw) {
+// coarse planes per CTA: as many segments as fill one wave of resident CTAs
+// (per_sm of them per SM; more segments would leave a partial second wave)
+static int ys_kseg(const GridN& gc, int cxw, int per_sm) {
   const int64_t cols = cdiv(gc.nx, cxw) * cdiv(gc.ny, YS_JB);
-  const int64_t want = 6LL * sm_count();  // CTAs: 6 per SM (shared memory)
-  const int64_t segs = std::max<int64_t>(1, std::min<int64_t>(gc.nz, cdiv(want, cols)));
+  const int64_t want = (int64_t)per_sm * sm_count();
+  const int64_t segs = std::max<int64_t>(1, std::min<int64_t>(gc.nz, want / cols));
   return (int)cdiv(gc.nz, segs);
 }
 
@@ -539,6 +545,8 @@ static size_t restrict_ys_smem(int cxw) {
 // fine[j][c] = (accumulate ? fine[j][c] : 0) + sum_{i: |j - 2i| <= 1} w(j - 2i) coarse[i][c].
 __global__ void k_prolong(const float* __restrict__ coarse, float* __restrict__ fine, GridN gf,
                           GridN gc, int accumulate, const uint8_t* __restrict__ fmask) {
+  pdl_wait();
+  pdl_trigger();
   const int64_t nf = (int64_t)gf.nx * gf.ny * gf.nz;
   for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nf;
        n += (int64_t)gridDim.x * blockDim.x) {
@@ -581,6 +589,8 @@ __global__ void k_prolong(const float* __restrict__ coarse, float* __restrict__ 
 // BF16, stored as half-rows (act16).
 __global__ void k_lift(const float* __restrict__ x, const float* __restrict__ feat,
                        __nv_bfloat16* __restrict__ X, GridN g) {
+  pdl_wait();
+  pdl_trigger();
   const int64_t nn = (int64_t)g.nx * g.ny * g.nz;
   for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn;
        n += (int64_t)gridDim.x * blockDim.x) {
@@ -605,6 +615,8 @@ __global__ void k_lift(const float* __restrict__ x, const float* __restrict__ fe
 // acc[n][c] (+)= Y[c] + feat * Y[c + 3].
 __global__ void k_unlift(const __nv_bfloat16* __restrict__ Y, const float* __restrict__ feat,
                          float* __restrict__ acc, int accumulate, int64_t nn) {
+  pdl_wait();
+  pdl_trigger();
   for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn;
        n += (int64_t)gridDim.x * blockDim.x) {
     const uint4 yy = *reinterpret_cast<const uint4*>(Y + n * 8);
@@ -636,6 +648,8 @@ __global__ void __launch_bounds__(256)
     k_net_output(const T* __restrict__ r, const T* __restrict__ minv, const float* __restrict__ t,
                  GridN gf, GridN gc, int cxw, CgState* st, double scale_mul, T* __restrict__ z,
                  const T* __restrict__ q_old, double* partials) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ float cyz[4][(ROW_CX + 1) * 3];  // [oy + 2 oz][cell][c]
   if (st->status != HX_RUNNING) return;
   const double s = sqrt(st->rz * scale_mul);
@@ -799,11 +813,14 @@ void launch_restrict_ys(cudaStream_t s, const __nv_bfloat16* ys, const CgState* 
                                  (int)restrict_ys_smem(YS_CX)));
   });
   const int cxw = (int)cdiv(gc.nx, cdiv(gc.nx, YS_CX));
-  const int kseg = ys_kseg(gc, cxw);
+  int per_sm = 0;
+  HX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_restrict_ys, 256,
+                                                        restrict_ys_smem(cxw)));
+  const int kseg = ys_kseg(gc, cxw, std::max(per_sm, 1));
   const dim3 grid((unsigned)cdiv(gc.nx, cxw), (unsigned)cdiv(gc.ny, YS_JB),
                   (unsigned)cdiv(gc.nz, kseg));
-  k_restrict_ys<<<grid, 256, restrict_ys_smem(cxw), s>>>(ys, sst, scale_mul, out, gf, gc, cxw,
-                                                         kseg);
+  launch_pdl(k_restrict_ys, grid, 256, restrict_ys_smem(cxw), s, ys, sst, scale_mul, out, gf, gc,
+             cxw, kseg);
   HX_CHECK_LAUNCH();
 }
 
@@ -812,9 +829,10 @@ void launch_restrict(cudaStream_t s, int ch, const float* in, float* out, const 
   const int64_t nc = (int64_t)gc.nx * gc.ny * gc.nz;
   HX_REQUIRE(ch == 3 || !cmask, "a DOF mask needs 3 channels");
   if (ch == 3)
-    k_restrict<3><<<vec_blocks(nc), 256, 0, s>>>(in, out, gf, gc, normalise ? 1 : 0, cmask);
+    launch_pdl(k_restrict<3>, vec_blocks(nc), 256, 0, s, in, out, gf, gc, normalise ? 1 : 0, cmask);
   else if (ch == 1)
-    k_restrict<1><<<vec_blocks(nc), 256, 0, s>>>(in, out, gf, gc, normalise ? 1 : 0, nullptr);
+    launch_pdl(k_restrict<1>, vec_blocks(nc), 256, 0, s, in, out, gf, gc, normalise ? 1 : 0,
+               (const uint8_t*)nullptr);
   else
     throw Error{HX_BAD_ARG, "unsupported channel count"};
   HX_CHECK_LAUNCH();
@@ -823,19 +841,19 @@ void launch_restrict(cudaStream_t s, int ch, const float* in, float* out, const 
 void launch_prolong(cudaStream_t s, const float* coarse, float* fine, const GridN& gf,
                     const GridN& gc, bool accumulate, const uint8_t* fmask) {
   const int64_t nf = (int64_t)gf.nx * gf.ny * gf.nz;
-  k_prolong<<<vec_blocks(nf), 256, 0, s>>>(coarse, fine, gf, gc, accumulate ? 1 : 0, fmask);
+  launch_pdl(k_prolong, vec_blocks(nf), 256, 0, s, coarse, fine, gf, gc, accumulate ? 1 : 0, fmask);
   HX_CHECK_LAUNCH();
 }
 
 void launch_lift(cudaStream_t s, const float* x, const float* feat, __nv_bfloat16* X,
                  const GridN& g) {
-  k_lift<<<vec_blocks((int64_t)g.nx * g.ny * g.nz), 256, 0, s>>>(x, feat, X, g);
+  launch_pdl(k_lift, vec_blocks((int64_t)g.nx * g.ny * g.nz), 256, 0, s, x, feat, X, g);
   HX_CHECK_LAUNCH();
 }
 
 void launch_unlift(cudaStream_t s, const __nv_bfloat16* Y, const float* feat, float* acc,
                    bool accumulate, int64_t nn) {
-  k_unlift<<<vec_blocks(nn), 256, 0, s>>>(Y, feat, acc, accumulate ? 1 : 0, nn);
+  launch_pdl(k_unlift, vec_blocks(nn), 256, 0, s, Y, feat, acc, accumulate ? 1 : 0, nn);
   HX_CHECK_LAUNCH();
 }
 
@@ -847,8 +865,8 @@ void launch_net_output(cudaStream_t s, const T* r, const T* minv, const float* t
   // 2 net_output_blocks(gf) values
   const int cxw = row_chunk(gc.nx);
   const dim3 grid((unsigned)cdiv(gc.nx, cxw), (unsigned)gc.ny, (unsigned)gc.nz);
-  k_net_output<T><<<grid, 256, 0, s>>>(r, minv, t, gf, gc, cxw, st, scale_mul, z, q_old,
-                                       partials);
+  launch_pdl(k_net_output<T>, grid, 256, 0, s, r, minv, t, gf, gc, cxw, st, scale_mul, z, q_old,
+             partials);
   HX_CHECK_LAUNCH();
 }
 

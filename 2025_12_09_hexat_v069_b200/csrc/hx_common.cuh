@@ -7,6 +7,7 @@
 
 #include <atomic>
 #include <string>
+#include <utility>
 
 #include "../../include/hexat_b200.h"
 
@@ -45,6 +46,32 @@ int64_t& launch_counter();
   do {                                                       \
     if (!(cond)) throw ::hx::Error{HX_BAD_ARG, (msg)};       \
   } while (0)
+
+// Programmatic dependent launch.  A kernel launched by launch_pdl may be
+// scheduled while the previous kernel on its stream is still running; it
+// calls pdl_wait() before its first global memory access, which returns once
+// that kernel has completed and its writes are visible (and at once after an
+// ordinary launch), and pdl_trigger() to let its own dependent be scheduled.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                Args&&... args) {
+  cudaLaunchConfig_t lc{};
+  lc.gridDim = grid;
+  lc.blockDim = block;
+  lc.dynamicSmemBytes = smem;
+  lc.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  lc.attrs = at;
+  lc.numAttrs = 1;
+  HX_CUDA(cudaLaunchKernelEx(&lc, kernel, std::forward<Args>(args)...));
+}
 
 // ---------------------------------------------------------------------------
 // Device-resident Krylov state.  All scalars of a CG run (alpha, beta, dot
