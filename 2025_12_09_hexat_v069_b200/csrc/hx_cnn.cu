@@ -644,7 +644,7 @@ __global__ void k_unlift(const __nv_bfloat16* __restrict__ Y, const float* __res
 // memory (one row per fine (fy, fz)); each fine DOF then needs two shared
 // loads for its x interpolation.
 template <typename T>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 6 : 5)
     k_net_output(const T* __restrict__ r, const T* __restrict__ minv, const float* __restrict__ t,
                  GridN gf, GridN gc, int cxw, CgState* st, double scale_mul, T* __restrict__ z,
                  const T* __restrict__ q_old, double* partials) {
@@ -683,13 +683,22 @@ __global__ void __launch_bounds__(256)
   // row 0 and not stored
   const int fx0 = 2 * cx0;
   const int L = 3 * (min(2 * (cx0 + w), gf.nx) - fx0);
-  int64_t rowb[4];
-  bool rowok[4];
+  // the rows' first DOFs as offsets from row 0's (32-bit: at most a fine
+  // plane of DOFs and a row, which the grid extent limit keeps below 2^31),
+  // to save registers: 6 CTAs per SM instead of 5 keep more loads in flight
+  const int64_t base = 3 * (((int64_t)(2 * k) * gf.ny + 2 * j) * gf.nx + fx0);
+  const T* rb = r + base;
+  const T* mb = minv + base;
+  const T* qb = q_old ? q_old + base : nullptr;
+  T* zb = z + base;
+  int rowo[4];
+  unsigned rowok = 0;
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     const int fy = 2 * j + (q & 1), fz = 2 * k + (q >> 1);
-    rowok[q] = fy < gf.ny && fz < gf.nz;
-    rowb[q] = rowok[q] ? 3 * (((int64_t)fz * gf.ny + fy) * gf.nx + fx0) : rowb[0];
+    const bool ok = fy < gf.ny && fz < gf.nz;
+    rowok |= (ok ? 1u : 0u) << q;
+    rowo[q] = ok ? 3 * ((q >> 1) * gf.ny * gf.nx + (q & 1) * gf.nx) : 0;
   }
   const float sf = (float)s;
   T zq = T(0), zr = T(0);  // per-thread partials in the vectors' precision
@@ -699,17 +708,17 @@ __global__ void __launch_bounds__(256)
     T mv[4], rv[4], qv[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      mv[q] = minv[rowb[q] + dl];
-      rv[q] = r[rowb[q] + dl];
-      qv[q] = q_old ? q_old[rowb[q] + dl] : T(0);
+      mv[q] = mb[rowo[q] + dl];
+      rv[q] = rb[rowo[q] + dl];
+      qv[q] = qb ? qb[rowo[q] + dl] : T(0);
     }
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      if (!rowok[q]) continue;
+      if (!((rowok >> q) & 1u)) continue;
       const float a = (fl & 1) ? 0.5f * (cyz[q][ce] + cyz[q][ce + 3]) : cyz[q][ce];
       // the correction is BF16-accurate: formed in FP32
       const T zi = mv[q] * rv[q] + (T)(sf * dinv_sqrt((float)mv[q]) * a);
-      z[rowb[q] + dl] = zi;
+      zb[rowo[q] + dl] = zi;
       zq += zi * qv[q];
       zr += zi * rv[q];
     }
