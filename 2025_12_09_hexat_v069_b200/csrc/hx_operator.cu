@@ -419,11 +419,28 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
       }
       face(pl1, a1, b1, c, v);
       face_fwd(v, Pt);
+      if constexpr (sizeof(T) == 4) {  // packed pairs: (q, q + 1)
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        if (PREFETCH) Pcarry[c][q] = Pt[q];
-        U[c][q] = Pb[q] + Pt[q];
-        U[c][q + 4] = Pt[q] - Pb[q];
+        for (int q = 0; q < 4; q += 2) {
+          if (PREFETCH) {
+            Pcarry[c][q] = Pt[q];
+            Pcarry[c][q + 1] = Pt[q + 1];
+          }
+          const float2 b = make_float2(Pb[q], Pb[q + 1]), t = make_float2(Pt[q], Pt[q + 1]);
+          const float2 su = __fadd2_rn(b, t);
+          const float2 di = __ffma2_rn(make_float2(-1.f, -1.f), b, t);
+          U[c][q] = su.x;
+          U[c][q + 1] = su.y;
+          U[c][q + 4] = di.x;
+          U[c][q + 5] = di.y;
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          if (PREFETCH) Pcarry[c][q] = Pt[q];
+          U[c][q] = Pb[q] + Pt[q];
+          U[c][q + 4] = Pt[q] - Pb[q];
+        }
       }
     }
     T rowS[3];
@@ -434,16 +451,26 @@ __global__ void __launch_bounds__(MV_BX* BY, MINB) k_struct(OpArgs<T> A) {
       else if (c == 1) lambda_row<T, 1>(A.K, U, Y);
       else lambda_row<T, 2>(A.K, U, Y);
       T F[4];
+      // bottom face: f (Y_s - Y_d) plus the layer below's top face; top
+      // face: f (Y_s + Y_d), carried to the layer above.  FP32 forms the sum
+      // and difference first and works in packed pairs (q, q + 1); in FP64
+      // that order needs more live registers than the 128-register bound.
+      if constexpr (sizeof(T) == 4) {
+        const float2 f2 = make_float2(f, f);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        // bottom face: f (Y_s - Y_d) plus the layer below's top face; top
-        // face: f (Y_s + Y_d), carried to the layer above.  (FP32 forms the
-        // sum and difference first, one instruction less; in FP64 that
-        // order needs more live registers than the 128-register bound.)
-        if (sizeof(T) == 4) {
-          F[q] = fma(f, Y[q] - Y[q + 4], Ytp[c][q]);
-          Ytp[c][q] = f * (Y[q] + Y[q + 4]);
-        } else {
+        for (int q = 0; q < 4; q += 2) {
+          const float2 ys = make_float2(Y[q], Y[q + 1]), yd = make_float2(Y[q + 4], Y[q + 5]);
+          const float2 di = __ffma2_rn(make_float2(-1.f, -1.f), yd, ys);
+          const float2 Fq = __ffma2_rn(f2, di, make_float2(Ytp[c][q], Ytp[c][q + 1]));
+          const float2 nt = __fmul2_rn(f2, __fadd2_rn(ys, yd));
+          F[q] = Fq.x;
+          F[q + 1] = Fq.y;
+          Ytp[c][q] = nt.x;
+          Ytp[c][q + 1] = nt.y;
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
           const T ys = Y[q] * f, yd = Y[q + 4] * f;
           F[q] = (ys - yd) + Ytp[c][q];
           Ytp[c][q] = ys + yd;
